@@ -1,0 +1,134 @@
+// Host-side helpers of the C ABI: errors carried as exceptions inside the library and turned into status codes at
+// the boundary, and owning wrappers of device and page-locked memory.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/es_b200.h"
+#include "es_kernels.h"
+
+namespace es {
+
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+void set_last_error(const std::string &msg);
+void clear_last_error();
+
+inline void cuda_check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return;
+    const int status = e == cudaErrorMemoryAllocation ? ES_ERR_ALLOC
+                       : (e == cudaErrorNoDevice || e == cudaErrorNoKernelImageForDevice || e == cudaErrorInsufficientDriver)
+                           ? ES_ERR_DEVICE
+                           : ES_ERR_CUDA;
+    throw Error(status, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+inline void require(bool ok, const std::string &what)
+{
+    if (!ok) throw Error(ES_ERR_INVALID, what);
+}
+
+// Runs f, turning exceptions into a status and the thread's last error.
+template <typename F>
+int guarded(F &&f)
+{
+    try {
+        clear_last_error();
+        f();
+        return ES_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        set_last_error("out of host memory");
+        return ES_ERR_ALLOC;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return ES_ERR_CUDA;
+    }
+}
+
+template <typename T>
+struct DeviceBuffer {
+    T *ptr = nullptr;
+    size_t count = 0;
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t n) { reset(n); }
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer() { release(); }
+    void reset(size_t n)
+    {
+        release();
+        if (n) cuda_check(cudaMalloc((void **)&ptr, n * sizeof(T)), "allocating GPU memory");
+        count = n;
+    }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+template <typename T>
+struct PinnedBuffer {
+    T *ptr = nullptr;
+    size_t count = 0;
+    PinnedBuffer() = default;
+    explicit PinnedBuffer(size_t n) { reset(n); }
+    PinnedBuffer(const PinnedBuffer &) = delete;
+    PinnedBuffer &operator=(const PinnedBuffer &) = delete;
+    ~PinnedBuffer() { release(); }
+    void reset(size_t n)
+    {
+        release();
+        if (n) cuda_check(cudaMallocHost((void **)&ptr, n * sizeof(T)), "allocating host memory");
+        count = n;
+    }
+    void release()
+    {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "creating a stream"); }
+    ~Stream() { if (s) cudaStreamDestroy(s); }
+    Stream(const Stream &) = delete;
+};
+
+struct Event {
+    cudaEvent_t e = nullptr;
+    Event() { cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating an event"); }
+    ~Event() { if (e) cudaEventDestroy(e); }
+    Event(const Event &) = delete;
+};
+
+// The current device must be an sm_100 part whose kernels load; throws ES_ERR_DEVICE otherwise.
+void check_device();
+
+// CAMBI's derived parameters (src/cambi.cpp:39-53).
+es_cambi_params derive_params(int w, int h);
+// lut[i] = 1/i as float for i < (2 pad + 1)^2 + 1, lut[0] = 0.
+void reciprocal_table(int pad, float *lut, size_t n);
+// src/cambi.cpp:29: clip((int)(topk * n), 1, n).
+unsigned long long topk_count(unsigned long long n, double topk);
+
+}  // namespace es
+
+struct es_module {
+    int device = 0;
+};

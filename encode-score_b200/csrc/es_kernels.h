@@ -1,0 +1,183 @@
+// Job descriptors and launchers shared by the host code (C++) and the kernels (CUDA).
+//
+// Kernels take their work as tables of jobs passed by value in the kernel parameters (up to 32 KB since CUDA 12.1),
+// so that one launch covers any mix of pictures and scales: the single-picture Cambi path and the batched frame step
+// use the same kernels. Each launcher returns the cudaError_t of the launch.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace es {
+
+constexpr int kScales = 5;
+constexpr int kDiffs = 4;
+constexpr uint16_t kNone = 0xFFFF;
+constexpr uint16_t kMaskBit = 0x8000;  // a scale's plane holds value | mask << 15
+constexpr int kMaxBand = 1024;         // codes of a 10-bit pipeline
+constexpr int kMaxPad = 64;            // window 129
+constexpr int kMaxJobs = 80;           // pictures x scales in one c-value launch
+constexpr int kWin = 16;               // detail window side (src/kernels.cu:331)
+
+// CAMBI's band parameters (src/kernels.cu:65-69 CambiParams without the per-scale size).
+struct Band {
+    int band_base, band_size, vlt;
+    int tvi[kDiffs];
+    int weight[kDiffs];
+};
+
+// ---- scale 0: preprocessing, zero-derivative mask and mode filter of one plane -------------------------------------
+struct Prep0Job {
+    const uint16_t *img;  // input plane, `pitch` pixels per row
+    int pitch, w, h, depth, mask_index;
+    uint16_t *word;       // out: w x h, mode-filtered value | mask << 15
+    int tiles_x, first_tile;
+};
+constexpr int kPrep0MaxJobs = 32;
+struct Prep0Batch {
+    Prep0Job job[kPrep0MaxJobs];
+    int njobs, total_tiles;
+};
+cudaError_t launch_prep0(const Prep0Batch &b, cudaStream_t s);
+
+// ---- scales 1..4: decimation and mode filter ------------------------------------------------------------------------
+struct DecJob {
+    const uint16_t *src;  // previous scale's words, sw x sh
+    int sw, sh;
+    uint16_t *dst;        // this scale's words, w x h
+    int w, h;
+    int first_block;      // blocks of 256 pixels
+};
+constexpr int kDecMaxJobs = 32;
+struct DecBatch {
+    DecJob job[kDecMaxJobs];
+    int njobs, total_blocks;
+};
+cudaError_t launch_decimate_mode(const DecBatch &b, cudaStream_t s);
+
+// ---- c-values --------------------------------------------------------------------------------------------------------
+// Per picture-scale counters in device memory. The c-values are exact multiples of 2^-24 (they are at least 0.5), so
+// their sum is kept exactly as an integer in those units; the order of additions does not matter.
+struct CvSlot {
+    unsigned long long sum_fx, count;  // positive c-values: sum in 2^-24 units, number
+    unsigned long long list_n;         // values appended to `list`
+    unsigned long long n, k;           // pixels of the scale, top-k count
+    unsigned long long remaining, above_fx, above_n;
+    unsigned prefix, mask;             // radix select state
+    float *list;                       // positive c-values (capacity n)
+    unsigned hist[2048];
+};
+
+struct CvJob {
+    const uint16_t *word;
+    int w, h, pad;
+    int tiles_x, first_tile;
+    int slot;       // index into the CvSlot array
+    float *plane;   // optional: every computed c-value at its pixel
+};
+struct CvBatch {
+    CvJob job[kMaxJobs];
+    int njobs, total_tiles, max_pad;
+    Band band;
+    const float *lut;  // lut[i] = 1/i as float, i < (2 max_pad + 1)^2 + 1
+    CvSlot *slots;
+};
+constexpr int kCvTX = 64, kCvTY = 32, kCvThreads = 256, kCvBins = 32;
+size_t cvalues_smem_bytes(int max_pad);
+cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s);
+
+// ---- top-k pooling and score -------------------------------------------------------------------------------------
+// Clears the counters of slots [0, nslots) and sets each slot's n and k.
+cudaError_t launch_slots_reset(CvSlot *slots, int nslots, const unsigned long long *n, const unsigned long long *k,
+                               cudaStream_t s);
+// One radix round of the exact k-th largest c-value of every slot whose positive count exceeds k.
+cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width, cudaStream_t s);
+// Sum and count of the values above the selected threshold.
+cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s);
+struct ScoreJob {
+    int first_slot;  // kScales consecutive slots
+    int window;
+    double *score;   // out
+};
+constexpr int kScoreMaxJobs = 32;
+struct ScoreBatch {
+    ScoreJob job[kScoreMaxJobs];
+    int njobs;
+    const CvSlot *slots;
+};
+cudaError_t launch_score(const ScoreBatch &b, cudaStream_t s);
+
+// ---- frame unpacking ---------------------------------------------------------------------------------------------
+struct FrameViewDev {
+    const void *y, *u, *v;
+    int ypitch, cpitch, semi, bytes, shift, depth;
+};
+struct UnpackJob {
+    FrameViewDev f;
+    int x0, y0;
+    uint16_t *y16, *u16, *v16;  // w x h, w/2 x h/2
+    int first_block;            // blocks of 2 x 2-pixel groups
+};
+constexpr int kUnpackMaxJobs = 32;
+struct UnpackBatch {
+    UnpackJob job[kUnpackMaxJobs];
+    int njobs, total_blocks, w, h, pd;
+};
+cudaError_t launch_unpack(const UnpackBatch &b, cudaStream_t s);
+
+// ---- detail window statistics ------------------------------------------------------------------------------------
+constexpr int kMaxEncodes = 16;
+struct WindowJob {
+    const uint16_t *yr;                 // source luma (pipeline depth)
+    const uint16_t *yd[kMaxEncodes];    // encode luma
+    float *stats[kMaxEncodes];          // per encode: windows x 8
+    int nenc, w, h, up;
+};
+cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s);
+
+// ---- lasting texture ------------------------------------------------------------------------------------------------
+// Running sums of the source's luma over the even and odd frame offsets of the centre frame c = f - 6:
+//   E(c) = sum y(c + k), k = +-2, +-4, +-6;   O(c) = sum y(c + k), k = +-1, +-3, +-5
+// with E(c) = O(c-1) - y(c) + y(c+6) and O(c) = E(c-1) - y(c-7) + y(c-1); missing frames count as 0.
+struct PersistJob {
+    const uint16_t *e_old, *o_old;  // 10-bit scale, w x h
+    uint16_t *e_new, *o_new;
+    const uint16_t *y_m13, *y_m7, *y_c, *y_f;  // frames f-13, f-7, f-6 (= centre), f; nullptr = zero
+    const uint16_t *yd[kMaxEncodes];           // encodes' luma at the centre frame
+    float *out[kMaxEncodes];                   // per encode: windows x 5
+    int nenc, w, h, up;
+    int stats;  // 0: only advance the running sums
+};
+cudaError_t launch_persist(const PersistJob &j, cudaStream_t s);
+
+// ---- PSNR squared errors and color sums --------------------------------------------------------------------------
+struct PairSumsJob {
+    const uint16_t *ry, *ru, *rv;  // source planes (pipeline depth)
+    const uint16_t *dy[kMaxEncodes], *du[kMaxEncodes], *dv[kMaxEncodes];
+    unsigned long long *sse;       // [nenc][3]
+    unsigned long long *color;     // [nenc + 1][3]: sum U, sum V, strength in 2^-30 units; source last
+    int nenc, w, h, up;
+};
+cudaError_t launch_pair_sums(const PairSumsJob &j, cudaStream_t s);
+
+// ---- per-frame reduction of the window figures (src/main.cpp:606-641) -------------------------------------------
+struct FrameFigures {
+    double all_r[3], all_d[3], st_r[3], st_d[3];
+    double sh_all_x[2], sh_st_x[2];
+    double own, mine;
+    unsigned n_structure, n_lasting;
+    float threshold;
+    unsigned pad_;
+};
+struct CollectJob {
+    const float *stats[kMaxEncodes];    // windows x 8
+    const float *persist[kMaxEncodes];  // windows x 5, centre frame (nullptr: no lasting texture this frame)
+    const uint8_t *centre_mask;         // structure mask of the centre frame
+    uint8_t *mask;                      // out: structure mask of this frame
+    FrameFigures *fig[kMaxEncodes];
+    uint16_t *bins[kMaxEncodes];        // out: 6 arrays of `windows` bins (amount 0-2, matching 0-1, lasting)
+    int nenc, windows;
+};
+cudaError_t launch_collect(const CollectJob &j, cudaStream_t s);
+
+}  // namespace es

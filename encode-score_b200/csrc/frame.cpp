@@ -1,0 +1,404 @@
+// es_frame: the per-frame measures of one source against its encodes, the queue / collect pair of
+// src/main.cpp:518-643 behind a C ABI.
+//
+// Frame f's GPU work is queued on the caller's stream (CAMBI continues on its instances' own streams) and its figures
+// arrive in page-locked memory; collect(f) waits for them and adds them to the caller's accumulators while the GPU
+// works on frame f + 1. Like the reference, whatever a frame's figures are read from comes in two, used by f % 2.
+//
+// Device state per run: the source's luma for the last 14 frames (the lasting texture needs frames f-13 .. f), each
+// encode's luma for the last 7 (its texture is measured at f - 6), the running even / odd luma sums of the source
+// around the centre frame (double-buffered), and the structure masks of the last 7 frames.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "es_internal.h"
+
+using namespace es;
+
+namespace {
+constexpr int kRing = 14, kEncRing = 7, kRadius = 6, kStats = 8, kPersist = 5, kBinArrays = 6;
+}
+
+struct es_frame {
+    int w = 0, h = 0, pd = 10, nenc = 0, ww = 0, wh = 0, windows = 0;
+    size_t n = 0;
+    DeviceBuffer<uint16_t> src_ring, src_u, src_v;
+    std::vector<std::unique_ptr<DeviceBuffer<uint16_t>>> enc_ring, enc_u, enc_v;
+    DeviceBuffer<uint16_t> run_e[2], run_o[2];
+    DeviceBuffer<float> stats[2], persist[2];  // [nenc][windows][8 | 5]
+    DeviceBuffer<uint8_t> masks;               // [kEncRing][windows]
+    DeviceBuffer<unsigned long long> sums[2];  // sse [nenc][3], then color [nenc + 1][3]
+    DeviceBuffer<FrameFigures> figs[2];
+    DeviceBuffer<uint16_t> bins[2];            // [nenc][6][windows]
+    PinnedBuffer<unsigned long long> h_sums[2];
+    PinnedBuffer<FrameFigures> h_figs[2];
+    PinnedBuffer<uint16_t> h_bins[2];
+    es_cambi *src_cambi[2] = {nullptr, nullptr};
+    std::vector<es_cambi *> enc_cambi[2];
+    Event done[2];
+    bool source_cambi[2] = {false, false};
+    long queued[2] = {-1, -1};
+    long next = 0, last_collected = -1;
+
+    ~es_frame()
+    {
+        for (int i = 0; i < 2; i++) {
+            es_cambi_destroy(src_cambi[i]);
+            for (es_cambi *c : enc_cambi[i]) es_cambi_destroy(c);
+        }
+    }
+    uint16_t *src_plane(long f) const { return src_ring.ptr + (size_t)(f % kRing) * n; }
+    uint16_t *enc_plane(int e, long f) const { return enc_ring[e]->ptr + (size_t)(f % kEncRing) * n; }
+};
+
+namespace {
+
+FrameViewDev view_of(const es_frame_view &v)
+{
+    FrameViewDev d;
+    d.y = v.y;
+    d.u = v.u;
+    d.v = v.v;
+    d.ypitch = v.ypitch;
+    d.cpitch = v.cpitch;
+    d.semi = v.semi;
+    d.bytes = v.bytes;
+    d.shift = v.shift;
+    d.depth = v.depth;
+    return d;
+}
+
+void check_view(const es_frame_view &v, int pd, const char *what)
+{
+    require(v.y != nullptr && v.u != nullptr && (v.semi || v.v != nullptr), std::string(what) + ": missing plane");
+    require(v.bytes == 1 || v.bytes == 2, std::string(what) + ": samples must be 1 or 2 bytes");
+    require(v.depth == 8 || v.depth == 10, std::string(what) + ": depth must be 8 or 10");
+    require(v.depth <= pd, std::string(what) + ": deeper than the pipeline");
+    require(v.shift >= 0 && v.shift < 16, std::string(what) + ": bad shift");
+}
+
+void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int sy, int source_cambi,
+                 const es_frame_view *encodes, const int *ex, const int *ey, cudaStream_t s)
+{
+    const int at = (int)(f % 2), up = 10 - fr->pd;
+    // unpack every picture of the step in one launch
+    UnpackBatch ub{};
+    ub.w = fr->w;
+    ub.h = fr->h;
+    ub.pd = fr->pd;
+    const int blocks = (int)(((size_t)(fr->w / 2) * (fr->h / 2) + 255) / 256);
+    int first = 0;
+    for (int p = 0; p <= fr->nenc; p++) {
+        UnpackJob &j = ub.job[p];
+        if (p == 0) {
+            j.f = view_of(*source);
+            j.x0 = sx;
+            j.y0 = sy;
+            j.y16 = fr->src_plane(f);
+            j.u16 = fr->src_u.ptr;
+            j.v16 = fr->src_v.ptr;
+        } else {
+            j.f = view_of(encodes[p - 1]);
+            j.x0 = ex ? ex[p - 1] : 0;
+            j.y0 = ey ? ey[p - 1] : 0;
+            j.y16 = fr->enc_plane(p - 1, f);
+            j.u16 = fr->enc_u[p - 1]->ptr;
+            j.v16 = fr->enc_v[p - 1]->ptr;
+        }
+        j.first_block = first;
+        first += blocks;
+    }
+    ub.njobs = fr->nenc + 1;
+    ub.total_blocks = first;
+    cuda_check(launch_unpack(ub, s), "unpacking frames");
+
+    // CAMBI of the source (unless cached) and of each encode; each continues on its own stream
+    fr->source_cambi[at] = source_cambi != 0;
+    if (source_cambi) {
+        const int r = es_cambi_launch(fr->src_cambi[at], (uint64_t)fr->src_plane(f), fr->w, s);
+        if (r) throw Error(r, es_last_error());
+    }
+    for (int e = 0; e < fr->nenc; e++) {
+        const int r = es_cambi_launch(fr->enc_cambi[at][e], (uint64_t)fr->enc_plane(e, f), fr->w, s);
+        if (r) throw Error(r, es_last_error());
+    }
+
+    // PSNR squared errors and color sums
+    cuda_check(cudaMemsetAsync(fr->sums[at].ptr, 0, fr->sums[at].bytes(), s), "clearing");
+    PairSumsJob pj{};
+    pj.ry = fr->src_plane(f);
+    pj.ru = fr->src_u.ptr;
+    pj.rv = fr->src_v.ptr;
+    for (int e = 0; e < fr->nenc; e++) {
+        pj.dy[e] = fr->enc_plane(e, f);
+        pj.du[e] = fr->enc_u[e]->ptr;
+        pj.dv[e] = fr->enc_v[e]->ptr;
+    }
+    pj.sse = fr->sums[at].ptr;
+    pj.color = fr->sums[at].ptr + 3 * fr->nenc;
+    pj.nenc = fr->nenc;
+    pj.w = fr->w;
+    pj.h = fr->h;
+    pj.up = up;
+    cuda_check(launch_pair_sums(pj, s), "squared errors and colors");
+
+    // detail window figures of frame f
+    WindowJob wj{};
+    wj.yr = fr->src_plane(f);
+    for (int e = 0; e < fr->nenc; e++) {
+        wj.yd[e] = fr->enc_plane(e, f);
+        wj.stats[e] = fr->stats[at].ptr + (size_t)e * fr->windows * kStats;
+    }
+    wj.nenc = fr->nenc;
+    wj.w = fr->w;
+    wj.h = fr->h;
+    wj.up = up;
+    cuda_check(launch_window_stats(wj, s), "window figures");
+
+    // lasting texture of frame f - 6, once frames f - 12 .. f are in
+    const bool texture = f >= 2 * kRadius;
+    PersistJob qj{};
+    const int cur = at;
+    qj.e_old = fr->run_e[cur ^ 1].ptr;
+    qj.o_old = fr->run_o[cur ^ 1].ptr;
+    qj.e_new = fr->run_e[cur].ptr;
+    qj.o_new = fr->run_o[cur].ptr;
+    qj.y_m13 = f >= 13 ? fr->src_plane(f - 13) : nullptr;
+    qj.y_m7 = f >= 7 ? fr->src_plane(f - 7) : nullptr;
+    qj.y_c = f >= 6 ? fr->src_plane(f - 6) : nullptr;
+    qj.y_f = fr->src_plane(f);
+    for (int e = 0; e < fr->nenc; e++) {
+        qj.yd[e] = f >= 6 ? fr->enc_plane(e, f - 6) : nullptr;
+        qj.out[e] = fr->persist[at].ptr + (size_t)e * fr->windows * kPersist;
+    }
+    qj.nenc = fr->nenc;
+    qj.w = fr->w;
+    qj.h = fr->h;
+    qj.up = up;
+    qj.stats = texture ? 1 : 0;
+    cuda_check(launch_persist(qj, s), "lasting texture");
+
+    // per-frame reduction on the device
+    CollectJob cj{};
+    for (int e = 0; e < fr->nenc; e++) {
+        cj.stats[e] = wj.stats[e];
+        cj.persist[e] = texture ? qj.out[e] : nullptr;
+        cj.fig[e] = fr->figs[at].ptr + e;
+        cj.bins[e] = fr->bins[at].ptr + (size_t)e * kBinArrays * fr->windows;
+    }
+    cj.centre_mask = fr->masks.ptr + (size_t)((f + kEncRing - kRadius) % kEncRing) * fr->windows;
+    cj.mask = fr->masks.ptr + (size_t)(f % kEncRing) * fr->windows;
+    cj.nenc = fr->nenc;
+    cj.windows = fr->windows;
+    if (fr->windows > 0) cuda_check(launch_collect(cj, s), "collecting figures");
+
+    cuda_check(cudaMemcpyAsync(fr->h_sums[at].ptr, fr->sums[at].ptr, fr->sums[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
+    if (fr->windows > 0) {
+        cuda_check(cudaMemcpyAsync(fr->h_figs[at].ptr, fr->figs[at].ptr, fr->figs[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
+        cuda_check(cudaMemcpyAsync(fr->h_bins[at].ptr, fr->bins[at].ptr, fr->bins[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
+    }
+    cuda_check(cudaEventRecord(fr->done[at].e, s), "event");
+    fr->queued[at] = f;
+}
+
+void add_bins(es_histogram &hist, const uint16_t *bins, int n)
+{
+    for (int i = 0; i < n; i++) {
+        const uint16_t b = bins[i];
+        if (b != kNone) {
+            hist.bins[b]++;
+            hist.n++;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int es_frame_create(const es_module *m, int w, int h, int pd, int n_encodes, es_frame **out)
+{
+    return guarded([&] {
+        require(m != nullptr && out != nullptr, "es_frame_create: NULL argument");
+        require(w >= 16 && h >= 16 && w % 2 == 0 && h % 2 == 0, "es_frame_create: the picture must be even and at least 16 x 16");
+        require(pd == 8 || pd == 10, "es_frame_create: pipeline depth must be 8 or 10");
+        require(n_encodes >= 1 && n_encodes <= kMaxEncodes, "es_frame_create: 1 to 16 encodes");
+        auto fr = std::make_unique<es_frame>();
+        fr->w = w;
+        fr->h = h;
+        fr->pd = pd;
+        fr->nenc = n_encodes;
+        fr->n = (size_t)w * h;
+        fr->ww = w / kWin;
+        fr->wh = h / kWin;
+        fr->windows = fr->ww * fr->wh;
+        const size_t n = fr->n, cn = n / 4, win = (size_t)fr->windows;
+        fr->src_ring.reset(n * kRing);
+        fr->src_u.reset(cn);
+        fr->src_v.reset(cn);
+        for (int e = 0; e < n_encodes; e++) {
+            fr->enc_ring.push_back(std::make_unique<DeviceBuffer<uint16_t>>(n * kEncRing));
+            fr->enc_u.push_back(std::make_unique<DeviceBuffer<uint16_t>>(cn));
+            fr->enc_v.push_back(std::make_unique<DeviceBuffer<uint16_t>>(cn));
+        }
+        for (int i = 0; i < 2; i++) {
+            fr->run_e[i].reset(n);
+            fr->run_o[i].reset(n);
+            cuda_check(cudaMemset(fr->run_e[i].ptr, 0, n * 2), "clearing");
+            cuda_check(cudaMemset(fr->run_o[i].ptr, 0, n * 2), "clearing");
+            fr->stats[i].reset(std::max<size_t>(1, win * kStats * n_encodes));
+            fr->persist[i].reset(std::max<size_t>(1, win * kPersist * n_encodes));
+            fr->sums[i].reset((size_t)3 * n_encodes + 3 * (n_encodes + 1));
+            fr->figs[i].reset(n_encodes);
+            fr->bins[i].reset(std::max<size_t>(1, win * kBinArrays * n_encodes));
+            fr->h_sums[i].reset(fr->sums[i].count);
+            fr->h_figs[i].reset(n_encodes);
+            fr->h_bins[i].reset(fr->bins[i].count);
+            std::memset(fr->h_figs[i].ptr, 0, sizeof(FrameFigures) * n_encodes);
+            for (int r = 0; r < 1 + n_encodes; r++) {
+                es_cambi *c = nullptr;
+                const int st = es_cambi_create(m, w, h, pd, &c);
+                if (st) throw Error(st, es_last_error());
+                if (r == 0) fr->src_cambi[i] = c;
+                else fr->enc_cambi[i].push_back(c);
+            }
+        }
+        fr->masks.reset(std::max<size_t>(1, win * kEncRing));
+        cuda_check(cudaMemset(fr->masks.ptr, 0, fr->masks.bytes()), "clearing");
+        cuda_check(cudaDeviceSynchronize(), "frame set-up");
+        *out = fr.release();
+    });
+}
+
+int es_frame_queue(es_frame *fr, long f, const es_frame_view *source, int sx, int sy, int source_cambi,
+                   const es_frame_view *encodes, const int *ex, const int *ey, void *stream)
+{
+    return guarded([&] {
+        require(fr != nullptr && source != nullptr && encodes != nullptr, "es_frame_queue: NULL argument");
+        require(f == fr->next, "es_frame_queue: frames must be queued in order from 0");
+        require(sx >= 0 && sy >= 0 && (sx % 2) == 0 && (sy % 2) == 0, "es_frame_queue: crop offsets must be even and >= 0");
+        check_view(*source, fr->pd, "source");
+        for (int e = 0; e < fr->nenc; e++) {
+            check_view(encodes[e], fr->pd, "encode");
+            if (ex) require(ex[e] >= 0 && ex[e] % 2 == 0, "es_frame_queue: crop offsets must be even and >= 0");
+            if (ey) require(ey[e] >= 0 && ey[e] % 2 == 0, "es_frame_queue: crop offsets must be even and >= 0");
+        }
+        const int at = (int)(f % 2);
+        if (fr->queued[at] > fr->last_collected)
+            throw Error(ES_ERR_STATE, "es_frame_queue: frame " + std::to_string(fr->queued[at]) + " has not been collected");
+        queue_frame(fr, f, source, sx, sy, source_cambi, encodes, ex, ey, (cudaStream_t)stream);
+        fr->next = f + 1;
+    });
+}
+
+int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es_accum *const *frame_acc,
+                     es_accum *const *centre_acc, es_frame_result *out)
+{
+    return guarded([&] {
+        require(fr != nullptr, "es_frame_collect: NULL frame");
+        const int at = (int)(f % 2);
+        if (fr->queued[at] != f) throw Error(ES_ERR_STATE, "es_frame_collect: frame " + std::to_string(f) + " was not queued");
+        if (f <= fr->last_collected) throw Error(ES_ERR_STATE, "es_frame_collect: frame collected twice");
+        cuda_check(cudaEventSynchronize(fr->done[at].e), "waiting for a frame");
+        double source_banding = 0;
+        if (fr->source_cambi[at]) {
+            const int r = es_cambi_finish(fr->src_cambi[at], &source_banding);
+            if (r) throw Error(r, es_last_error());
+        } else {
+            require(cached_source_cambi != nullptr, "es_frame_collect: the source's CAMBI was skipped and no cached value given");
+            source_banding = *cached_source_cambi;
+        }
+        const bool texture = f >= 2 * kRadius;
+        const size_t cn = fr->n / 4;
+        const unsigned long long *sse = fr->h_sums[at].ptr, *color = sse + 3 * fr->nenc;
+        const unsigned long long *scol = color + 3 * fr->nenc;
+        auto color_of = [](const unsigned long long *c, int i) {
+            return i < 2 ? (double)c[i] : (double)c[2] * (1.0 / 1073741824.0);
+        };
+        for (int e = 0; e < fr->nenc; e++) {
+            double banding = 0;
+            const int r = es_cambi_finish(fr->enc_cambi[at][e], &banding);
+            if (r) throw Error(r, es_last_error());
+            es_frame_result res{};
+            res.cambi = banding;
+            res.cambi_source = source_banding;
+            res.psnr[0] = es_psnr(sse[3 * e + 0], fr->n, fr->pd);
+            res.psnr[1] = es_psnr(sse[3 * e + 1], cn, fr->pd);
+            res.psnr[2] = es_psnr(sse[3 * e + 2], cn, fr->pd);
+            for (int i = 0; i < 3; i++) {
+                res.color_source[i] = color_of(scol, i) / (double)cn;
+                res.color_encode[i] = color_of(color + 3 * e, i) / (double)cn;
+            }
+            const FrameFigures &fg = fr->h_figs[at].ptr[e];
+            res.texture = texture;
+            res.structure_windows = fr->windows > 0 ? fg.n_structure : 0;
+            res.lasting_windows = texture && fr->windows > 0 ? fg.n_lasting : 0;
+            if (frame_acc && frame_acc[e]) {
+                es_accum &acc = *frame_acc[e];
+                acc.frames++;
+                acc.cambi += banding;
+                acc.cambi_source += source_banding;
+                for (int i = 0; i < 3; i++) {
+                    acc.psnr[i] += res.psnr[i];
+                    acc.color_r[i] += color_of(scol, i) / (double)cn;
+                    acc.color_d[i] += color_of(color + 3 * e, i) / (double)cn;
+                }
+                if (fr->windows > 0) {
+                    for (int k = 0; k < 3; k++) {
+                        acc.all_r[k] += fg.all_r[k];
+                        acc.all_d[k] += fg.all_d[k];
+                        acc.st_r[k] += fg.st_r[k];
+                        acc.st_d[k] += fg.st_d[k];
+                    }
+                    for (int k = 0; k < 2; k++) {
+                        acc.sh_all_r[k] += fg.all_r[k];
+                        acc.sh_all_x[k] += fg.sh_all_x[k];
+                        acc.sh_st_r[k] += fg.st_r[k];
+                        acc.sh_st_x[k] += fg.sh_st_x[k];
+                    }
+                    const uint16_t *b = fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows;
+                    for (int k = 0; k < 3; k++) add_bins(acc.amount[k], b + (size_t)k * fr->windows, fr->windows);
+                    for (int k = 0; k < 2; k++) add_bins(acc.matching[k], b + (size_t)(3 + k) * fr->windows, fr->windows);
+                }
+            }
+            if (texture && fr->windows > 0 && centre_acc && centre_acc[e]) {
+                es_accum &cacc = *centre_acc[e];
+                cacc.own += fg.own;
+                cacc.mine += fg.mine;
+                const uint16_t *b = fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows;
+                add_bins(cacc.lasting, b + (size_t)5 * fr->windows, fr->windows);
+            }
+            if (out) out[e] = res;
+        }
+        fr->last_collected = f;
+    });
+}
+
+int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist)
+{
+    return guarded([&] {
+        require(fr != nullptr, "es_frame_read_windows: NULL frame");
+        require(encode >= 0 && encode < fr->nenc, "es_frame_read_windows: encode out of range");
+        if (fr->last_collected < 0) throw Error(ES_ERR_STATE, "es_frame_read_windows: no frame collected");
+        const int at = (int)(fr->last_collected % 2);
+        const size_t win = (size_t)fr->windows;
+        if (stats && win)
+            cuda_check(cudaMemcpy(stats, fr->stats[at].ptr + (size_t)encode * win * kStats, win * kStats * 4, cudaMemcpyDeviceToHost), "reading");
+        if (persist && win) {
+            require(fr->last_collected >= 2 * kRadius, "es_frame_read_windows: no lasting texture before frame 12");
+            cuda_check(cudaMemcpy(persist, fr->persist[at].ptr + (size_t)encode * win * kPersist, win * kPersist * 4, cudaMemcpyDeviceToHost), "reading");
+        }
+    });
+}
+
+void es_frame_destroy(es_frame *fr)
+{
+    if (!fr) return;
+    cudaDeviceSynchronize();
+    delete fr;
+}
+
+}  // extern "C"

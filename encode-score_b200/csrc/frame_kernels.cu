@@ -1,0 +1,519 @@
+// Per-frame measures other than CAMBI, for sm_100a: frame unpacking, the detail / structure-tensor window energies,
+// the lasting-texture statistics, PSNR squared errors, color sums and the per-frame reduction into segment figures.
+//
+// The reference (src/kernels.cu:297-484, src/main.cpp:518-643) computes the window energies in FP32 from exact box
+// sums, writes two full FP32 mid-detail planes per encode, re-reads 13 of them per encode for the lasting texture and
+// reduces the windows on the host. Here every figure is computed from integer numerators (fine x 9, mid x 81,
+// gradients x 9) summed exactly in int64 and rounded once; the lasting texture keeps running integer sums of the
+// source's luma over the even and odd frame offsets (mid detail is linear in luma), so a frame step reads a few
+// 16-bit planes once for all encodes; and the per-frame reduction (structure threshold as an exact order statistic,
+// masks, sums, histogram bins) runs on the device.
+#include "es_kernels.h"
+
+namespace es {
+namespace {
+
+// ---------------------------------------------------------------------------------------------------------------
+// Frame unpacking: src/kernels.cu:289-310.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned sample_at(const void *plane, int pitch, int x, int y, const FrameViewDev &f)
+{
+    const unsigned char *row = (const unsigned char *)plane + (size_t)y * pitch;
+    const unsigned v = f.bytes == 1 ? row[x] : ((const uint16_t *)row)[x];
+    return v >> f.shift;
+}
+
+__global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ UnpackBatch b)
+{
+    int j = 0;
+    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
+    const UnpackJob &J = b.job[j];
+    const int cw = b.w / 2, ch = b.h / 2;
+    const int i = (blockIdx.x - J.first_block) * 256 + threadIdx.x;
+    if (i >= cw * ch) return;
+    const int cx = i % cw, cy = i / cw, up = b.pd - J.f.depth;
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+        const int y = 2 * cy + dy;
+        const unsigned a = sample_at(J.f.y, J.f.ypitch, 2 * cx + J.x0, y + J.y0, J.f);
+        const unsigned c = sample_at(J.f.y, J.f.ypitch, 2 * cx + 1 + J.x0, y + J.y0, J.f);
+        *(uint32_t *)(J.y16 + (size_t)y * b.w + 2 * cx) = (a << up) | ((c << up) << 16);
+    }
+    const int sx = (2 * cx + J.x0) / 2, sy = (2 * cy + J.y0) / 2;
+    const unsigned u = J.f.semi ? sample_at(J.f.u, J.f.cpitch, 2 * sx, sy, J.f) : sample_at(J.f.u, J.f.cpitch, sx, sy, J.f);
+    const unsigned v = J.f.semi ? sample_at(J.f.u, J.f.cpitch, 2 * sx + 1, sy, J.f) : sample_at(J.f.v, J.f.cpitch, sx, sy, J.f);
+    J.u16[(size_t)cy * cw + cx] = (uint16_t)(u << up);
+    J.v16[(size_t)cy * cw + cx] = (uint16_t)(v << up);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Box sums over a 64 x 32 tile with a 4-pixel margin, edge pixels repeated (src/kernels.cu:346-428 and
+// reference/encode_score/compare.py:77-108). A block of 256 threads: warp w owns window (w % 4, w / 4) of the tile,
+// lane l its column l % 16 and rows (l / 16) * 8 .. + 8.
+// ---------------------------------------------------------------------------------------------------------------
+constexpr int kTW = 64, kTH = 32, kM = 4;
+constexpr int kRW = kTW + 2 * kM, kRH = kTH + 2 * kM;  // 72 x 40
+
+struct BoxSmem {
+    uint16_t y[kRH][kRW];          // values on the 10-bit scale (or running sums)
+    uint16_t h3[kRH][kTW + 2];     // horizontal 3-sums at x0-1 .. x0+64
+    uint16_t h9[kRH][kTW];         // horizontal 9-sums at x0 .. x0+63
+    uint16_t s3[kTH + 2][kTW + 2]; // 3x3 sums at y0-1 .. y0+32, x0-1 .. x0+64
+    int32_t s9[kTH][kTW];          // 9x9 sums
+};
+
+// Loads a plane's region (clamped coordinates), shifted left by `up`; a null plane reads 0.
+__device__ __forceinline__ void load_region(uint16_t (*dst)[kRW], const uint16_t *src, int w, int h, int up, int x0, int y0)
+{
+    for (int i = threadIdx.x; i < kRH * kRW; i += 256) {
+        const int r = i / kRW, c = i - r * kRW;
+        const int x = min(max(x0 - kM + c, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
+        dst[r][c] = src ? (uint16_t)(src[(size_t)y * w + x] << up) : (uint16_t)0;
+    }
+}
+
+// h3, h9, s3, s9 of the region in sm.y; the caller synchronises before and after.
+__device__ __forceinline__ void box_sums(BoxSmem &sm, bool need_s3_margin)
+{
+    for (int i = threadIdx.x; i < kRH * (kTW + 2); i += 256) {
+        const int r = i / (kTW + 2), c = i - r * (kTW + 2);
+        sm.h3[r][c] = (uint16_t)(sm.y[r][c + 2] + sm.y[r][c + 3] + sm.y[r][c + 4]);
+    }
+    for (int i = threadIdx.x; i < kRH * kTW; i += 256) {
+        const int r = i / kTW, c = i - r * kTW;
+        unsigned s = 0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) s += sm.y[r][c + k];
+        sm.h9[r][c] = (uint16_t)s;
+    }
+    __syncthreads();
+    const int r0 = need_s3_margin ? 0 : 1, r1 = need_s3_margin ? kTH + 2 : kTH + 1;
+    for (int i = threadIdx.x; i < (r1 - r0) * (kTW + 2); i += 256) {
+        const int r = r0 + i / (kTW + 2), c = i % (kTW + 2);
+        sm.s3[r][c] = (uint16_t)(sm.h3[r + 2][c] + sm.h3[r + 3][c] + sm.h3[r + 4][c]);
+    }
+    for (int i = threadIdx.x; i < kTH * kTW; i += 256) {
+        const int r = i / kTW, c = i - r * kTW;
+        int s = 0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) s += sm.h9[r + k][c];
+        sm.s9[r][c] = s;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float exact_ratio(long long num, double den) { return __double2float_rn(__ddiv_rn((double)num, den)); }
+
+__device__ __forceinline__ float oriented_of(long long jxx, long long jyy, long long jxy)
+{
+    const double d = (double)(jxx - jyy), x = (double)jxy;
+    const double s = __dadd_rn(__dmul_rn(d, d), __dmul_rn(4.0, __dmul_rn(x, x)));
+    return __double2float_rn(__ddiv_rn(__dsqrt_rn(s), 81.0));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Window statistics of one source frame against every encode: src/kernels.cu:346-428, exact.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) window_stats_kernel(const __grid_constant__ WindowJob J)
+{
+    __shared__ BoxSmem sm;
+    const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
+    const int tiles_x = (ww + 3) / 4;
+    const int x0 = (blockIdx.x % tiles_x) * kTW, y0 = (blockIdx.x / tiles_x) * kTH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wx = x0 / kWin + (warp & 3), wy = y0 / kWin + (warp >> 2);
+    const bool inside = wx < ww && wy < wh;
+    const int c = (warp & 3) * kWin + (lane & 15), r0 = (warp >> 2) * kWin + (lane >> 4) * 8;  // tile coordinates
+    const int x = x0 + c;
+    int fr[8], mr[8];
+    long long src_f = 0, src_m = 0, src_jxx = 0, src_jyy = 0, src_jxy = 0;
+    for (int p = 0; p <= J.nenc; p++) {
+        const uint16_t *plane = p == 0 ? J.yr : J.yd[p - 1];
+        __syncthreads();
+        load_region(sm.y, plane, w, h, J.up, x0, y0);
+        __syncthreads();
+        box_sums(sm, true);
+        __syncthreads();
+        int fine_sq = 0, jxx = 0, jyy = 0, jxy = 0, fine_x = 0;
+        long long mid_sq = 0, mid_x = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int r = r0 + i, y = y0 + r;
+            const int s3 = sm.s3[r + 1][c + 1], s9 = sm.s9[r][c];
+            const int f = 9 * (int)sm.y[r + kM][c + kM] - s3, m = 9 * s3 - s9;
+            const int gx = (x > 0 && x < w - 1) ? (int)sm.s3[r + 1][c + 2] - (int)sm.s3[r + 1][c] : 0;
+            const int gy = (y > 0 && y < h - 1) ? (int)sm.s3[r + 2][c + 1] - (int)sm.s3[r][c + 1] : 0;
+            if (p == 0) {
+                fr[i] = f;
+                mr[i] = m;
+            } else {
+                fine_x += f * fr[i];
+                mid_x += (long long)m * mr[i];
+            }
+            fine_sq += f * f;
+            mid_sq += (long long)m * m;
+            jxx += gx * gx;
+            jyy += gy * gy;
+            jxy += gx * gy;
+        }
+        const long long sf = warp_sum((long long)fine_sq), sm2 = warp_sum(mid_sq), sxx = warp_sum((long long)jxx),
+                        syy = warp_sum((long long)jyy), sxy = warp_sum((long long)jxy);
+        if (p == 0) {
+            src_f = sf; src_m = sm2; src_jxx = sxx; src_jyy = syy; src_jxy = sxy;
+            continue;
+        }
+        const long long cf = warp_sum((long long)fine_x), cm = warp_sum(mid_x);
+        if (inside && lane == 0) {
+            float *o = J.stats[p - 1] + ((size_t)wy * ww + wx) * 8;
+            o[0] = exact_ratio(src_f, 81.0);
+            o[1] = exact_ratio(src_m, 6561.0);
+            o[2] = exact_ratio(sf, 81.0);
+            o[3] = exact_ratio(sm2, 6561.0);
+            o[4] = exact_ratio(cf, 81.0);
+            o[5] = exact_ratio(cm, 6561.0);
+            o[6] = oriented_of(src_jxx, src_jyy, src_jxy);
+            o[7] = oriented_of(sxx, syy, sxy);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Lasting texture: src/kernels.cu:435-451, exact, from running luma sums (see PersistJob).
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mids_of(BoxSmem &sm, int c, int r0, int *mid)
+{
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int r = r0 + i;
+        mid[i] = 9 * (int)sm.s3[r + 1][c + 1] - sm.s9[r][c];
+    }
+}
+
+__global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ PersistJob J)
+{
+    __shared__ BoxSmem sm;
+    __shared__ uint16_t o_reg[kRH][kRW];
+    const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
+    const int tiles_x = (w + kTW - 1) / kTW;
+    const int x0 = (blockIdx.x % tiles_x) * kTW, y0 = (blockIdx.x / tiles_x) * kTH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // advance the running sums over the region (clamped coordinates, so the margins repeat the edges)
+    for (int i = threadIdx.x; i < kRH * kRW; i += 256) {
+        const int r = i / kRW, cc = i - r * kRW;
+        const int x = min(max(x0 - kM + cc, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
+        const size_t k = (size_t)y * w + x;
+        const int ym13 = J.y_m13 ? (int)(J.y_m13[k] << J.up) : 0, ym7 = J.y_m7 ? (int)(J.y_m7[k] << J.up) : 0;
+        const int yc = J.y_c ? (int)(J.y_c[k] << J.up) : 0, yf = J.y_f ? (int)(J.y_f[k] << J.up) : 0;
+        const int e = (int)J.o_old[k] - yc + yf;   // E(c) = O(c-1) - y(c) + y(c+6)
+        const int o = (int)J.e_old[k] - ym13 + ym7;  // O(c) = E(c-1) - y(c-7) + y(c-1)
+        sm.y[r][cc] = (uint16_t)e;
+        o_reg[r][cc] = (uint16_t)o;
+        const int xi = x0 - kM + cc, yi = y0 - kM + r;
+        if (xi >= x0 && xi < x0 + kTW && yi >= y0 && yi < y0 + kTH && xi < w && yi < h) {
+            J.e_new[k] = (uint16_t)e;
+            J.o_new[k] = (uint16_t)o;
+        }
+    }
+    if (!J.stats) return;
+    const int wx = x0 / kWin + (warp & 3), wy = y0 / kWin + (warp >> 2);
+    const bool inside = wx < ww && wy < wh;
+    const int c = (warp & 3) * kWin + (lane & 15), r0 = (warp >> 2) * kWin + (lane >> 4) * 8;
+    int a[8], bb[8], t[8];
+    __syncthreads();
+    box_sums(sm, false);
+    __syncthreads();
+    mids_of(sm, c, r0, a);  // A x 486 = mid x 81 of E
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRH * kRW; i += 256) sm.y[i / kRW][i % kRW] = o_reg[i / kRW][i % kRW];
+    __syncthreads();
+    box_sums(sm, false);
+    __syncthreads();
+    mids_of(sm, c, r0, bb);  // B x 486
+    long long sab = 0, saa = 0, sbb = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        t[i] = a[i] + bb[i];  // T x 972
+        sab += (long long)a[i] * bb[i];
+        saa += (long long)a[i] * a[i];
+        sbb += (long long)bb[i] * bb[i];
+    }
+    sab = warp_sum(sab);
+    saa = warp_sum(saa);
+    sbb = warp_sum(sbb);
+    long long own = 0;
+    for (int p = 0; p <= J.nenc; p++) {
+        const uint16_t *plane = p == 0 ? J.y_c : J.yd[p - 1];
+        __syncthreads();
+        load_region(sm.y, plane, w, h, J.up, x0, y0);
+        __syncthreads();
+        box_sums(sm, false);
+        __syncthreads();
+        int m[8];
+        mids_of(sm, c, r0, m);
+        long long s = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) s += (long long)m[i] * t[i];
+        s = warp_sum(s);
+        if (p == 0) {
+            own = s;
+            continue;
+        }
+        if (inside && lane == 0) {
+            float *o = J.out[p - 1] + ((size_t)wy * ww + wx) * 5;
+            o[0] = exact_ratio(own, 78732.0);
+            o[1] = exact_ratio(s, 78732.0);
+            o[2] = exact_ratio(sab, 236196.0);
+            o[3] = exact_ratio(saa, 236196.0);
+            o[4] = exact_ratio(sbb, 236196.0);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// PSNR squared errors (src/kernels.cu:454-464) and color sums (470-484), exact integers; the color strength of each
+// sample sqrt(du^2 + dv^2) is rounded to units of 2^-30 so its sum is exact too. blockIdx.y picks the picture:
+// 0 .. nenc-1 the encodes (squared errors against the source, and their colors), nenc the source's colors.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ PairSumsJob J)
+{
+    const int p = blockIdx.y;
+    const bool src_only = p == J.nenc;
+    const size_t n = (size_t)J.w * J.h, cn = n / 4;
+    const size_t stride = (size_t)gridDim.x * 256, i0 = (size_t)blockIdx.x * 256 + threadIdx.x;
+    unsigned long long sy = 0, su = 0, sv = 0, cu = 0, cv = 0, cs = 0;
+    if (!src_only) {
+        const uint16_t *a = J.ry, *b = J.dy[p];
+        for (size_t i = i0; i < n; i += stride) {
+            const long long d = (long long)a[i] - (long long)b[i];
+            sy += (unsigned long long)(d * d);
+        }
+    }
+    const uint16_t *u = src_only ? J.ru : J.du[p], *v = src_only ? J.rv : J.dv[p];
+    for (size_t i = i0; i < cn; i += stride) {
+        if (!src_only) {
+            const long long du = (long long)J.ru[i] - (long long)u[i], dv = (long long)J.rv[i] - (long long)v[i];
+            su += (unsigned long long)(du * du);
+            sv += (unsigned long long)(dv * dv);
+        }
+        const int uu = u[i] << J.up, vv = v[i] << J.up, eu = uu - 512, ev = vv - 512;
+        cu += (unsigned long long)uu;
+        cv += (unsigned long long)vv;
+        cs += (unsigned long long)__double2ll_rn(__dmul_rn(__dsqrt_rn((double)(eu * eu + ev * ev)), 1073741824.0));
+    }
+    sy = warp_sum(sy); su = warp_sum(su); sv = warp_sum(sv);
+    cu = warp_sum(cu); cv = warp_sum(cv); cs = warp_sum(cs);
+    if ((threadIdx.x & 31) == 0) {
+        if (!src_only) {
+            atomicAdd(&J.sse[p * 3 + 0], sy);
+            atomicAdd(&J.sse[p * 3 + 1], su);
+            atomicAdd(&J.sse[p * 3 + 2], sv);
+        }
+        atomicAdd(&J.color[p * 3 + 0], cu);
+        atomicAdd(&J.color[p * 3 + 1], cv);
+        atomicAdd(&J.color[p * 3 + 2], cs);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Per-frame reduction, src/main.cpp:606-641 with quantile() of 280-289 and Histogram::add's binning of
+// src/stats.hpp:14-19. One block of 1024 threads per encode; each block finds the structure threshold itself (an
+// exact order statistic by a 3-round radix select of the source's oriented figures), so no block waits for another.
+// ---------------------------------------------------------------------------------------------------------------
+constexpr int kCT = 1024;
+
+__device__ __forceinline__ uint16_t hist_bin(double pct)
+{
+    const double c = pct < -500.0 ? -500.0 : pct > 500.0 ? 500.0 : pct;
+    return (uint16_t)llround(__ddiv_rn(__dadd_rn(c, 500.0), 0.05));
+}
+
+// The t-th smallest (0-based) of the non-negative floats v[i * stride] (their bit patterns order as the values).
+__device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, unsigned *hist)
+{
+    __shared__ unsigned s_prefix, s_mask, s_rem;
+    if (threadIdx.x == 0) { s_prefix = 0; s_mask = 0; s_rem = t; }
+    const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+    for (int round = 0; round < 3; round++) {
+        const int shift = shifts[round], nb = 1 << widths[round];
+        for (int i = threadIdx.x; i < 2048; i += kCT) hist[i] = 0;
+        __syncthreads();
+        const unsigned prefix = s_prefix, mask = s_mask;
+        for (int i = threadIdx.x; i < n; i += kCT) {
+            const unsigned bits = __float_as_uint(v[(size_t)i * stride]);
+            if ((bits & mask) == prefix) atomicAdd(&hist[(bits >> shift) & (unsigned)(nb - 1)], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned below = 0, rem = s_rem;
+            int d = 0;
+            for (; d < nb - 1 && below + hist[d] <= rem; d++) below += hist[d];
+            s_rem = rem - below;
+            s_prefix = prefix | ((unsigned)d << shift);
+            s_mask = mask | ((unsigned)(nb - 1) << shift);
+        }
+        __syncthreads();
+    }
+    return s_prefix;
+}
+
+template <typename T>
+__device__ T block_sum(T v, T *scratch)
+{
+    v = warp_sum(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T s = 0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kCT / 32; k++) s += scratch[k];
+    return s;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(kCT) collect_kernel(const __grid_constant__ CollectJob J)
+{
+    __shared__ unsigned hist[2048];
+    __shared__ double dscr[kCT / 32];
+    __shared__ unsigned uscr[kCT / 32];
+    __shared__ float s_q;
+    const int e = blockIdx.x, n = J.windows;
+    const float *st = J.stats[e];
+    // quantile(oriented of the source, 0.8) as numpy's linear interpolation of exact order statistics
+    {
+        const double pos = 0.8 * (double)(n - 1);
+        const unsigned lo = (unsigned)pos;
+        const float a = __uint_as_float(select_kth(st + 6, n, 8, lo, hist));
+        float q = a;
+        if (lo + 1 < (unsigned)n) {
+            const float b = __uint_as_float(select_kth(st + 6, n, 8, lo + 1, hist));
+            const float diff = __fsub_rn(b, a);
+            q = __double2float_rn(__dadd_rn((double)a, __dmul_rn((double)diff, __dsub_rn(pos, (double)lo))));
+        }
+        if (threadIdx.x == 0) s_q = q;
+        __syncthreads();
+    }
+    const float q = s_q;
+    const bool lasting = J.persist[e] != nullptr;
+    double all_r[3] = {0, 0, 0}, all_d[3] = {0, 0, 0}, st_r[3] = {0, 0, 0}, st_d[3] = {0, 0, 0};
+    double sh_all_x[2] = {0, 0}, sh_st_x[2] = {0, 0}, own = 0, mine = 0;
+    unsigned n_st = 0, n_last = 0;
+    uint16_t *bins = J.bins[e];
+    for (int i = threadIdx.x; i < n; i += kCT) {
+        const float *s = st + (size_t)i * 8;
+        const bool m = s[6] >= q && s[6] > 0.0f;
+        if (e == 0) J.mask[i] = m;
+        const double er[3] = {(double)s[0], (double)s[1], (double)s[6]}, ed[3] = {(double)s[2], (double)s[3], (double)s[7]};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            all_r[k] += er[k];
+            all_d[k] += ed[k];
+            uint16_t bin = kNone;
+            if (m) {
+                st_r[k] += er[k];
+                st_d[k] += ed[k];
+                bin = hist_bin(__dmul_rn(100.0, __dsqrt_rn(__ddiv_rn(ed[k], fmax(er[k], 1e-9)))));
+            }
+            bins[(size_t)k * n + i] = bin;
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const double x = (double)s[4 + k];
+            sh_all_x[k] += x;
+            uint16_t bin = kNone;
+            if (m) {
+                sh_st_x[k] += x;
+                bin = hist_bin(__ddiv_rn(__dmul_rn(100.0, x), fmax(er[k], 1e-9)));
+            }
+            bins[(size_t)(3 + k) * n + i] = bin;
+        }
+        n_st += m;
+        uint16_t lbin = kNone;
+        if (lasting) {
+            const float *ps = J.persist[e] + (size_t)i * 5;
+            const double agree = __ddiv_rn((double)ps[2], __dsqrt_rn(fmax(__dmul_rn((double)ps[3], (double)ps[4]), 1e-9)));
+            if (J.centre_mask[i] && agree > 0.5 && ps[0] > 0.0f) {
+                own += (double)ps[0];
+                mine += (double)ps[1];
+                lbin = hist_bin(__ddiv_rn(__dmul_rn(100.0, (double)ps[1]), (double)ps[0]));
+                n_last++;
+            }
+        }
+        bins[(size_t)5 * n + i] = lbin;
+    }
+    FrameFigures *f = J.fig[e];
+    double r;
+#define ES_REDUCE(dst, val) r = block_sum<double>(val, dscr); if (threadIdx.x == 0) dst = r;
+    for (int k = 0; k < 3; k++) {
+        ES_REDUCE(f->all_r[k], all_r[k]);
+        ES_REDUCE(f->all_d[k], all_d[k]);
+        ES_REDUCE(f->st_r[k], st_r[k]);
+        ES_REDUCE(f->st_d[k], st_d[k]);
+    }
+    for (int k = 0; k < 2; k++) {
+        ES_REDUCE(f->sh_all_x[k], sh_all_x[k]);
+        ES_REDUCE(f->sh_st_x[k], sh_st_x[k]);
+    }
+    ES_REDUCE(f->own, own);
+    ES_REDUCE(f->mine, mine);
+#undef ES_REDUCE
+    unsigned u = block_sum<unsigned>(n_st, uscr);
+    if (threadIdx.x == 0) f->n_structure = u;
+    u = block_sum<unsigned>(n_last, uscr);
+    if (threadIdx.x == 0) {
+        f->n_lasting = u;
+        f->threshold = q;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_unpack(const UnpackBatch &b, cudaStream_t s)
+{
+    if (b.total_blocks <= 0) return cudaSuccess;
+    unpack_kernel<<<b.total_blocks, 256, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s)
+{
+    const int ww = j.w / kWin, wh = j.h / kWin;
+    if (ww <= 0 || wh <= 0 || j.nenc <= 0) return cudaSuccess;
+    const int blocks = ((ww + 3) / 4) * ((wh + 1) / 2);
+    window_stats_kernel<<<blocks, 256, 0, s>>>(j);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_persist(const PersistJob &j, cudaStream_t s)
+{
+    const int blocks = ((j.w + kTW - 1) / kTW) * ((j.h + kTH - 1) / kTH);
+    persist_kernel<<<blocks, 256, 0, s>>>(j);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair_sums(const PairSumsJob &j, cudaStream_t s)
+{
+    pair_sums_kernel<<<dim3(148, j.nenc + 1), 256, 0, s>>>(j);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_collect(const CollectJob &j, cudaStream_t s)
+{
+    if (j.nenc <= 0 || j.windows <= 0) return cudaSuccess;
+    collect_kernel<<<j.nenc, kCT, 0, s>>>(j);
+    return cudaGetLastError();
+}
+
+const void *kernel_entry_unpack() { return (const void *)unpack_kernel; }
+const void *kernel_entry_window_stats() { return (const void *)window_stats_kernel; }
+const void *kernel_entry_persist() { return (const void *)persist_kernel; }
+const void *kernel_entry_pair_sums() { return (const void *)pair_sums_kernel; }
+const void *kernel_entry_collect() { return (const void *)collect_kernel; }
+
+}  // namespace es

@@ -1,0 +1,261 @@
+"""ctypes binding of libes_b200.so, the C ABI in include/es_b200.h.
+
+The library is built in-tree (``make -C encode-score_b200``). There is no fallback: if the library or a CUDA device
+is missing, loading or the first call raises.
+
+Device buffers are passed as integer addresses (``tensor.data_ptr()`` of a CUDA tensor works), streams as integer
+handles (``torch.cuda.current_stream().cuda_stream``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libes_b200.so")
+
+ES_OK, ES_ERR_INVALID, ES_ERR_CUDA, ES_ERR_ALLOC, ES_ERR_STATE, ES_ERR_DEVICE = range(6)
+HIST_BINS = 20001
+SCALES = 5
+
+# every symbol include/es_b200.h declares, for the load check
+SYMBOLS = (
+    "es_last_error", "es_version", "es_module_load", "es_module_unload", "es_module_get", "es_module_launch",
+    "es_cambi_create", "es_cambi_create_with", "es_cambi_derive_params", "es_cambi_get_params", "es_cambi_launch",
+    "es_cambi_finish", "es_cambi_destroy", "es_cambi_scale_stats", "es_cambi_read_scale", "es_cambi_set_cvalue_planes",
+    "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
+    "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
+)
+
+
+class EsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class CambiParams(ctypes.Structure):
+    _fields_ = [("w", ctypes.c_int), ("h", ctypes.c_int), ("window", ctypes.c_int), ("pad", ctypes.c_int), ("mask_index", ctypes.c_int),
+                ("band_base", ctypes.c_int), ("band_size", ctypes.c_int), ("vlt", ctypes.c_int), ("tvi", ctypes.c_int * 4),
+                ("weight", ctypes.c_int * 4), ("topk", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"w": self.w, "h": self.h, "window": self.window, "pad": self.pad, "mask_index": self.mask_index, "band_base": self.band_base,
+                "band_size": self.band_size, "vlt": self.vlt, "tvi": list(self.tvi), "weight": list(self.weight), "topk": self.topk}
+
+
+class FrameView(ctypes.Structure):
+    _fields_ = [("y", ctypes.c_void_p), ("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("ypitch", ctypes.c_int), ("cpitch", ctypes.c_int),
+                ("semi", ctypes.c_int), ("bytes", ctypes.c_int), ("shift", ctypes.c_int), ("depth", ctypes.c_int)]
+
+
+class Histogram(ctypes.Structure):
+    _fields_ = [("bins", ctypes.c_uint64 * HIST_BINS), ("n", ctypes.c_uint64)]
+
+
+class Accum(ctypes.Structure):
+    _fields_ = [("frames", ctypes.c_uint64), ("vmaf", ctypes.c_double), ("vmaf_min", ctypes.c_double), ("psnr", ctypes.c_double * 3),
+                ("cambi", ctypes.c_double), ("cambi_source", ctypes.c_double), ("color_r", ctypes.c_double * 3), ("color_d", ctypes.c_double * 3),
+                ("all_r", ctypes.c_double * 3), ("all_d", ctypes.c_double * 3), ("st_r", ctypes.c_double * 3), ("st_d", ctypes.c_double * 3),
+                ("amount", Histogram * 3), ("sh_all_r", ctypes.c_double * 2), ("sh_all_x", ctypes.c_double * 2), ("sh_st_r", ctypes.c_double * 2),
+                ("sh_st_x", ctypes.c_double * 2), ("matching", Histogram * 2), ("own", ctypes.c_double), ("mine", ctypes.c_double),
+                ("lasting", Histogram)]
+
+
+class Weights(ctypes.Structure):
+    _fields_ = [("fidelity", ctypes.c_double), ("texture", ctypes.c_double), ("banding", ctypes.c_double), ("grain", ctypes.c_double)]
+
+
+class Parts(ctypes.Structure):
+    _fields_ = [("fidelity", ctypes.c_double), ("texture", ctypes.c_double), ("banding", ctypes.c_double), ("grain", ctypes.c_double),
+                ("score", ctypes.c_double)]
+
+
+class FrameResult(ctypes.Structure):
+    _fields_ = [("cambi", ctypes.c_double), ("cambi_source", ctypes.c_double), ("psnr", ctypes.c_double * 3),
+                ("color_source", ctypes.c_double * 3), ("color_encode", ctypes.c_double * 3), ("texture", ctypes.c_int),
+                ("structure_windows", ctypes.c_uint32), ("lasting_windows", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library (raises OSError with the path if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
+        L.es_last_error.restype = ctypes.c_char_p
+        L.es_module_load.argtypes = [ctypes.POINTER(P)]
+        L.es_module_unload.argtypes = [P]
+        L.es_module_get.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(P)]
+        L.es_module_launch.argtypes = [P, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(P), P]
+        L.es_cambi_create.argtypes = [P, I, I, I, ctypes.POINTER(P)]
+        L.es_cambi_create_with.argtypes = [P, I, I, I, ctypes.POINTER(CambiParams), ctypes.POINTER(P)]
+        L.es_cambi_derive_params.argtypes = [I, I, ctypes.POINTER(CambiParams)]
+        L.es_cambi_get_params.argtypes = [P, ctypes.POINTER(CambiParams)]
+        L.es_cambi_launch.argtypes = [P, U64, I, P]
+        L.es_cambi_finish.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+        L.es_cambi_destroy.argtypes = [P]
+        L.es_cambi_scale_stats.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(U64), ctypes.POINTER(U64)]
+        L.es_cambi_read_scale.argtypes = [P, I, P, P]
+        L.es_cambi_set_cvalue_planes.argtypes = [P, ctypes.POINTER(P)]
+        L.es_histogram_add.argtypes = [ctypes.POINTER(Histogram), ctypes.c_double]
+        L.es_histogram_quantile.argtypes = [ctypes.POINTER(Histogram), ctypes.c_double]
+        L.es_histogram_quantile.restype = ctypes.c_double
+        L.es_accum_init.argtypes = [ctypes.POINTER(Accum)]
+        L.es_accum_merge.argtypes = [ctypes.POINTER(Accum), ctypes.POINTER(Accum)]
+        L.es_accum_score.argtypes = [ctypes.POINTER(Accum), ctypes.POINTER(Weights), ctypes.POINTER(Parts)]
+        L.es_accum_json.argtypes = [ctypes.POINTER(Accum), ctypes.c_char_p, ctypes.c_size_t]
+        L.es_accum_json.restype = ctypes.c_size_t
+        L.es_psnr.argtypes = [U64, U64, I]
+        L.es_psnr.restype = ctypes.c_double
+        L.es_frame_create.argtypes = [P, I, I, I, I, ctypes.POINTER(P)]
+        L.es_frame_queue.argtypes = [P, ctypes.c_long, ctypes.POINTER(FrameView), I, I, I, ctypes.POINTER(FrameView), ctypes.POINTER(I),
+                                     ctypes.POINTER(I), P]
+        L.es_frame_collect.argtypes = [P, ctypes.c_long, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.POINTER(Accum)),
+                                       ctypes.POINTER(ctypes.POINTER(Accum)), ctypes.POINTER(FrameResult)]
+        L.es_frame_read_windows.argtypes = [P, I, P, P]
+        L.es_frame_destroy.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != ES_OK:
+        raise EsError(status, lib().es_last_error().decode(errors="replace"))
+
+
+def derive_params(w: int, h: int) -> CambiParams:
+    p = CambiParams()
+    check(lib().es_cambi_derive_params(w, h, ctypes.byref(p)))
+    return p
+
+
+class Module:
+    """Kernels (src/gpu.hpp:15-23): binds to the current device, which must be sm_100."""
+
+    def __init__(self):
+        self.handle = ctypes.c_void_p()
+        check(lib().es_module_load(ctypes.byref(self.handle)))
+
+    def get(self, name: str) -> int:
+        f = ctypes.c_void_p()
+        check(lib().es_module_get(self.handle, name.encode(), ctypes.byref(f)))
+        return f.value
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_module_unload(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+class Cambi:
+    """class Cambi (src/cambi.hpp:9-21) through the C ABI."""
+
+    def __init__(self, module: Module, w: int, h: int, depth: int, params: CambiParams | None = None):
+        self.handle = ctypes.c_void_p()
+        self.w, self.h = w, h
+        if params is None:
+            check(lib().es_cambi_create(module.handle, w, h, depth, ctypes.byref(self.handle)))
+        else:
+            check(lib().es_cambi_create_with(module.handle, w, h, depth, ctypes.byref(params), ctypes.byref(self.handle)))
+
+    def params(self) -> CambiParams:
+        p = CambiParams()
+        check(lib().es_cambi_get_params(self.handle, ctypes.byref(p)))
+        return p
+
+    def launch(self, img: int, pitch: int, stream: int = 0) -> None:
+        check(lib().es_cambi_launch(self.handle, img, pitch, ctypes.c_void_p(stream)))
+
+    def finish(self) -> float:
+        s = ctypes.c_double()
+        check(lib().es_cambi_finish(self.handle, ctypes.byref(s)))
+        return s.value
+
+    def scale_stats(self) -> tuple[list, list, list]:
+        pooled = (ctypes.c_double * SCALES)()
+        sums = (ctypes.c_uint64 * SCALES)()
+        counts = (ctypes.c_uint64 * SCALES)()
+        check(lib().es_cambi_scale_stats(self.handle, pooled, sums, counts))
+        return list(pooled), list(sums), list(counts)
+
+    def read_scale(self, s: int):
+        import numpy as np
+        w, h = self.w, self.h
+        for _ in range(s):
+            w, h = (w + 1) >> 1, (h + 1) >> 1
+        image = np.zeros((h, w), np.uint16)
+        mask = np.zeros((h, w), np.uint8)
+        check(lib().es_cambi_read_scale(self.handle, s, image.ctypes.data, mask.ctypes.data))
+        return image, mask
+
+    def set_cvalue_planes(self, ptrs: list | None) -> None:
+        arr = (ctypes.c_void_p * SCALES)(*(ptrs or [None] * SCALES))
+        check(lib().es_cambi_set_cvalue_planes(self.handle, arr if ptrs else None))
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_cambi_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+def new_accum() -> Accum:
+    a = Accum()
+    lib().es_accum_init(ctypes.byref(a))
+    return a
+
+
+def accum_json(a: Accum) -> str:
+    n = lib().es_accum_json(ctypes.byref(a), None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib().es_accum_json(ctypes.byref(a), buf, n + 1)
+    return buf.value.decode()
+
+
+def accum_score(a: Accum, weights: Weights | None = None) -> Parts:
+    p = Parts()
+    lib().es_accum_score(ctypes.byref(a), ctypes.byref(weights) if weights else None, ctypes.byref(p))
+    return p
+
+
+class Frame:
+    """The per-frame queue / collect of src/main.cpp:518-643 through the C ABI."""
+
+    def __init__(self, module: Module, w: int, h: int, pd: int, n_encodes: int):
+        self.handle = ctypes.c_void_p()
+        self.w, self.h, self.n = w, h, n_encodes
+        check(lib().es_frame_create(module.handle, w, h, pd, n_encodes, ctypes.byref(self.handle)))
+
+    def queue(self, f: int, source: FrameView, encodes: list, stream: int = 0, sx: int = 0, sy: int = 0, source_cambi: bool = True,
+              ex: list | None = None, ey: list | None = None) -> None:
+        encs = (FrameView * self.n)(*encodes)
+        exa = (ctypes.c_int * self.n)(*(ex or [0] * self.n))
+        eya = (ctypes.c_int * self.n)(*(ey or [0] * self.n))
+        check(lib().es_frame_queue(self.handle, f, ctypes.byref(source), sx, sy, int(source_cambi), encs, exa, eya, ctypes.c_void_p(stream)))
+
+    def collect(self, f: int, frame_acc: list | None, centre_acc: list | None, cached_source_cambi: float | None = None) -> list:
+        out = (FrameResult * self.n)()
+        fa = (ctypes.POINTER(Accum) * self.n)(*[ctypes.pointer(a) for a in frame_acc]) if frame_acc else None
+        ca = (ctypes.POINTER(Accum) * self.n)(*[ctypes.pointer(a) for a in centre_acc]) if centre_acc else None
+        cached = ctypes.byref(ctypes.c_double(cached_source_cambi)) if cached_source_cambi is not None else None
+        check(lib().es_frame_collect(self.handle, f, cached, fa, ca, out))
+        return list(out)
+
+    def read_windows(self, encode: int, persist: bool = False):
+        import numpy as np
+        windows = (self.w // 16) * (self.h // 16)
+        st = np.zeros((windows, 8), np.float32)
+        ps = np.zeros((windows, 5), np.float32) if persist else None
+        check(lib().es_frame_read_windows(self.handle, encode, st.ctypes.data, ps.ctypes.data if persist else None))
+        return st, ps
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_frame_destroy(self.handle)
+            self.handle = ctypes.c_void_p()

@@ -1,0 +1,177 @@
+/*
+ * es_b200.h -- C ABI of the B200 (sm_100a) implementation of encode-score's per-frame measurement path.
+ *
+ * Every function returns an int status (ES_OK = 0) unless noted; es_last_error() gives the message of the calling
+ * thread's last failure. Device memory is passed as plain addresses (uint64_t, a CUdeviceptr), streams as void*
+ * (a CUstream / cudaStream_t). No function falls back to the CPU: without an sm_100 device they fail with
+ * ES_ERR_DEVICE.
+ *
+ * Reference interfaces replaced (paths inside the encode-score project):
+ *   es_module_*      Kernels::load / get / launch, src/gpu.hpp:15-23, src/gpu.cpp:6-19
+ *   es_cambi_*       class Cambi, src/cambi.hpp:9-21, src/cambi.cpp:31-184
+ *   es_frame_*       the per-frame queue / collect of src/main.cpp:518-643 (which launches frame_planes,
+ *                    window_stats, persist_stats, plane_sse and color_sums by name, src/main.cpp:229-234)
+ *   es_accum_*, es_histogram_*   struct Histogram / Accum / score, src/stats.hpp:10-83
+ */
+#ifndef ES_B200_H
+#define ES_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ES_OK 0
+#define ES_ERR_INVALID 1 /* an argument is out of range */
+#define ES_ERR_CUDA 2    /* a CUDA call failed */
+#define ES_ERR_ALLOC 3   /* device or pinned memory could not be allocated */
+#define ES_ERR_STATE 4   /* a call out of order, such as finish() without launch() */
+#define ES_ERR_DEVICE 5  /* no sm_100 device, or the kernels do not load on it */
+
+/* The message of the calling thread's last failure ("" if none). The pointer stays valid until the thread's next
+ * call into this library. */
+const char *es_last_error(void);
+/* Library version as MAJOR * 10000 + MINOR * 100 + PATCH. */
+int es_version(void);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Kernel module. Replaces Kernels (src/gpu.hpp:15-23): load() checks the current device and the kernels' image,
+ * get(name) returns a CUfunction of one of this library's kernels, launch() runs a 2-D kernel in 32 x 8 blocks.
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct es_module es_module;
+/* Kernels::load (src/gpu.cpp:6): binds to the current CUDA context's device; fails unless it is sm_100. */
+int es_module_load(es_module **out);
+void es_module_unload(es_module *m);
+/* Kernels::get (src/gpu.cpp:8-13): the CUfunction of a kernel by name, written to *function. */
+int es_module_get(const es_module *m, const char *name, void **function);
+/* Kernels::launch (src/gpu.cpp:15-19): grid ceil(w/32) x ceil(h/8) of 32 x 8 threads. */
+int es_module_launch(void *function, unsigned w, unsigned h, void **args, void *stream);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * CAMBI of one luma plane. Replaces class Cambi (src/cambi.hpp:9-21): create = Cambi(k, w, h, depth), launch =
+ * Cambi::launch, finish = Cambi::finish. launch() reads the plane on the caller's stream (after the work already
+ * queued there), then continues on the instance's own stream, so the caller may overwrite the plane with work it
+ * queues on its stream afterwards; each launch() must be followed by its finish() before the next launch().
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct es_cambi es_cambi;
+
+/* The parameters src/cambi.cpp:39-53 derives from the picture size; tvi[] in cambi.c's "+4" adjusted space. */
+typedef struct {
+    int w, h;       /* picture size */
+    int window;     /* odd window side (cambi.c adjust_window_size) */
+    int pad;        /* window >> 1 */
+    int mask_index; /* more than this many flat pixels in the 7x7 square put a pixel in the mask */
+    int band_base, band_size, vlt;
+    int tvi[4];
+    int weight[4];
+    double topk; /* share of each scale's pixels pooled (0.6) */
+} es_cambi_params;
+
+/* Cambi::Cambi (src/cambi.cpp:31-77): `depth` is the bit depth of the planes launch() will get, 8 or 10. */
+int es_cambi_create(const es_module *m, int w, int h, int depth, es_cambi **out);
+/* As es_cambi_create with the derived parameters replaced by *params (w and h must match); window up to 129. */
+int es_cambi_create_with(const es_module *m, int w, int h, int depth, const es_cambi_params *params, es_cambi **out);
+/* The parameters src/cambi.cpp:39-53 would derive for a w x h picture. */
+int es_cambi_derive_params(int w, int h, es_cambi_params *out);
+int es_cambi_get_params(const es_cambi *c, es_cambi_params *out);
+/* Cambi::launch (src/cambi.cpp:88-135): `img` is a device plane of w x h values at `depth` bits, `pitch` in
+ * pixels. */
+int es_cambi_launch(es_cambi *c, uint64_t img, int pitch, void *stream);
+/* Cambi::finish (src/cambi.cpp:172-184): waits and gives the score, capped at 1000. */
+int es_cambi_finish(es_cambi *c, double *score);
+void es_cambi_destroy(es_cambi *c);
+
+/* Introspection for tests and tools (no counterpart in the reference, whose buffers are private). After a finish():
+ * per scale, the pooled value, the exact sum of the positive c-values in units of 2^-24 and their count. */
+int es_cambi_scale_stats(const es_cambi *c, double pooled[5], uint64_t sums_fx[5], uint64_t counts[5]);
+/* After a finish(): copies scale s's picture (mode-filtered values, u16) and mask (u8) to host memory. */
+int es_cambi_read_scale(const es_cambi *c, int s, uint16_t *image, uint8_t *mask);
+/* With dev_planes[s] device buffers of scale s's size (float, zeroed by the caller), later launches also write every
+ * computed c-value there (the buffer kernels.cu's cambi_cvalues fills). NULL entries switch it off per scale. */
+int es_cambi_set_cvalue_planes(es_cambi *c, float *const dev_planes[5]);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * A decoded frame as the kernels read it: src/main.cpp:99-102 FrameView / src/kernels.cu:284-287 Frame. Planar or
+ * semi-planar 4:2:0 (chroma interleaved in u when semi), `bytes` per sample (1 or 2), sample value >> shift (6 for
+ * P010) with `depth` bits (8 or 10). Pitches in bytes. Device addresses.
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct {
+    const void *y, *u, *v;
+    int ypitch, cpitch, semi, bytes, shift, depth;
+} es_frame_view;
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Histogram / Accum / score: src/stats.hpp:10-83, identical layout and arithmetic.
+ * --------------------------------------------------------------------------------------------------------------- */
+#define ES_HIST_BINS 20001
+typedef struct {
+    uint64_t bins[ES_HIST_BINS];
+    uint64_t n;
+} es_histogram;
+
+typedef struct {
+    uint64_t frames;
+    double vmaf, vmaf_min, psnr[3], cambi, cambi_source;
+    double color_r[3], color_d[3];
+    double all_r[3], all_d[3], st_r[3], st_d[3];
+    es_histogram amount[3];
+    double sh_all_r[2], sh_all_x[2], sh_st_r[2], sh_st_x[2];
+    es_histogram matching[2];
+    double own, mine;
+    es_histogram lasting;
+} es_accum;
+
+typedef struct { double fidelity, texture, banding, grain; } es_weights;          /* src/stats.hpp:34 */
+typedef struct { double fidelity, texture, banding, grain, score; } es_parts;     /* src/stats.hpp:69 */
+
+void es_histogram_add(es_histogram *hist, double pct);                  /* src/stats.hpp:14-19 */
+double es_histogram_quantile(const es_histogram *hist, double q);       /* src/stats.hpp:20-30 */
+void es_accum_init(es_accum *a);                                        /* Accum{} (vmaf_min = 1e9) */
+void es_accum_merge(es_accum *a, const es_accum *o);                    /* src/stats.hpp:50-64 */
+/* src/stats.hpp:70-82; weights NULL = {0.30, 0.30, 0.25, 0.15}. */
+void es_accum_score(const es_accum *a, const es_weights *weights, es_parts *out);
+/* The segment's JSON object as src/main.cpp:738-757 writes it; returns the length it needs (excluding the NUL),
+ * writing at most `size` bytes. */
+size_t es_accum_json(const es_accum *a, char *buf, size_t size);
+
+/* PSNR as src/main.cpp:272-277: 10 log10(peak^2 / mse) capped at 6 depth + 12. */
+double es_psnr(uint64_t sse, uint64_t n, int depth);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Per-frame measures of one source against n encodes: src/main.cpp:518-643. es_frame_queue queues frame f's GPU
+ * work on `stream` (double-buffered by f % 2 like the reference), es_frame_collect(f) waits for it and adds the
+ * figures into the caller's accumulators.
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct es_frame es_frame;
+
+typedef struct {
+    double cambi, cambi_source; /* this frame */
+    double psnr[3];             /* Y, Cb, Cr */
+    double color_source[3], color_encode[3]; /* mean Cb, Cr and color strength on a 10-bit scale */
+    int texture;                /* 1 when the lasting texture of frame f - 6 was added */
+    uint32_t structure_windows; /* windows in the structure mask of frame f */
+    uint32_t lasting_windows;   /* lasting-texture windows of frame f - 6 (when texture) */
+} es_frame_result;
+
+/* `w` x `h` is the common picture area (even), `pd` the pipeline depth (8 or 10, src/main.cpp:377-382). */
+int es_frame_create(const es_module *m, int w, int h, int pd, int n_encodes, es_frame **out);
+/* Frame f (0, 1, 2, ... in order). source / encodes[i] are device frames cropped at (sx, sy) / (ex[i], ey[i]);
+ * source_cambi = 0 skips the source's CAMBI (src/main.cpp:522-523, a cached value given to collect instead). */
+int es_frame_queue(es_frame *fr, long f, const es_frame_view *source, int sx, int sy, int source_cambi,
+                   const es_frame_view *encodes, const int *ex, const int *ey, void *stream);
+/* Waits for frame f and adds its figures: frame_acc[i] receives encode i's figures of frame f, centre_acc[i] the
+ * lasting texture of frame f - 6 (src/main.cpp:630-641; may equal frame_acc[i] or be NULL when f < 12). With
+ * source_cambi = 0 at queue time, *cached_source_cambi is used (else ignored; may be NULL). out[i] may be NULL. */
+int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es_accum *const *frame_acc,
+                     es_accum *const *centre_acc, es_frame_result *out);
+/* Introspection for tests: after collect(f), encode i's window figures of frame f (windows x 8 floats, the layout of
+ * src/kernels.cu:340-341) and, when f >= 12, the lasting-texture figures of frame f - 6 (windows x 5 floats,
+ * src/kernels.cu:434); either pointer may be NULL. */
+int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist);
+void es_frame_destroy(es_frame *fr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,104 @@
+"""The product against the reference's own GPU implementation (its kernels and class Cambi compiled from its sources
+into oracle/_ref/), on the same inputs and the same CAMBI parameters:
+
+* CAMBI: every scale's picture, mask and c-value bit for bit, and the score within the reference's own summation
+  noise (it adds doubles in atomic order);
+* PSNR squared errors and color value sums exactly; the color strength within FP32 rounding;
+* window and lasting-texture figures within the reference's FP32 rounding, which the product does not share (it is
+  exact), measured against the FP64 oracle.
+"""
+
+import numpy as np
+import pytest
+
+import es_b200
+import es_synth
+import oracle
+from gpu_util import from_dev, to_dev, zeros_dev
+from test_gpu_cambi import CASES, oracle_params, params_for
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name,make,depth,over", [c for c in CASES if c[0] != "tiny"], ids=[c[0] for c in CASES if c[0] != "tiny"])
+def test_cambi_steps_match_the_reference_kernels(cuda, module, ref, name, make, depth, over):
+    torch = cuda
+    img = make()
+    h, w = img.shape
+    p = params_for(img, over)
+    if p.window > 65:
+        pytest.skip("the reference's reciprocal table stops at window 65")
+    sizes = oracle.scale_sizes(w, h)
+    images = [zeros_dev(torch, (sh, sw), np.uint16) for sw, sh in sizes]
+    masks = [zeros_dev(torch, (sh, sw), np.uint8) for sw, sh in sizes]
+    cvals = [zeros_dev(torch, (sh, sw), np.float32) for sw, sh in sizes]
+    scratch = zeros_dev(torch, (h, w), np.uint16)
+    sums = zeros_dev(torch, (10,), np.float64)
+    dimg = to_dev(torch, img)
+    ref.cambi_steps(dimg.data_ptr(), w, w, h, depth, p.as_dict(), [t.data_ptr() for t in images], [t.data_ptr() for t in masks],
+                    [t.data_ptr() for t in cvals], scratch.data_ptr(), sums.data_ptr())
+    cam = es_b200.Cambi(module, w, h, depth, p)
+    planes = [zeros_dev(torch, (sh, sw), np.float32) for sw, sh in sizes]
+    cam.set_cvalue_planes([t.data_ptr() for t in planes])
+    cam.launch(dimg.data_ptr(), w, 0)
+    cam.finish()
+    for s in range(oracle.SCALES):
+        image, mask = cam.read_scale(s)
+        assert np.array_equal(image, from_dev(images[s], np.uint16)), f"scale {s} picture"
+        assert np.array_equal(mask, from_dev(masks[s], np.uint8)), f"scale {s} mask"
+        assert np.array_equal(from_dev(planes[s], np.float32).view(np.uint32), from_dev(cvals[s], np.float32).view(np.uint32)), f"scale {s} c-values"
+    ref_sums = from_dev(sums, np.float64)
+    ref_counts = ref_sums[5:].view(np.uint64)
+    _, fx, counts = cam.scale_stats()
+    assert list(ref_counts) == counts
+    assert np.allclose(ref_sums[:5], np.array(fx) / 2.0 ** 24, rtol=1e-12, atol=0)
+    cam.close()
+
+
+@pytest.mark.parametrize("w,h,depth", [(1920, 1080, 10), (1280, 720, 8), (640, 360, 10)])
+def test_cambi_score_matches_the_reference_class(cuda, module, ref, w, h, depth):
+    torch = cuda
+    step = es_synth.c1_step(0, w=w, h=h) if depth == 8 else es_synth.c2_step(0, w=w, h=h, n_encodes=3)
+    for pic in [step.source] + step.encodes:
+        d = to_dev(torch, pic.y)
+        want = ref.cambi_score(d.data_ptr(), w, h, depth)
+        cam = es_b200.Cambi(module, w, h, depth)
+        cam.launch(d.data_ptr(), w, 0)
+        got = cam.finish()
+        cam.close()
+        assert abs(got - want) <= 1e-9 * max(1.0, abs(want)), (got, want)
+
+
+def test_sums_match_the_reference_kernels(cuda, ref):
+    torch = cuda
+    step = es_synth.c2_step(3, w=320, h=192, n_encodes=1)
+    a, b = to_dev(torch, step.source.y), to_dev(torch, step.encodes[0].y)
+    s = zeros_dev(torch, (3,), np.float64)
+    ref.plane_sse(a.data_ptr(), b.data_ptr(), 320 * 192, s.data_ptr())
+    assert int(from_dev(s, np.uint64)[0]) == oracle.plane_sse(step.source.y, step.encodes[0].y)
+    u, v = to_dev(torch, step.source.u), to_dev(torch, step.source.v)
+    ref.color_sums(u.data_ptr(), v.data_ptr(), u.numel(), 0, s.data_ptr())
+    got = from_dev(s, np.float64)
+    want = oracle.color_sums(step.source.u, step.source.v, 0)
+    assert got[0] == want[0] and got[1] == want[1]
+    assert abs(got[2] - want[2]) <= 1e-6 * want[2]
+
+
+def test_window_figures_against_the_reference_and_fp64(cuda, ref):
+    """The reference's FP32 window figures and the product's exact ones, each against the FP64 oracle."""
+    torch = cuda
+    w, h = 640, 368
+    step = es_synth.c2_step(1, w=w, h=h, n_encodes=1)
+    yr, yd = to_dev(torch, step.source.y), to_dev(torch, step.encodes[0].y)
+    ww, wh = w // 16, h // 16
+    mid_r, mid_d = zeros_dev(torch, (h, w), np.float32), zeros_dev(torch, (h, w), np.float32)
+    out = zeros_dev(torch, (ww * wh, 8), np.float32)
+    ref.window_stats(yr.data_ptr(), yd.data_ptr(), 0, w, h, mid_r.data_ptr(), mid_d.data_ptr(), out.data_ptr())
+    got_ref = from_dev(out, np.float32).astype(np.float64)
+    exact, exact32 = oracle.window_stats(step.source.y, step.encodes[0].y, 0)
+    scale = np.abs(exact).max(axis=0) + 1e-30
+    ref_err = np.abs(got_ref - exact) / scale
+    mine_err = np.abs(exact32.astype(np.float64) - exact) / scale
+    # the product rounds each figure once; the reference's FP32 sums differ by more, but stay close
+    assert mine_err.max() <= 2 ** -24
+    assert ref_err.max() < 1e-3
