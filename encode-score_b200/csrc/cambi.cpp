@@ -26,7 +26,7 @@ struct es_cambi {
     DeviceBuffer<double> score;  // score, then pooled per scale
     PinnedBuffer<double> host;
     Stream stream;
-    Event copied;
+    Event copied, finished;
     float *planes[kScales] = {};
     bool pending = false, done = false;
 };
@@ -90,7 +90,7 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
     pj.word = c->words[0].ptr;
     pj.tiles_x = (c->w + 63) / 64;
     pj.first_tile = 0;
-    pb.total_tiles = pj.tiles_x * ((c->h + 15) / 16);
+    pb.total_tiles = pj.tiles_x * ((c->h + 31) / 32);
     cuda_check(launch_prep0(pb, caller), "cambi scale 0");
     cuda_check(cudaEventRecord(c->copied.e, caller), "cambi event");
     cudaStream_t s = c->stream.s;
@@ -155,6 +155,7 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
     cuda_check(launch_score(sb, s), "cambi score");
     cuda_check(cudaMemcpyAsync(c->host.ptr, c->score.ptr, sizeof(double) * (1 + kScales), cudaMemcpyDeviceToHost, s),
                "reading the score");
+    cuda_check(cudaEventRecord(c->finished.e, s), "cambi event");
 }
 
 void set_lists(es_cambi *c)
@@ -167,6 +168,11 @@ void set_lists(es_cambi *c)
 }
 
 }  // namespace
+
+void cambi_join(es_cambi *c, cudaStream_t stream)
+{
+    cuda_check(cudaStreamWaitEvent(stream, c->finished.e, 0), "cambi event");
+}
 
 extern "C" {
 

@@ -1,0 +1,354 @@
+// CAMBI c-values for sm_100a: src/kernels.cu:113-278 (cambi.c's c_value_pixel over the (2 pad + 1)^2 window of every
+// masked pixel in the band, histogram windows clipped at the picture's edges), bit-exact, with a different algorithm.
+//
+// One 256-thread block per 64 x 32 tile of any scale of any picture (a table of jobs):
+//  1. a pre-check of the tile's own pixels lets tiles with nothing to compute (most tiles of most pictures) leave
+//     after reading 2048 words;
+//  2. the tile and its window margins are staged in shared memory as band codes (value - band_base of a masked pixel
+//     in the band, kNone otherwise); the codes that can matter -- occurring within kDiffs of a code whose c-value is
+//     needed -- are ranked in order, and each such code gets a table of the rank offsets of its 8 neighbours;
+//  3. per pass over 32 ranks: column counts of the ranks over the window rows slide down the tile; per row, only the
+//     ranks some pixel of that row reads are turned into window counts, by a warp-parallel prefix sum over the
+//     columns (window count = difference of two prefix values), and two warps compute the row's c-values from them.
+// Positive c-values are summed exactly (they are multiples of 2^-24), counted, and appended to the scale's list for
+// the top-k selection; nothing per pixel is written unless the caller asks for the c-value planes.
+#include "es_kernels.h"
+
+namespace es {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ bool needs_cvalue(int code, const Band &bd)
+{
+    const int value = code + bd.band_base + kDiffs;
+    bool any = false;
+#pragma unroll
+    for (int d = 0; d < kDiffs; d++) any |= value <= bd.tvi[d] && value + d + 1 > bd.vlt;
+    return any;
+}
+
+__host__ __device__ constexpr int cv_rw(int pad) { return kCvTX + 2 * pad; }
+__host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // column stride (scan width)
+__host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+struct CvLayout {
+    size_t codes, rank, nbr, colcnt, prefix, list, total;
+};
+__host__ __device__ inline CvLayout cv_layout(int pad)
+{
+    CvLayout l;
+    l.codes = 0;
+    l.rank = align16((size_t)cv_rw(pad) * (kCvTY + 2 * pad) * 2);
+    l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
+    l.colcnt = align16(l.nbr + (size_t)kMaxBand * 4);
+    l.prefix = align16(l.colcnt + (size_t)kCvBins * cv_cs(pad));
+    l.list = align16(l.prefix + (size_t)kCvBins * cv_cs(pad) * 2);
+    l.total = align16(l.list + (size_t)kCvTX * kCvTY * 4);
+    return l;
+}
+
+__device__ __forceinline__ uint16_t code_of(uint16_t word, const Band &bd)
+{
+    const unsigned u = (unsigned)(word & 0x7FFF) - (unsigned)bd.band_base;
+    return ((word & kMaskBit) && u < (unsigned)bd.band_size) ? (uint16_t)u : kNone;
+}
+
+__global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_constant__ CvBatch b)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t occ[32], srv[32], rel[32];
+    __shared__ uint16_t relpre[33];
+    __shared__ uint32_t rowneed[kCvTY];
+    __shared__ unsigned list_n;
+    __shared__ unsigned long long list_base;
+    __shared__ unsigned long long red_sum[kCvThreads / 32];
+    __shared__ unsigned red_cnt[kCvThreads / 32];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int j = 0;
+    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
+    const CvJob &J = b.job[j];
+    const Band &bd = b.band;
+    const int tile = blockIdx.x - J.first_tile;
+    const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * kCvTY;
+    const int w = J.w, h = J.h, P = J.pad;
+    const int rows = min(kCvTY, h - y0), cols = min(kCvTX, w - x0);
+
+    // 1. does any pixel of the tile need a c-value?
+    bool any = false;
+    for (int i = tid; i < kCvTX * kCvTY; i += kCvThreads) {
+        const int r = i >> 6, c = i & (kCvTX - 1);
+        if (r < rows && c < cols) {
+            const uint16_t code = code_of(J.word[(size_t)(y0 + r) * w + x0 + c], bd);
+            any |= code != kNone && needs_cvalue(code, bd);
+        }
+    }
+    if (!__syncthreads_or(any)) return;
+
+    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P);
+    const CvLayout L = cv_layout(P);
+    uint16_t *codes = (uint16_t *)(smem + L.codes);
+    uint16_t *rank = (uint16_t *)(smem + L.rank);
+    uint32_t *nbr = (uint32_t *)(smem + L.nbr);
+    uint8_t *colcnt = smem + L.colcnt;
+    uint16_t *prefix = (uint16_t *)(smem + L.prefix);
+    float *blist = (float *)(smem + L.list);
+    if (tid < 32) occ[tid] = srv[tid] = 0;
+    if (tid == 0) list_n = 0;
+    __syncthreads();
+
+    // 2. stage the region: threads cover 128 (or 256) columns of 2 (or 1) rows per iteration
+    {
+        const int wide = RW > 128, c = wide ? tid : (tid & 127), dr = wide ? 0 : (tid >> 7), step = wide ? 1 : 2;
+        const int x = x0 - P + c;
+        const bool col_in = c < RW && x >= 0 && x < w;
+        const bool col_tile = c >= P && c < P + cols;
+        for (int r0 = 0; r0 < RH; r0 += step) {
+            const int r = r0 + dr, y = y0 - P + r;
+            uint16_t code = kNone;
+            if (col_in && r < RH && y >= 0 && y < h) code = code_of(J.word[(size_t)y * w + x], bd);
+            if (c < RW && r < RH) codes[r * RW + c] = code;
+            const bool served = code != kNone && col_tile && r >= P && r < P + rows && needs_cvalue(code, bd);
+            // mark each run of equal codes in the warp once
+            const unsigned prev = __shfl_up_sync(kFull, (unsigned)code, 1);
+            if (code != kNone && (lane == 0 || prev != code)) atomicOr(&occ[code >> 5], 1u << (code & 31));
+            const unsigned sv = served ? code : 0xFFFFu;
+            const unsigned sprev = __shfl_up_sync(kFull, sv, 1);
+            if (served && (lane == 0 || sprev != sv)) atomicOr(&srv[code >> 5], 1u << (code & 31));
+        }
+    }
+    __syncthreads();
+
+    // the relevant codes: occurring within kDiffs of a code that needs c-values, ranked in order
+    if (warp == 0) {
+        const uint32_t s = srv[lane], sp = lane > 0 ? srv[lane - 1] : 0u, sn = lane < 31 ? srv[lane + 1] : 0u;
+        uint32_t dil = s;
+#pragma unroll
+        for (int k = 1; k <= kDiffs; k++) dil |= (s << k) | (sp >> (32 - k)) | (s >> k) | (sn << (32 - k));
+        const uint32_t r = occ[lane] & dil;
+        rel[lane] = r;
+        const unsigned cnt = __popc(r);
+        unsigned incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+        }
+        relpre[lane] = (uint16_t)(incl - cnt);
+        if (lane == 31) relpre[32] = (uint16_t)incl;
+    }
+    __syncthreads();
+    const int R = relpre[32];
+    for (int c = tid; c < bd.band_size; c += kCvThreads) {
+        const uint32_t word = rel[c >> 5], bit = 1u << (c & 31);
+        rank[c] = (word & bit) ? (uint16_t)(relpre[c >> 5] + __popc(word & (bit - 1u))) : kNone;
+    }
+    __syncthreads();
+    // the rank offsets (+4) of the 8 neighbours u-4 .. u-1, u+1 .. u+4 of each served code; 15 = none
+    for (int c = tid; c < bd.band_size; c += kCvThreads) {
+        if (!(srv[c >> 5] & (1u << (c & 31)))) continue;
+        const int rc = rank[c];
+        uint32_t packed = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int q = c + (i < 4 ? i - 4 : i - 3);
+            unsigned nib = 15u;
+            if (q >= 0 && q < bd.band_size && rank[q] != kNone) nib = (unsigned)((int)rank[q] - rc + 4);
+            packed |= nib << (4 * i);
+        }
+        nbr[c] = packed;
+    }
+
+    unsigned long long my_sum = 0;
+    unsigned my_cnt = 0;
+    const int cv_warp0 = kCvThreads / 32 - kCvTX / 32;  // the last two warps compute c-values
+    const int ct = tid - cv_warp0 * 32;                // their pixel column in the tile
+
+    for (int b0 = 0;;) {
+        const int B = min(kCvBins, R - b0);
+        const int lo = b0 ? b0 + kDiffs : 0, hi = b0 + kCvBins >= R ? R : b0 + kCvBins - kDiffs;
+        if (tid < kCvTY) rowneed[tid] = 0;
+        for (int i = tid * 16; i < kCvBins * CS; i += kCvThreads * 16) *(uint4 *)(colcnt + i) = make_uint4(0, 0, 0, 0);
+        __syncthreads();
+        // the ranks each row's pixels read in this pass: a warp covers 32 pixels of one row
+        for (int i = tid; i < kCvTY * kCvTX; i += kCvThreads) {
+            const int r = i >> 6, c = i & (kCvTX - 1);
+            uint32_t need = 0;
+            if (r < rows && c < cols) {
+                const uint16_t code = codes[(r + P) * RW + c + P];
+                if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
+                    const int rk = rank[code];
+                    if (rk >= lo && rk < hi) {
+                        need = 1u << (rk - b0);
+                        const uint32_t nb = nbr[code];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            const unsigned o = (nb >> (4 * k)) & 15u;
+                            if (o != 15u) need |= 1u << (rk + (int)o - 4 - b0);
+                        }
+                    }
+                }
+            }
+            need = __reduce_or_sync(kFull, need);
+            if (lane == 0 && need) atomicOr(&rowneed[r], need);
+        }
+        // column counts over the window rows of tile row 0 (region rows 0 .. 2P)
+        if (tid < RW) {
+            uint8_t *col = colcnt + tid;
+            const int last = min(2 * P, RH - 1);
+            for (int r = 0; r <= last; r++) {
+                const uint16_t code = codes[r * RW + tid];
+                if (code != kNone) {
+                    const int k = (int)rank[code] - b0;
+                    if ((unsigned)k < (unsigned)B) col[k * CS]++;
+                }
+            }
+        }
+        __syncthreads();
+        for (int r = 0; r < rows; r++) {
+            if (r > 0 && tid < RW) {
+                uint8_t *col = colcnt + tid;
+                const uint16_t cl = codes[(r - 1) * RW + tid];
+                if (cl != kNone) {
+                    const int k = (int)rank[cl] - b0;
+                    if ((unsigned)k < (unsigned)B) col[k * CS]--;
+                }
+                if (r + 2 * P < RH) {
+                    const uint16_t ce = codes[(r + 2 * P) * RW + tid];
+                    if (ce != kNone) {
+                        const int k = (int)rank[ce] - b0;
+                        if ((unsigned)k < (unsigned)B) col[k * CS]++;
+                    }
+                }
+            }
+            const uint32_t need = rowneed[r];
+            if (!need) continue;
+            __syncthreads();
+            // inclusive prefix sums over the columns of the ranks this row reads; warp w takes every 8th of them
+            for (int n = warp;; n += kCvThreads / 32) {
+                const int k = __fns(need, 0, n + 1);
+                if (k < 0 || k >= 32) break;
+                const uint8_t *col = colcnt + k * CS;
+                uint16_t *hrow = prefix + k * CS;
+                unsigned carry = 0;
+                for (int base = 0; base < CS; base += 128) {
+                    const uint32_t four = *(const uint32_t *)(col + base + 4 * lane);
+                    const unsigned s1 = four & 255u, s2 = s1 + ((four >> 8) & 255u), s3 = s2 + ((four >> 16) & 255u),
+                                   s4 = s3 + (four >> 24);
+                    unsigned incl = s4;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const unsigned v = __shfl_up_sync(kFull, incl, o);
+                        if (lane >= o) incl += v;
+                    }
+                    const unsigned ex = incl - s4 + carry;
+                    uint2 out;
+                    out.x = (ex + s1) | ((ex + s2) << 16);
+                    out.y = (ex + s3) | ((ex + s4) << 16);
+                    *(uint2 *)(hrow + base + 4 * lane) = out;
+                    carry += __shfl_sync(kFull, incl, 31);
+                }
+            }
+            __syncthreads();
+            if (warp >= cv_warp0) {
+                float c = 0.0f;
+                bool served = false;
+                if (ct < cols) {
+                    const uint16_t code = codes[(r + P) * RW + ct + P];
+                    if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
+                        const int rk = rank[code];
+                        if (rk >= lo && rk < hi) {
+                            served = true;
+                            const uint32_t nb = nbr[code];
+                            const int base = rk - b0 - 4;
+                            auto count = [&](int k) -> unsigned {  // window count of chunk rank k
+                                const uint16_t *row = prefix + k * CS;
+                                return (unsigned)row[ct + 2 * P] - (ct > 0 ? (unsigned)row[ct - 1] : 0u);
+                            };
+                            const int value = code + bd.band_base + kDiffs;
+                            const unsigned p0 = count(rk - b0);
+#pragma unroll
+                            for (int d = 0; d < kDiffs; d++) {
+                                if (value <= bd.tvi[d] && value + d + 1 > bd.vlt) {
+                                    const unsigned o1 = (nb >> (4 * (4 + d))) & 15u, o2 = (nb >> (4 * (3 - d))) & 15u;
+                                    const unsigned p1 = o1 != 15u ? count(base + (int)o1) : 0u;
+                                    const unsigned p2 = o2 != 15u ? count(base + (int)o2) : 0u;
+                                    const unsigned pm = p1 > p2 ? p1 : p2;
+                                    const float val = __fmul_rn(__uint2float_rn((unsigned)bd.weight[d] * p0 * pm), __ldg(b.lut + p0 + pm));
+                                    if (val > c) c = val;
+                                }
+                            }
+                        }
+                    }
+                }
+                const bool pos = c > 0.0f;
+                const unsigned m = __ballot_sync(kFull, pos);
+                if (m) {
+                    unsigned at = 0;
+                    if (lane == __ffs(m) - 1) at = atomicAdd(&list_n, (unsigned)__popc(m));
+                    at = __shfl_sync(kFull, at, __ffs(m) - 1);
+                    if (pos) blist[at + __popc(m & ((1u << lane) - 1u))] = c;
+                }
+                if (served && J.plane) J.plane[(size_t)(y0 + r) * w + x0 + ct] = c;
+                if (pos) {
+                    my_sum += __float2ull_rn(__fmul_rn(c, 16777216.0f));
+                    my_cnt++;
+                }
+            }
+            __syncthreads();
+        }
+        if (hi == R) break;
+        b0 = hi - kDiffs;
+        __syncthreads();
+    }
+
+    // block totals, and this block's positive c-values appended to the scale's list
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        my_sum += __shfl_down_sync(kFull, my_sum, o);
+        my_cnt += __shfl_down_sync(kFull, my_cnt, o);
+    }
+    if (lane == 0) {
+        red_sum[warp] = my_sum;
+        red_cnt[warp] = my_cnt;
+    }
+    __syncthreads();
+    CvSlot &S = b.slots[J.slot];
+    if (tid == 0) {
+        unsigned long long s = 0;
+        unsigned c = 0;
+        for (int k = 0; k < kCvThreads / 32; k++) {
+            s += red_sum[k];
+            c += red_cnt[k];
+        }
+        list_base = 0;
+        if (c) {
+            atomicAdd(&S.sum_fx, s);
+            atomicAdd(&S.count, (unsigned long long)c);
+            list_base = atomicAdd(&S.list_n, (unsigned long long)list_n);
+        }
+    }
+    __syncthreads();
+    const unsigned ln = list_n;
+    for (unsigned i = tid; i < ln; i += kCvThreads) S.list[list_base + i] = blist[i];
+}
+
+}  // namespace
+
+size_t cvalues_smem_bytes(int max_pad) { return cv_layout(max_pad).total; }
+
+cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s)
+{
+    if (b.total_tiles <= 0) return cudaSuccess;
+    const size_t smem = cvalues_smem_bytes(b.max_pad);
+    cudaError_t e = cudaFuncSetAttribute(cvalues_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    LaunchTimer t("cambi_cvalues", s);
+    cvalues_kernel<<<b.total_tiles, kCvThreads, smem, s>>>(b);
+    return after_launch();
+}
+
+const void *kernel_entry_cvalues() { return (const void *)cvalues_kernel; }
+
+}  // namespace es

@@ -129,6 +129,10 @@ unsigned long long topk_count(unsigned long long n, double topk);
 
 }  // namespace es
 
+// Makes `stream` wait until the work of the instance's last launch is done (used by es_frame so that one event on
+// the caller's stream marks the end of a whole frame step).
+void cambi_join(es_cambi *c, cudaStream_t stream);
+
 struct es_module {
     int device = 0;
 };

@@ -10,6 +10,24 @@
 
 namespace es {
 
+// Every launcher below ends with after_launch(): it counts the launch (es_launch_count) and returns its error.
+void count_launch();
+inline cudaError_t after_launch()
+{
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Brackets a launcher's kernel launch with CUDA events on its stream while kernel timing is switched on
+// (es_kernel_timing); a no-op otherwise.
+struct LaunchTimer {
+    int slot = -1;
+    cudaStream_t stream;
+    LaunchTimer(const char *name, cudaStream_t s);
+    ~LaunchTimer();
+    LaunchTimer(const LaunchTimer &) = delete;
+};
+
 constexpr int kScales = 5;
 constexpr int kDiffs = 4;
 constexpr uint16_t kNone = 0xFFFF;

@@ -25,6 +25,7 @@ constexpr int kRing = 14, kEncRing = 7, kRadius = 6, kStats = 8, kPersist = 5, k
 struct es_frame {
     int w = 0, h = 0, pd = 10, nenc = 0, ww = 0, wh = 0, windows = 0;
     size_t n = 0;
+    size_t slot = 0;  // elements between ring slots: n rounded up to 128, so every plane starts 256-byte aligned
     DeviceBuffer<uint16_t> src_ring, src_u, src_v;
     std::vector<std::unique_ptr<DeviceBuffer<uint16_t>>> enc_ring, enc_u, enc_v;
     DeviceBuffer<uint16_t> run_e[2], run_o[2];
@@ -50,8 +51,8 @@ struct es_frame {
             for (es_cambi *c : enc_cambi[i]) es_cambi_destroy(c);
         }
     }
-    uint16_t *src_plane(long f) const { return src_ring.ptr + (size_t)(f % kRing) * n; }
-    uint16_t *enc_plane(int e, long f) const { return enc_ring[e]->ptr + (size_t)(f % kEncRing) * n; }
+    uint16_t *src_plane(long f) const { return src_ring.ptr + (size_t)(f % kRing) * slot; }
+    uint16_t *enc_plane(int e, long f) const { return enc_ring[e]->ptr + (size_t)(f % kEncRing) * slot; }
 };
 
 namespace {
@@ -200,6 +201,9 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
         cuda_check(cudaMemcpyAsync(fr->h_figs[at].ptr, fr->figs[at].ptr, fr->figs[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
         cuda_check(cudaMemcpyAsync(fr->h_bins[at].ptr, fr->bins[at].ptr, fr->bins[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
     }
+    // the frame is done when the CAMBI streams are too
+    if (source_cambi) cambi_join(fr->src_cambi[at], s);
+    for (int e = 0; e < fr->nenc; e++) cambi_join(fr->enc_cambi[at][e], s);
     cuda_check(cudaEventRecord(fr->done[at].e, s), "event");
     fr->queued[at] = f;
 }
@@ -232,15 +236,16 @@ int es_frame_create(const es_module *m, int w, int h, int pd, int n_encodes, es_
         fr->pd = pd;
         fr->nenc = n_encodes;
         fr->n = (size_t)w * h;
+        fr->slot = (fr->n + 127) & ~(size_t)127;
         fr->ww = w / kWin;
         fr->wh = h / kWin;
         fr->windows = fr->ww * fr->wh;
         const size_t n = fr->n, cn = n / 4, win = (size_t)fr->windows;
-        fr->src_ring.reset(n * kRing);
+        fr->src_ring.reset(fr->slot * kRing);
         fr->src_u.reset(cn);
         fr->src_v.reset(cn);
         for (int e = 0; e < n_encodes; e++) {
-            fr->enc_ring.push_back(std::make_unique<DeviceBuffer<uint16_t>>(n * kEncRing));
+            fr->enc_ring.push_back(std::make_unique<DeviceBuffer<uint16_t>>(fr->slot * kEncRing));
             fr->enc_u.push_back(std::make_unique<DeviceBuffer<uint16_t>>(cn));
             fr->enc_v.push_back(std::make_unique<DeviceBuffer<uint16_t>>(cn));
         }

@@ -48,18 +48,18 @@ __global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ Unp
 
 // ---------------------------------------------------------------------------------------------------------------
 // Box sums over a 64 x 32 tile with a 4-pixel margin, edge pixels repeated (src/kernels.cu:346-428 and
-// reference/encode_score/compare.py:77-108). A block of 256 threads: warp w owns window (w % 4, w / 4) of the tile,
-// lane l its column l % 16 and rows (l / 16) * 8 .. + 8.
+// reference/encode_score/compare.py:77-108). The horizontal 3- and 9-sums of the region are built in shared memory
+// (the 9-sum from three 3-sums); the vertical sums are running sums in registers. A block of 256 threads: warp w owns
+// window (w % 4, w / 4) of the tile, lane l its column l % 16 and rows (l / 16) * 8 .. + 8.
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kTW = 64, kTH = 32, kM = 4;
 constexpr int kRW = kTW + 2 * kM, kRH = kTH + 2 * kM;  // 72 x 40
+constexpr int kH3 = kTW + 6;                           // 3-sums centred at x0-3 .. x0+66
 
 struct BoxSmem {
-    uint16_t y[kRH][kRW];          // values on the 10-bit scale (or running sums)
-    uint16_t h3[kRH][kTW + 2];     // horizontal 3-sums at x0-1 .. x0+64
-    uint16_t h9[kRH][kTW];         // horizontal 9-sums at x0 .. x0+63
-    uint16_t s3[kTH + 2][kTW + 2]; // 3x3 sums at y0-1 .. y0+32, x0-1 .. x0+64
-    int32_t s9[kTH][kTW];          // 9x9 sums
+    uint16_t y[kRH][kRW];   // values on the 10-bit scale (or running sums of them)
+    uint16_t h3[kRH][kH3];  // h3[r][j]: 3-sum centred at x0 - 3 + j
+    uint16_t h9[kRH][kTW];  // h9[r][c]: 9-sum centred at x0 + c
 };
 
 // Loads a plane's region (clamped coordinates), shifted left by `up`; a null plane reads 0.
@@ -72,32 +72,45 @@ __device__ __forceinline__ void load_region(uint16_t (*dst)[kRW], const uint16_t
     }
 }
 
-// h3, h9, s3, s9 of the region in sm.y; the caller synchronises before and after.
-__device__ __forceinline__ void box_sums(BoxSmem &sm, bool need_s3_margin)
+// h3 and h9 of the region in sm.y; the caller synchronises before and after.
+__device__ __forceinline__ void horizontal_sums(BoxSmem &sm)
 {
-    for (int i = threadIdx.x; i < kRH * (kTW + 2); i += 256) {
-        const int r = i / (kTW + 2), c = i - r * (kTW + 2);
-        sm.h3[r][c] = (uint16_t)(sm.y[r][c + 2] + sm.y[r][c + 3] + sm.y[r][c + 4]);
-    }
-    for (int i = threadIdx.x; i < kRH * kTW; i += 256) {
-        const int r = i / kTW, c = i - r * kTW;
-        unsigned s = 0;
-#pragma unroll
-        for (int k = 0; k < 9; k++) s += sm.y[r][c + k];
-        sm.h9[r][c] = (uint16_t)s;
+    for (int i = threadIdx.x; i < kRH * kH3; i += 256) {
+        const int r = i / kH3, j = i - r * kH3;
+        sm.h3[r][j] = (uint16_t)(sm.y[r][j] + sm.y[r][j + 1] + sm.y[r][j + 2]);
     }
     __syncthreads();
-    const int r0 = need_s3_margin ? 0 : 1, r1 = need_s3_margin ? kTH + 2 : kTH + 1;
-    for (int i = threadIdx.x; i < (r1 - r0) * (kTW + 2); i += 256) {
-        const int r = r0 + i / (kTW + 2), c = i % (kTW + 2);
-        sm.s3[r][c] = (uint16_t)(sm.h3[r + 2][c] + sm.h3[r + 3][c] + sm.h3[r + 4][c]);
+    for (int i = threadIdx.x; i < kRH * kTW; i += 256) {
+        const int r = i >> 6, c = i & (kTW - 1);
+        sm.h9[r][c] = (uint16_t)(sm.h3[r][c] + sm.h3[r][c + 3] + sm.h3[r][c + 6]);
     }
-    for (int i = threadIdx.x; i < kTH * kTW; i += 256) {
-        const int r = i / kTW, c = i - r * kTW;
-        int s = 0;
+}
+
+// 3x3 sums at tile column c (+ dc) for the N tile rows r_first .. r_first + N - 1.
+template <int N>
+__device__ __forceinline__ void column_s3(const BoxSmem &sm, int c, int dc, int r_first, int (&out)[N])
+{
+    int v[N + 2];
 #pragma unroll
-        for (int k = 0; k < 9; k++) s += sm.h9[r + k][c];
-        sm.s9[r][c] = s;
+    for (int i = 0; i < N + 2; i++) v[i] = sm.h3[r_first + kM - 1 + i][c + 3 + dc];
+#pragma unroll
+    for (int i = 0; i < N; i++) out[i] = v[i] + v[i + 1] + v[i + 2];
+}
+
+// 9x9 sums at tile column c for the 8 tile rows r0 .. r0 + 7 (a running sum down the column).
+__device__ __forceinline__ void column_s9(const BoxSmem &sm, int c, int r0, int (&out)[8])
+{
+    int v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = sm.h9[r0 + i][c];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) s += v[i];
+    out[0] = s;
+#pragma unroll
+    for (int i = 1; i < 8; i++) {
+        s += v[i + 8] - v[i - 1];
+        out[i] = s;
     }
 }
 
@@ -132,6 +145,7 @@ __global__ void __launch_bounds__(256) window_stats_kernel(const __grid_constant
     const bool inside = wx < ww && wy < wh;
     const int c = (warp & 3) * kWin + (lane & 15), r0 = (warp >> 2) * kWin + (lane >> 4) * 8;  // tile coordinates
     const int x = x0 + c;
+    const bool gx_on = x > 0 && x < w - 1;
     int fr[8], mr[8];
     long long src_f = 0, src_m = 0, src_jxx = 0, src_jyy = 0, src_jxy = 0;
     for (int p = 0; p <= J.nenc; p++) {
@@ -139,17 +153,21 @@ __global__ void __launch_bounds__(256) window_stats_kernel(const __grid_constant
         __syncthreads();
         load_region(sm.y, plane, w, h, J.up, x0, y0);
         __syncthreads();
-        box_sums(sm, true);
+        horizontal_sums(sm);
         __syncthreads();
+        int s3[10], s3l[8], s3r[8], s9[8];
+        column_s3<10>(sm, c, 0, r0 - 1, s3);
+        column_s3<8>(sm, c, -1, r0, s3l);
+        column_s3<8>(sm, c, 1, r0, s3r);
+        column_s9(sm, c, r0, s9);
         int fine_sq = 0, jxx = 0, jyy = 0, jxy = 0, fine_x = 0;
         long long mid_sq = 0, mid_x = 0;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            const int r = r0 + i, y = y0 + r;
-            const int s3 = sm.s3[r + 1][c + 1], s9 = sm.s9[r][c];
-            const int f = 9 * (int)sm.y[r + kM][c + kM] - s3, m = 9 * s3 - s9;
-            const int gx = (x > 0 && x < w - 1) ? (int)sm.s3[r + 1][c + 2] - (int)sm.s3[r + 1][c] : 0;
-            const int gy = (y > 0 && y < h - 1) ? (int)sm.s3[r + 2][c + 1] - (int)sm.s3[r][c + 1] : 0;
+            const int y = y0 + r0 + i;
+            const int f = 9 * (int)sm.y[r0 + i + kM][c + kM] - s3[i + 1], m = 9 * s3[i + 1] - s9[i];
+            const int gx = gx_on ? s3r[i] - s3l[i] : 0;
+            const int gy = (y > 0 && y < h - 1) ? s3[i + 2] - s3[i] : 0;
             if (p == 0) {
                 fr[i] = f;
                 mr[i] = m;
@@ -187,13 +205,14 @@ __global__ void __launch_bounds__(256) window_stats_kernel(const __grid_constant
 // ---------------------------------------------------------------------------------------------------------------
 // Lasting texture: src/kernels.cu:435-451, exact, from running luma sums (see PersistJob).
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ void mids_of(BoxSmem &sm, int c, int r0, int *mid)
+// mid detail x 81 (9 S3 - S9) of the region in sm.y at the thread's 8 pixels
+__device__ __forceinline__ void mids_of(BoxSmem &sm, int c, int r0, int (&mid)[8])
 {
+    int s3[8], s9[8];
+    column_s3<8>(sm, c, 0, r0, s3);
+    column_s9(sm, c, r0, s9);
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const int r = r0 + i;
-        mid[i] = 9 * (int)sm.s3[r + 1][c + 1] - sm.s9[r][c];
-    }
+    for (int i = 0; i < 8; i++) mid[i] = 9 * s3[i] - s9[i];
 }
 
 __global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ PersistJob J)
@@ -211,7 +230,7 @@ __global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ Pe
         const size_t k = (size_t)y * w + x;
         const int ym13 = J.y_m13 ? (int)(J.y_m13[k] << J.up) : 0, ym7 = J.y_m7 ? (int)(J.y_m7[k] << J.up) : 0;
         const int yc = J.y_c ? (int)(J.y_c[k] << J.up) : 0, yf = J.y_f ? (int)(J.y_f[k] << J.up) : 0;
-        const int e = (int)J.o_old[k] - yc + yf;   // E(c) = O(c-1) - y(c) + y(c+6)
+        const int e = (int)J.o_old[k] - yc + yf;     // E(c) = O(c-1) - y(c) + y(c+6)
         const int o = (int)J.e_old[k] - ym13 + ym7;  // O(c) = E(c-1) - y(c-7) + y(c-1)
         sm.y[r][cc] = (uint16_t)e;
         o_reg[r][cc] = (uint16_t)o;
@@ -227,13 +246,13 @@ __global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ Pe
     const int c = (warp & 3) * kWin + (lane & 15), r0 = (warp >> 2) * kWin + (lane >> 4) * 8;
     int a[8], bb[8], t[8];
     __syncthreads();
-    box_sums(sm, false);
+    horizontal_sums(sm);
     __syncthreads();
     mids_of(sm, c, r0, a);  // A x 486 = mid x 81 of E
     __syncthreads();
     for (int i = threadIdx.x; i < kRH * kRW; i += 256) sm.y[i / kRW][i % kRW] = o_reg[i / kRW][i % kRW];
     __syncthreads();
-    box_sums(sm, false);
+    horizontal_sums(sm);
     __syncthreads();
     mids_of(sm, c, r0, bb);  // B x 486
     long long sab = 0, saa = 0, sbb = 0;
@@ -253,7 +272,7 @@ __global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ Pe
         __syncthreads();
         load_region(sm.y, plane, w, h, J.up, x0, y0);
         __syncthreads();
-        box_sums(sm, false);
+        horizontal_sums(sm);
         __syncthreads();
         int m[8];
         mids_of(sm, c, r0, m);
@@ -288,24 +307,54 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
     const size_t n = (size_t)J.w * J.h, cn = n / 4;
     const size_t stride = (size_t)gridDim.x * 256, i0 = (size_t)blockIdx.x * 256 + threadIdx.x;
     unsigned long long sy = 0, su = 0, sv = 0, cu = 0, cv = 0, cs = 0;
+    // 8 samples per 16-byte load (the planes are allocated aligned); the remainder one at a time
+    auto sq = [](unsigned a, unsigned b) -> unsigned {  // squared differences of two pairs of 16-bit samples
+        const int d0 = (int)(a & 0xFFFFu) - (int)(b & 0xFFFFu), d1 = (int)(a >> 16) - (int)(b >> 16);
+        return (unsigned)(d0 * d0 + d1 * d1);
+    };
     if (!src_only) {
         const uint16_t *a = J.ry, *b = J.dy[p];
-        for (size_t i = i0; i < n; i += stride) {
+        const size_t nv = (((uintptr_t)a | (uintptr_t)b) & 15) ? 0 : n / 8;
+        for (size_t i = i0; i < nv; i += stride) {
+            const uint4 x = __ldg((const uint4 *)a + i), y = __ldg((const uint4 *)b + i);
+            sy += sq(x.x, y.x) + sq(x.y, y.y) + sq(x.z, y.z) + sq(x.w, y.w);
+        }
+        for (size_t i = nv * 8 + i0; i < n; i += stride) {
             const long long d = (long long)a[i] - (long long)b[i];
             sy += (unsigned long long)(d * d);
         }
     }
     const uint16_t *u = src_only ? J.ru : J.du[p], *v = src_only ? J.rv : J.dv[p];
-    for (size_t i = i0; i < cn; i += stride) {
+    auto color = [&](unsigned uu, unsigned vv) {
+        uu <<= J.up;
+        vv <<= J.up;
+        const int eu = (int)uu - 512, ev = (int)vv - 512;
+        cu += uu;
+        cv += vv;
+        cs += (unsigned long long)__double2ll_rn(__dmul_rn(__dsqrt_rn((double)(eu * eu + ev * ev)), 1073741824.0));
+    };
+    const size_t cnv = (((uintptr_t)u | (uintptr_t)v | (uintptr_t)J.ru | (uintptr_t)J.rv) & 15) ? 0 : cn / 8;
+    for (size_t i = i0; i < cnv; i += stride) {
+        const uint4 uq = __ldg((const uint4 *)u + i), vq = __ldg((const uint4 *)v + i);
+        if (!src_only) {
+            const uint4 ru = __ldg((const uint4 *)J.ru + i), rv = __ldg((const uint4 *)J.rv + i);
+            su += sq(ru.x, uq.x) + sq(ru.y, uq.y) + sq(ru.z, uq.z) + sq(ru.w, uq.w);
+            sv += sq(rv.x, vq.x) + sq(rv.y, vq.y) + sq(rv.z, vq.z) + sq(rv.w, vq.w);
+        }
+        const unsigned us[4] = {uq.x, uq.y, uq.z, uq.w}, vs[4] = {vq.x, vq.y, vq.z, vq.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            color(us[k] & 0xFFFFu, vs[k] & 0xFFFFu);
+            color(us[k] >> 16, vs[k] >> 16);
+        }
+    }
+    for (size_t i = cnv * 8 + i0; i < cn; i += stride) {
         if (!src_only) {
             const long long du = (long long)J.ru[i] - (long long)u[i], dv = (long long)J.rv[i] - (long long)v[i];
             su += (unsigned long long)(du * du);
             sv += (unsigned long long)(dv * dv);
         }
-        const int uu = u[i] << J.up, vv = v[i] << J.up, eu = uu - 512, ev = vv - 512;
-        cu += (unsigned long long)uu;
-        cv += (unsigned long long)vv;
-        cs += (unsigned long long)__double2ll_rn(__dmul_rn(__dsqrt_rn((double)(eu * eu + ev * ev)), 1073741824.0));
+        color(u[i], v[i]);
     }
     sy = warp_sum(sy); su = warp_sum(su); sv = warp_sum(sv);
     cu = warp_sum(cu); cv = warp_sum(cv); cs = warp_sum(cs);
@@ -326,7 +375,7 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
 // src/stats.hpp:14-19. One block of 1024 threads per encode; each block finds the structure threshold itself (an
 // exact order statistic by a 3-round radix select of the source's oriented figures), so no block waits for another.
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int kCT = 1024;
+constexpr int kCT = 512;
 
 __device__ __forceinline__ uint16_t hist_bin(double pct)
 {
@@ -350,10 +399,28 @@ __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, un
             if ((bits & mask) == prefix) atomicAdd(&hist[(bits >> shift) & (unsigned)(nb - 1)], 1u);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned below = 0, rem = s_rem;
-            int d = 0;
-            for (; d < nb - 1 && below + hist[d] <= rem; d++) below += hist[d];
+        // the digit holding the rem-th smallest: thread t sums digits [t per, t per + per), a block scan places it
+        const int per = nb / kCT, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+        unsigned local = 0;
+        for (int k = 0; k < per; k++) local += hist[t * per + k];
+        unsigned incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v2 = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v2;
+        }
+        __shared__ unsigned warp_tot[kCT / 32];
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        unsigned before = 0;
+        for (int k = 0; k < warp; k++) before += warp_tot[k];
+        incl += before;
+        const unsigned rem = s_rem, excl = incl - local;
+        __syncthreads();
+        if (excl <= rem && rem < incl) {
+            unsigned below = excl;
+            int d = t * per;
+            while (below + hist[d] <= rem) below += hist[d++];
             s_rem = rem - below;
             s_prefix = prefix | ((unsigned)d << shift);
             s_mask = mask | ((unsigned)(nb - 1) << shift);
@@ -477,8 +544,9 @@ __global__ void __launch_bounds__(kCT) collect_kernel(const __grid_constant__ Co
 cudaError_t launch_unpack(const UnpackBatch &b, cudaStream_t s)
 {
     if (b.total_blocks <= 0) return cudaSuccess;
+    LaunchTimer t("frame_unpack", s);
     unpack_kernel<<<b.total_blocks, 256, 0, s>>>(b);
-    return cudaGetLastError();
+    return after_launch();
 }
 
 cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s)
@@ -486,28 +554,32 @@ cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s)
     const int ww = j.w / kWin, wh = j.h / kWin;
     if (ww <= 0 || wh <= 0 || j.nenc <= 0) return cudaSuccess;
     const int blocks = ((ww + 3) / 4) * ((wh + 1) / 2);
+    LaunchTimer t("window_stats", s);
     window_stats_kernel<<<blocks, 256, 0, s>>>(j);
-    return cudaGetLastError();
+    return after_launch();
 }
 
 cudaError_t launch_persist(const PersistJob &j, cudaStream_t s)
 {
     const int blocks = ((j.w + kTW - 1) / kTW) * ((j.h + kTH - 1) / kTH);
+    LaunchTimer t("persist_stats", s);
     persist_kernel<<<blocks, 256, 0, s>>>(j);
-    return cudaGetLastError();
+    return after_launch();
 }
 
 cudaError_t launch_pair_sums(const PairSumsJob &j, cudaStream_t s)
 {
+    LaunchTimer t("pair_sums", s);
     pair_sums_kernel<<<dim3(148, j.nenc + 1), 256, 0, s>>>(j);
-    return cudaGetLastError();
+    return after_launch();
 }
 
 cudaError_t launch_collect(const CollectJob &j, cudaStream_t s)
 {
     if (j.nenc <= 0 || j.windows <= 0) return cudaSuccess;
+    LaunchTimer t("frame_collect", s);
     collect_kernel<<<j.nenc, kCT, 0, s>>>(j);
-    return cudaGetLastError();
+    return after_launch();
 }
 
 const void *kernel_entry_unpack() { return (const void *)unpack_kernel; }

@@ -2,9 +2,13 @@
 // parameters (src/cambi.cpp:21-53) with the luminance model restated from its published definitions.
 #include <cuda.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <vector>
 
 #include "es_internal.h"
 
@@ -12,6 +16,57 @@ namespace es {
 
 namespace {
 thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ---- kernel timing (diagnostics) -------------------------------------------------------------------------------------
+namespace {
+struct Timing {
+    std::mutex m;
+    std::atomic<bool> on{false};
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> free_pairs;
+    std::map<std::string, std::pair<double, uint64_t>> totals;
+};
+Timing &timing()
+{
+    static Timing *t = new Timing;  // never destroyed: launches may outlive static destruction
+    return *t;
+}
+}  // namespace
+
+LaunchTimer::LaunchTimer(const char *name, cudaStream_t s) : stream(s)
+{
+    Timing &t = timing();
+    if (!t.on.load(std::memory_order_relaxed)) return;
+    std::lock_guard<std::mutex> lock(t.m);
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    if (!t.free_pairs.empty()) {
+        ev = t.free_pairs.back();
+        t.free_pairs.pop_back();
+    } else if (cudaEventCreate(&ev.first) != cudaSuccess || cudaEventCreate(&ev.second) != cudaSuccess) {
+        return;
+    }
+    if (cudaEventRecord(ev.first, s) != cudaSuccess) {
+        t.free_pairs.push_back(ev);
+        return;
+    }
+    slot = (int)t.pending.size();
+    t.pending.push_back({name, ev.first, ev.second});
+}
+
+LaunchTimer::~LaunchTimer()
+{
+    if (slot < 0) return;
+    Timing &t = timing();
+    std::lock_guard<std::mutex> lock(t.m);
+    if (slot < (int)t.pending.size()) cudaEventRecord(t.pending[slot].b, stream);
 }
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
@@ -148,6 +203,51 @@ extern "C" {
 const char *es_last_error(void) { return g_last_error.c_str(); }
 
 int es_version(void) { return 10000; }
+
+uint64_t es_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int es_kernel_timing(int on)
+{
+    return guarded([&] {
+        Timing &t = timing();
+        std::lock_guard<std::mutex> lock(t.m);
+        t.on = on != 0;
+        if (on) t.totals.clear();
+    });
+}
+
+int es_kernel_times(char *names, double *total_ms, uint64_t *launches, int max, int *count)
+{
+    return guarded([&] {
+        require(count != nullptr, "es_kernel_times: count is NULL");
+        cuda_check(cudaDeviceSynchronize(), "waiting for timed kernels");
+        Timing &t = timing();
+        std::lock_guard<std::mutex> lock(t.m);
+        for (const Timing::Pending &p : t.pending) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+                auto &e = t.totals[p.name];
+                e.first += ms;
+                e.second++;
+            }
+            t.free_pairs.push_back({p.a, p.b});
+        }
+        t.pending.clear();
+        int i = 0;
+        for (const auto &kv : t.totals) {
+            if (i < max) {
+                if (names) {
+                    std::memset(names + (size_t)i * 32, 0, 32);
+                    std::strncpy(names + (size_t)i * 32, kv.first.c_str(), 31);
+                }
+                if (total_ms) total_ms[i] = kv.second.first;
+                if (launches) launches[i] = kv.second.second;
+            }
+            i++;
+        }
+        *count = i;
+    });
+}
 
 int es_module_load(es_module **out)
 {

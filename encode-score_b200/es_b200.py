@@ -21,7 +21,7 @@ SCALES = 5
 
 # every symbol include/es_b200.h declares, for the load check
 SYMBOLS = (
-    "es_last_error", "es_version", "es_module_load", "es_module_unload", "es_module_get", "es_module_launch",
+    "es_last_error", "es_version", "es_launch_count", "es_kernel_timing", "es_kernel_times", "es_module_load", "es_module_unload", "es_module_get", "es_module_launch",
     "es_cambi_create", "es_cambi_create_with", "es_cambi_derive_params", "es_cambi_get_params", "es_cambi_launch",
     "es_cambi_finish", "es_cambi_destroy", "es_cambi_scale_stats", "es_cambi_read_scale", "es_cambi_set_cvalue_planes",
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
@@ -90,6 +90,9 @@ def lib() -> ctypes.CDLL:
         L = ctypes.CDLL(LIB_PATH)
         P, I, U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
         L.es_last_error.restype = ctypes.c_char_p
+        L.es_launch_count.restype = U64
+        L.es_kernel_timing.argtypes = [I]
+        L.es_kernel_times.argtypes = [P, P, P, I, ctypes.POINTER(I)]
         L.es_module_load.argtypes = [ctypes.POINTER(P)]
         L.es_module_unload.argtypes = [P]
         L.es_module_get.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(P)]
@@ -128,6 +131,30 @@ def lib() -> ctypes.CDLL:
 def check(status: int) -> None:
     if status != ES_OK:
         raise EsError(status, lib().es_last_error().decode(errors="replace"))
+
+
+def launch_count() -> int:
+    return int(lib().es_launch_count())
+
+
+def kernel_timing(on: bool) -> None:
+    check(lib().es_kernel_timing(int(on)))
+
+
+def kernel_times() -> dict:
+    """{kernel name: (total ms, launches)} of the launches timed since kernel_timing(True)."""
+    n = ctypes.c_int()
+    check(lib().es_kernel_times(None, None, None, 0, ctypes.byref(n)))
+    m = n.value
+    names = ctypes.create_string_buffer(32 * max(m, 1))
+    ms = (ctypes.c_double * max(m, 1))()
+    cnt = (ctypes.c_uint64 * max(m, 1))()
+    check(lib().es_kernel_times(names, ms, cnt, m, ctypes.byref(n)))
+    out = {}
+    for i in range(min(m, n.value)):
+        name = names.raw[32 * i:32 * i + 32].split(b"\0", 1)[0].decode()
+        out[name] = (ms[i], int(cnt[i]))
+    return out
 
 
 def derive_params(w: int, h: int) -> CambiParams:

@@ -34,6 +34,16 @@ extern "C" {
 const char *es_last_error(void);
 /* Library version as MAJOR * 10000 + MINOR * 100 + PATCH. */
 int es_version(void);
+/* Diagnostics with no counterpart in the reference: the number of kernels this library has launched in this process
+ * (all threads), so a caller can check how many GPU launches a piece of work took. */
+uint64_t es_launch_count(void);
+/* Diagnostics with no counterpart in the reference: with on != 0, each later kernel launch of the library is
+ * bracketed by CUDA events on the stream it is launched on (and earlier totals are cleared); 0 stops it. */
+int es_kernel_timing(int on);
+/* Waits for the device, then writes per kernel (up to `max` kernels): its name in names[32 i .. 32 i + 31]
+ * (NUL-terminated), the summed event time in total_ms[i] and the number of timed launches in launches[i];
+ * *count receives the number of kernels timed so far. Any output pointer but count may be NULL. */
+int es_kernel_times(char *names, double *total_ms, uint64_t *launches, int max, int *count);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Kernel module. Replaces Kernels (src/gpu.hpp:15-23): load() checks the current device and the kernels' image,
