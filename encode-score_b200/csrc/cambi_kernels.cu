@@ -179,19 +179,31 @@ __global__ void __launch_bounds__(256) select_hist_kernel(CvSlot *slots, int shi
     for (int i = threadIdx.x; i < nb; i += 256) hist[i] = 0;
     __syncthreads();
     const unsigned *v = (const unsigned *)S.list;
-    const unsigned long long n = S.list_n;
-    const unsigned mask = S.mask, prefix = S.prefix, lane = threadIdx.x & 31;
-    // c-values repeat a lot, so equal digits of a warp are added once (uniform loop: every lane takes part)
-    for (unsigned long long base = blockIdx.x * 256ull; base < n; base += (unsigned long long)gridDim.x * 256ull) {
-        const unsigned long long i = base + threadIdx.x;
-        unsigned digit = 0xFFFFFFFFu;
-        if (i < n) {
-            const unsigned bits = v[i];
-            if ((bits & mask) == prefix) digit = (bits >> shift) & (unsigned)(nb - 1);
+    const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
+    const unsigned mask = S.mask, prefix = S.prefix;
+    // neighbouring c-values of the list are often equal (they come from the same tile), so each thread adds runs of
+    // equal digits at once; 4 values per 16-byte load
+    unsigned last = 0, run = 0;
+    auto add = [&](unsigned bits) {
+        if ((bits & mask) != prefix) return;
+        const unsigned d = (bits >> shift) & (unsigned)(nb - 1);
+        if (run && d == last) {
+            run++;
+            return;
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, digit);
-        if (digit != 0xFFFFFFFFu && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&hist[digit], (unsigned)__popc(peers));
+        if (run) atomicAdd(&hist[last], run);
+        last = d;
+        run = 1;
+    };
+    for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+        const uint4 q = __ldg((const uint4 *)v + i);
+        add(q.x);
+        add(q.y);
+        add(q.z);
+        add(q.w);
     }
+    for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(v[i]);
+    if (run) atomicAdd(&hist[last], run);
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += 256)
         if (hist[i]) atomicAdd(&S.hist[i], hist[i]);
@@ -234,15 +246,22 @@ __global__ void __launch_bounds__(256) sum_above_kernel(CvSlot *slots)
     CvSlot &S = slots[blockIdx.y];
     if (S.count <= S.k) return;
     const float threshold = __uint_as_float(S.prefix);
-    const unsigned long long n = S.list_n;
+    const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
     unsigned long long s = 0, c = 0;
-    for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n; i += (unsigned long long)gridDim.x * 256ull) {
-        const float v = S.list[i];
+    auto add = [&](float v) {
         if (v > threshold) {
             s += __float2ull_rn(__fmul_rn(v, 16777216.0f));
             c++;
         }
+    };
+    for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+        const float4 q = __ldg((const float4 *)S.list + i);
+        add(q.x);
+        add(q.y);
+        add(q.z);
+        add(q.w);
     }
+    for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(S.list[i]);
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         s += __shfl_down_sync(0xffffffffu, s, o);
@@ -312,7 +331,7 @@ cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width,
     if (nslots <= 0) return cudaSuccess;
     {
         LaunchTimer t("cambi_select_hist", s);
-        select_hist_kernel<<<dim3(120, nslots), 256, 0, s>>>(slots, shift, width);
+        select_hist_kernel<<<dim3(296, nslots), 256, 0, s>>>(slots, shift, width);
     }
     cudaError_t e = after_launch();
     if (e != cudaSuccess) return e;
@@ -325,7 +344,7 @@ cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s)
 {
     if (nslots <= 0) return cudaSuccess;
     LaunchTimer t("cambi_sum_above", s);
-    sum_above_kernel<<<dim3(64, nslots), 256, 0, s>>>(slots);
+    sum_above_kernel<<<dim3(296, nslots), 256, 0, s>>>(slots);
     return after_launch();
 }
 

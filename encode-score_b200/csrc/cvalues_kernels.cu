@@ -18,6 +18,7 @@ namespace es {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kCvChunk = kCvThreads / kCvTX;  // rows whose c-values are computed together
 
 __device__ __forceinline__ bool needs_cvalue(int code, const Band &bd)
 {
@@ -33,7 +34,7 @@ __host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 struct CvLayout {
-    size_t codes, rank, nbr, colcnt, prefix, list, total;
+    size_t codes, rank, nbr, colcnt, prefix, wcount, list, total;
 };
 __host__ __device__ inline CvLayout cv_layout(int pad)
 {
@@ -43,7 +44,8 @@ __host__ __device__ inline CvLayout cv_layout(int pad)
     l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
     l.colcnt = align16(l.nbr + (size_t)kMaxBand * 4);
     l.prefix = align16(l.colcnt + (size_t)kCvBins * cv_cs(pad));
-    l.list = align16(l.prefix + (size_t)kCvBins * cv_cs(pad) * 2);
+    l.wcount = align16(l.prefix + (size_t)(kCvThreads / 32) * cv_cs(pad) * 4);
+    l.list = align16(l.wcount + (size_t)kCvChunk * (kCvBins / 2) * kCvTX * 4);
     l.total = align16(l.list + (size_t)kCvTX * kCvTY * 4);
     return l;
 }
@@ -92,7 +94,8 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     uint16_t *rank = (uint16_t *)(smem + L.rank);
     uint32_t *nbr = (uint32_t *)(smem + L.nbr);
     uint8_t *colcnt = smem + L.colcnt;
-    uint16_t *prefix = (uint16_t *)(smem + L.prefix);
+    uint32_t *prefix = (uint32_t *)(smem + L.prefix);   // per-warp prefix rows
+    uint32_t *wcount = (uint32_t *)(smem + L.wcount);   // [chunk row][rank pair][column] packed window counts
     float *blist = (float *)(smem + L.list);
     if (tid < 32) occ[tid] = srv[tid] = 0;
     if (tid == 0) list_n = 0;
@@ -162,8 +165,6 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
 
     unsigned long long my_sum = 0;
     unsigned my_cnt = 0;
-    const int cv_warp0 = kCvThreads / 32 - kCvTX / 32;  // the last two warps compute c-values
-    const int ct = tid - cv_warp0 * 32;                // their pixel column in the tile
 
     for (int b0 = 0;;) {
         const int B = min(kCvBins, R - b0);
@@ -206,36 +207,41 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             }
         }
         __syncthreads();
-        for (int r = 0; r < rows; r++) {
-            if (r > 0 && tid < RW) {
-                uint8_t *col = colcnt + tid;
-                const uint16_t cl = codes[(r - 1) * RW + tid];
-                if (cl != kNone) {
-                    const int k = (int)rank[cl] - b0;
-                    if ((unsigned)k < (unsigned)B) col[k * CS]--;
-                }
-                if (r + 2 * P < RH) {
-                    const uint16_t ce = codes[(r + 2 * P) * RW + tid];
-                    if (ce != kNone) {
-                        const int k = (int)rank[ce] - b0;
-                        if ((unsigned)k < (unsigned)B) col[k * CS]++;
-                    }
+        // Rows go in chunks of kCvChunk. Per row: (a) slide the column counts down to it; (b) each warp turns every 8th
+        // pair of the ranks the row reads into a packed prefix sum over the columns (two ranks per 32-bit lane) and
+        // then into the window counts of the tile's 64 columns. Per chunk: (c) every thread computes one pixel's
+        // c-value from those counts.
+        auto slide = [&](int r) {
+            if (tid >= RW) return;
+            uint8_t *col = colcnt + tid;
+            const uint16_t cl = codes[(r - 1) * RW + tid];
+            if (cl != kNone) {
+                const int k = (int)rank[cl] - b0;
+                if ((unsigned)k < (unsigned)B) col[k * CS]--;
+            }
+            if (r + 2 * P < RH) {
+                const uint16_t ce = codes[(r + 2 * P) * RW + tid];
+                if (ce != kNone) {
+                    const int k = (int)rank[ce] - b0;
+                    if ((unsigned)k < (unsigned)B) col[k * CS]++;
                 }
             }
+        };
+        auto window_counts = [&](int r, int i) {  // row r into chunk slot i
             const uint32_t need = rowneed[r];
-            if (!need) continue;
-            __syncthreads();
-            // inclusive prefix sums over the columns of the ranks this row reads; warp w takes every 8th of them
-            for (int n = warp;; n += kCvThreads / 32) {
-                const int k = __fns(need, 0, n + 1);
-                if (k < 0 || k >= 32) break;
-                const uint8_t *col = colcnt + k * CS;
-                uint16_t *hrow = prefix + k * CS;
+            uint32_t *wpre = prefix + warp * CS;
+            const uint32_t pairs = (need | (need >> 1)) & 0x55555555u;  // bit 2p: pair p is read
+            const int npairs = __popc(pairs);
+            for (int n = warp; n < npairs; n += kCvThreads / 32) {  // warp w takes every 8th pair
+                const int p = (int)__fns(pairs, 0, n + 1) >> 1;
+                const uint8_t *ca = colcnt + (2 * p) * CS, *cb = ca + CS;
                 unsigned carry = 0;
                 for (int base = 0; base < CS; base += 128) {
-                    const uint32_t four = *(const uint32_t *)(col + base + 4 * lane);
-                    const unsigned s1 = four & 255u, s2 = s1 + ((four >> 8) & 255u), s3 = s2 + ((four >> 16) & 255u),
-                                   s4 = s3 + (four >> 24);
+                    const uint32_t fa = *(const uint32_t *)(ca + base + 4 * lane), fb = *(const uint32_t *)(cb + base + 4 * lane);
+                    const uint32_t a0 = fa & 0x00FF00FFu, c0 = fb & 0x00FF00FFu, a1 = (fa >> 8) & 0x00FF00FFu, c1 = (fb >> 8) & 0x00FF00FFu;
+                    // column 4 lane + i of rank 2p in the low 16 bits, of rank 2p + 1 in the high 16 bits
+                    const unsigned s1 = __byte_perm(a0, c0, 0x5410), s2 = s1 + __byte_perm(a1, c1, 0x5410),
+                                   s3 = s2 + __byte_perm(a0, c0, 0x7632), s4 = s3 + __byte_perm(a1, c1, 0x7632);
                     unsigned incl = s4;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
@@ -243,58 +249,76 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
                         if (lane >= o) incl += v;
                     }
                     const unsigned ex = incl - s4 + carry;
-                    uint2 out;
-                    out.x = (ex + s1) | ((ex + s2) << 16);
-                    out.y = (ex + s3) | ((ex + s4) << 16);
-                    *(uint2 *)(hrow + base + 4 * lane) = out;
+                    *(uint4 *)(wpre + base + 4 * lane) = make_uint4(ex + s1, ex + s2, ex + s3, ex + s4);
                     carry += __shfl_sync(kFull, incl, 31);
                 }
-            }
-            __syncthreads();
-            if (warp >= cv_warp0) {
-                float c = 0.0f;
-                bool served = false;
-                if (ct < cols) {
-                    const uint16_t code = codes[(r + P) * RW + ct + P];
-                    if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
-                        const int rk = rank[code];
-                        if (rk >= lo && rk < hi) {
-                            served = true;
-                            const uint32_t nb = nbr[code];
-                            const int base = rk - b0 - 4;
-                            auto count = [&](int k) -> unsigned {  // window count of chunk rank k
-                                const uint16_t *row = prefix + k * CS;
-                                return (unsigned)row[ct + 2 * P] - (ct > 0 ? (unsigned)row[ct - 1] : 0u);
-                            };
-                            const int value = code + bd.band_base + kDiffs;
-                            const unsigned p0 = count(rk - b0);
+                __syncwarp();
+                uint32_t *wrow = wcount + (i * (kCvBins / 2) + p) * kCvTX;
 #pragma unroll
-                            for (int d = 0; d < kDiffs; d++) {
-                                if (value <= bd.tvi[d] && value + d + 1 > bd.vlt) {
-                                    const unsigned o1 = (nb >> (4 * (4 + d))) & 15u, o2 = (nb >> (4 * (3 - d))) & 15u;
-                                    const unsigned p1 = o1 != 15u ? count(base + (int)o1) : 0u;
-                                    const unsigned p2 = o2 != 15u ? count(base + (int)o2) : 0u;
-                                    const unsigned pm = p1 > p2 ? p1 : p2;
-                                    const float val = __fmul_rn(__uint2float_rn((unsigned)bd.weight[d] * p0 * pm), __ldg(b.lut + p0 + pm));
-                                    if (val > c) c = val;
-                                }
+                for (int h2 = 0; h2 < 2; h2++) {
+                    const int x = lane + 32 * h2;
+                    wrow[x] = wpre[x + 2 * P] - (x > 0 ? wpre[x - 1] : 0u);
+                }
+                __syncwarp();
+            }
+        };
+        const int ci = tid >> 6, cc = tid & (kCvTX - 1);  // this thread's pixel in a chunk
+        for (int r0 = 0; r0 < rows; r0 += kCvChunk) {
+            const int n_rows = min(kCvChunk, rows - r0);
+            bool chunk_any = false;
+            for (int i = 0; i < n_rows; i++) {
+                const int r = r0 + i;
+                if (r > 0) slide(r);
+                const uint32_t need = rowneed[r];
+                if (!need) continue;
+                chunk_any = true;
+                __syncthreads();
+                window_counts(r, i);
+                __syncthreads();
+            }
+            if (!chunk_any) continue;
+            // (c) the chunk's c-values, one pixel per thread
+            float c = 0.0f;
+            bool served = false;
+            const int r = r0 + ci;
+            if (ci < n_rows && cc < cols) {
+                const uint16_t code = codes[(r + P) * RW + cc + P];
+                if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
+                    const int rk = rank[code];
+                    if (rk >= lo && rk < hi) {
+                        served = true;
+                        const uint32_t nb = nbr[code];
+                        const int base = rk - b0 - 4;
+                        const uint32_t *wc = wcount + ci * (kCvBins / 2) * kCvTX + cc;
+                        auto count = [&](int k) -> unsigned { return (wc[(k >> 1) * kCvTX] >> ((k & 1) * 16)) & 0xFFFFu; };
+                        const int value = code + bd.band_base + kDiffs;
+                        const unsigned p0 = count(rk - b0);
+#pragma unroll
+                        for (int d = 0; d < kDiffs; d++) {
+                            if (value <= bd.tvi[d] && value + d + 1 > bd.vlt) {
+                                const unsigned o1 = (nb >> (4 * (4 + d))) & 15u, o2 = (nb >> (4 * (3 - d))) & 15u;
+                                const unsigned p1 = o1 != 15u ? count(base + (int)o1) : 0u;
+                                const unsigned p2 = o2 != 15u ? count(base + (int)o2) : 0u;
+                                const unsigned pm = p1 > p2 ? p1 : p2;
+                                const float val = __fmul_rn(__uint2float_rn((unsigned)bd.weight[d] * p0 * pm), __ldg(b.lut + p0 + pm));
+                                if (val > c) c = val;
                             }
                         }
                     }
                 }
-                const bool pos = c > 0.0f;
-                const unsigned m = __ballot_sync(kFull, pos);
-                if (m) {
-                    unsigned at = 0;
-                    if (lane == __ffs(m) - 1) at = atomicAdd(&list_n, (unsigned)__popc(m));
-                    at = __shfl_sync(kFull, at, __ffs(m) - 1);
-                    if (pos) blist[at + __popc(m & ((1u << lane) - 1u))] = c;
-                }
-                if (served && J.plane) J.plane[(size_t)(y0 + r) * w + x0 + ct] = c;
-                if (pos) {
-                    my_sum += __float2ull_rn(__fmul_rn(c, 16777216.0f));
-                    my_cnt++;
-                }
+            }
+            const bool pos = c > 0.0f;
+            const unsigned m = __ballot_sync(kFull, pos);
+            if (m) {
+                unsigned at = 0;
+                if (lane == __ffs(m) - 1) at = atomicAdd(&list_n, (unsigned)__popc(m));
+                at = __shfl_sync(kFull, at, __ffs(m) - 1);
+                if (pos) blist[at + __popc(m & ((1u << lane) - 1u))] = c;
+            }
+            if (served && J.plane) J.plane[(size_t)(y0 + r) * w + x0 + cc] = c;
+            if (pos) {
+                my_sum += __float2ull_rn(__fmul_rn(c, 16777216.0f));
+                my_cnt++;
             }
             __syncthreads();
         }

@@ -194,8 +194,12 @@ struct CollectJob {
     uint8_t *mask;                      // out: structure mask of this frame
     FrameFigures *fig[kMaxEncodes];
     uint16_t *bins[kMaxEncodes];        // out: 6 arrays of `windows` bins (amount 0-2, matching 0-1, lasting)
+    float *threshold;                   // scratch: the frame's structure threshold
+    double *partials;                   // scratch: [nenc][collect_blocks(windows)][kCollectSums]
     int nenc, windows;
 };
+constexpr int kCollectSums = 20;  // 18 double sums and 2 counts per block
+int collect_blocks(int windows);
 cudaError_t launch_collect(const CollectJob &j, cudaStream_t s);
 
 }  // namespace es

@@ -34,6 +34,8 @@ struct es_frame {
     DeviceBuffer<unsigned long long> sums[2];  // sse [nenc][3], then color [nenc + 1][3]
     DeviceBuffer<FrameFigures> figs[2];
     DeviceBuffer<uint16_t> bins[2];            // [nenc][6][windows]
+    DeviceBuffer<float> threshold;             // the frame's structure threshold (scratch)
+    DeviceBuffer<double> partials;             // per-block sums of the per-frame reduction (scratch)
     PinnedBuffer<unsigned long long> h_sums[2];
     PinnedBuffer<FrameFigures> h_figs[2];
     PinnedBuffer<uint16_t> h_bins[2];
@@ -194,6 +196,8 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     cj.mask = fr->masks.ptr + (size_t)(f % kEncRing) * fr->windows;
     cj.nenc = fr->nenc;
     cj.windows = fr->windows;
+    cj.threshold = fr->threshold.ptr;
+    cj.partials = fr->partials.ptr;
     if (fr->windows > 0) cuda_check(launch_collect(cj, s), "collecting figures");
 
     cuda_check(cudaMemcpyAsync(fr->h_sums[at].ptr, fr->sums[at].ptr, fr->sums[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
@@ -271,6 +275,8 @@ int es_frame_create(const es_module *m, int w, int h, int pd, int n_encodes, es_
                 else fr->enc_cambi[i].push_back(c);
             }
         }
+        fr->threshold.reset(1);
+        fr->partials.reset(std::max<size_t>(1, (size_t)n_encodes * collect_blocks(fr->windows) * kCollectSums));
         fr->masks.reset(std::max<size_t>(1, win * kEncRing));
         cuda_check(cudaMemset(fr->masks.ptr, 0, fr->masks.bytes()), "clearing");
         cuda_check(cudaDeviceSynchronize(), "frame set-up");

@@ -372,10 +372,13 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
 
 // ---------------------------------------------------------------------------------------------------------------
 // Per-frame reduction, src/main.cpp:606-641 with quantile() of 280-289 and Histogram::add's binning of
-// src/stats.hpp:14-19. One block of 1024 threads per encode; each block finds the structure threshold itself (an
-// exact order statistic by a 3-round radix select of the source's oriented figures), so no block waits for another.
+// src/stats.hpp:14-19, in three launches: (1) the structure threshold, an exact order statistic of the source's
+// oriented figures by a 3-round radix select, and the frame's structure mask; (2) every window of every encode: its
+// bins and the block's sums, added in a fixed order; (3) per encode the blocks' sums, in a fixed order -- so the
+// figures are the same on every run.
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int kCT = 512;
+constexpr int kCT = 1024;  // threshold block
+constexpr int kCW = 256;   // windows per block
 
 __device__ __forceinline__ uint16_t hist_bin(double pct)
 {
@@ -387,6 +390,7 @@ __device__ __forceinline__ uint16_t hist_bin(double pct)
 __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, unsigned *hist)
 {
     __shared__ unsigned s_prefix, s_mask, s_rem;
+    __shared__ unsigned warp_tot[kCT / 32];
     if (threadIdx.x == 0) { s_prefix = 0; s_mask = 0; s_rem = t; }
     const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
     for (int round = 0; round < 3; round++) {
@@ -409,7 +413,6 @@ __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, un
             const unsigned v2 = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += v2;
         }
-        __shared__ unsigned warp_tot[kCT / 32];
         if (lane == 31) warp_tot[warp] = incl;
         __syncthreads();
         unsigned before = 0;
@@ -430,61 +433,51 @@ __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, un
     return s_prefix;
 }
 
-template <typename T>
-__device__ T block_sum(T v, T *scratch)
-{
-    v = warp_sum(v);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();
-    if (lane == 0) scratch[warp] = v;
-    __syncthreads();
-    T s = 0;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < kCT / 32; k++) s += scratch[k];
-    return s;  // valid in thread 0
-}
-
-__global__ void __launch_bounds__(kCT) collect_kernel(const __grid_constant__ CollectJob J)
+__global__ void __launch_bounds__(kCT) collect_threshold_kernel(const __grid_constant__ CollectJob J)
 {
     __shared__ unsigned hist[2048];
-    __shared__ double dscr[kCT / 32];
-    __shared__ unsigned uscr[kCT / 32];
-    __shared__ float s_q;
-    const int e = blockIdx.x, n = J.windows;
-    const float *st = J.stats[e];
-    // quantile(oriented of the source, 0.8) as numpy's linear interpolation of exact order statistics
-    {
-        const double pos = 0.8 * (double)(n - 1);
-        const unsigned lo = (unsigned)pos;
-        const float a = __uint_as_float(select_kth(st + 6, n, 8, lo, hist));
-        float q = a;
-        if (lo + 1 < (unsigned)n) {
-            const float b = __uint_as_float(select_kth(st + 6, n, 8, lo + 1, hist));
-            const float diff = __fsub_rn(b, a);
-            q = __double2float_rn(__dadd_rn((double)a, __dmul_rn((double)diff, __dsub_rn(pos, (double)lo))));
-        }
-        if (threadIdx.x == 0) s_q = q;
-        __syncthreads();
+    const float *st = J.stats[0];  // the source's oriented figures are the same in every encode's array
+    const int n = J.windows;
+    // numpy's linear quantile at 0.8 of exact order statistics, in the reference's float / double arithmetic
+    const double pos = 0.8 * (double)(n - 1);
+    const unsigned lo = (unsigned)pos;
+    const float a = __uint_as_float(select_kth(st + 6, n, 8, lo, hist));
+    float q = a;
+    if (lo + 1 < (unsigned)n) {
+        const float b = __uint_as_float(select_kth(st + 6, n, 8, lo + 1, hist));
+        const float diff = __fsub_rn(b, a);
+        q = __double2float_rn(__dadd_rn((double)a, __dmul_rn((double)diff, __dsub_rn(pos, (double)lo))));
     }
-    const float q = s_q;
-    const bool lasting = J.persist[e] != nullptr;
-    double all_r[3] = {0, 0, 0}, all_d[3] = {0, 0, 0}, st_r[3] = {0, 0, 0}, st_d[3] = {0, 0, 0};
-    double sh_all_x[2] = {0, 0}, sh_st_x[2] = {0, 0}, own = 0, mine = 0;
-    unsigned n_st = 0, n_last = 0;
-    uint16_t *bins = J.bins[e];
+    if (threadIdx.x == 0) *J.threshold = q;
     for (int i = threadIdx.x; i < n; i += kCT) {
-        const float *s = st + (size_t)i * 8;
+        const float o = st[(size_t)i * 8 + 6];
+        J.mask[i] = o >= q && o > 0.0f;
+    }
+}
+
+__global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_constant__ CollectJob J)
+{
+    __shared__ double part[kCW / 32][kCollectSums];
+    const int e = blockIdx.y, n = J.windows, i = blockIdx.x * kCW + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // sums: all_r[3] all_d[3] st_r[3] st_d[3] sh_all_x[2] sh_st_x[2] own mine n_structure n_lasting
+    double v[kCollectSums];
+#pragma unroll
+    for (int k = 0; k < kCollectSums; k++) v[k] = 0.0;
+    if (i < n) {
+        const float q = *J.threshold;
+        const float *s = J.stats[e] + (size_t)i * 8;
+        uint16_t *bins = J.bins[e];
         const bool m = s[6] >= q && s[6] > 0.0f;
-        if (e == 0) J.mask[i] = m;
         const double er[3] = {(double)s[0], (double)s[1], (double)s[6]}, ed[3] = {(double)s[2], (double)s[3], (double)s[7]};
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            all_r[k] += er[k];
-            all_d[k] += ed[k];
+            v[k] = er[k];
+            v[3 + k] = ed[k];
             uint16_t bin = kNone;
             if (m) {
-                st_r[k] += er[k];
-                st_d[k] += ed[k];
+                v[6 + k] = er[k];
+                v[9 + k] = ed[k];
                 bin = hist_bin(__dmul_rn(100.0, __dsqrt_rn(__ddiv_rn(ed[k], fmax(er[k], 1e-9)))));
             }
             bins[(size_t)k * n + i] = bin;
@@ -492,51 +485,59 @@ __global__ void __launch_bounds__(kCT) collect_kernel(const __grid_constant__ Co
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const double x = (double)s[4 + k];
-            sh_all_x[k] += x;
+            v[12 + k] = x;
             uint16_t bin = kNone;
             if (m) {
-                sh_st_x[k] += x;
+                v[14 + k] = x;
                 bin = hist_bin(__ddiv_rn(__dmul_rn(100.0, x), fmax(er[k], 1e-9)));
             }
             bins[(size_t)(3 + k) * n + i] = bin;
         }
-        n_st += m;
+        v[18] = m ? 1.0 : 0.0;
         uint16_t lbin = kNone;
-        if (lasting) {
+        if (J.persist[e]) {
             const float *ps = J.persist[e] + (size_t)i * 5;
             const double agree = __ddiv_rn((double)ps[2], __dsqrt_rn(fmax(__dmul_rn((double)ps[3], (double)ps[4]), 1e-9)));
             if (J.centre_mask[i] && agree > 0.5 && ps[0] > 0.0f) {
-                own += (double)ps[0];
-                mine += (double)ps[1];
+                v[16] = (double)ps[0];
+                v[17] = (double)ps[1];
+                v[19] = 1.0;
                 lbin = hist_bin(__ddiv_rn(__dmul_rn(100.0, (double)ps[1]), (double)ps[0]));
-                n_last++;
             }
         }
         bins[(size_t)5 * n + i] = lbin;
     }
+#pragma unroll
+    for (int k = 0; k < kCollectSums; k++) {
+        const double x = warp_sum(v[k]);
+        if (lane == 0) part[warp][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kCollectSums) {
+        double s = 0.0;
+        for (int k = 0; k < kCW / 32; k++) s += part[k][threadIdx.x];
+        J.partials[((size_t)e * gridDim.x + blockIdx.x) * kCollectSums + threadIdx.x] = s;
+    }
+}
+
+__global__ void collect_final_kernel(const __grid_constant__ CollectJob J, int nblocks)
+{
+    const int e = blockIdx.x, k = threadIdx.x;
+    if (k >= kCollectSums) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; b++) s += J.partials[((size_t)e * nblocks + b) * kCollectSums + k];
     FrameFigures *f = J.fig[e];
-    double r;
-#define ES_REDUCE(dst, val) r = block_sum<double>(val, dscr); if (threadIdx.x == 0) dst = r;
-    for (int k = 0; k < 3; k++) {
-        ES_REDUCE(f->all_r[k], all_r[k]);
-        ES_REDUCE(f->all_d[k], all_d[k]);
-        ES_REDUCE(f->st_r[k], st_r[k]);
-        ES_REDUCE(f->st_d[k], st_d[k]);
-    }
-    for (int k = 0; k < 2; k++) {
-        ES_REDUCE(f->sh_all_x[k], sh_all_x[k]);
-        ES_REDUCE(f->sh_st_x[k], sh_st_x[k]);
-    }
-    ES_REDUCE(f->own, own);
-    ES_REDUCE(f->mine, mine);
-#undef ES_REDUCE
-    unsigned u = block_sum<unsigned>(n_st, uscr);
-    if (threadIdx.x == 0) f->n_structure = u;
-    u = block_sum<unsigned>(n_last, uscr);
-    if (threadIdx.x == 0) {
-        f->n_lasting = u;
-        f->threshold = q;
-    }
+    if (k < 3) f->all_r[k] = s;
+    else if (k < 6) f->all_d[k - 3] = s;
+    else if (k < 9) f->st_r[k - 6] = s;
+    else if (k < 12) f->st_d[k - 9] = s;
+    else if (k < 14) f->sh_all_x[k - 12] = s;
+    else if (k < 16) f->sh_st_x[k - 14] = s;
+    else if (k == 16) f->own = s;
+    else if (k == 17) f->mine = s;
+    else if (k == 18) f->n_structure = (unsigned)s;
+    else f->n_lasting = (unsigned)s;
+    if (k == 0) f->threshold = *J.threshold;
 }
 
 }  // namespace
@@ -574,11 +575,26 @@ cudaError_t launch_pair_sums(const PairSumsJob &j, cudaStream_t s)
     return after_launch();
 }
 
+int collect_blocks(int windows) { return (windows + kCW - 1) / kCW; }
+
 cudaError_t launch_collect(const CollectJob &j, cudaStream_t s)
 {
     if (j.nenc <= 0 || j.windows <= 0) return cudaSuccess;
-    LaunchTimer t("frame_collect", s);
-    collect_kernel<<<j.nenc, kCT, 0, s>>>(j);
+    const int nb = collect_blocks(j.windows);
+    {
+        LaunchTimer t("frame_collect_threshold", s);
+        collect_threshold_kernel<<<1, kCT, 0, s>>>(j);
+    }
+    cudaError_t e = after_launch();
+    if (e != cudaSuccess) return e;
+    {
+        LaunchTimer t("frame_collect_windows", s);
+        collect_windows_kernel<<<dim3(nb, j.nenc), kCW, 0, s>>>(j);
+    }
+    e = after_launch();
+    if (e != cudaSuccess) return e;
+    LaunchTimer t("frame_collect_final", s);
+    collect_final_kernel<<<j.nenc, 32, 0, s>>>(j, nb);
     return after_launch();
 }
 
@@ -586,6 +602,6 @@ const void *kernel_entry_unpack() { return (const void *)unpack_kernel; }
 const void *kernel_entry_window_stats() { return (const void *)window_stats_kernel; }
 const void *kernel_entry_persist() { return (const void *)persist_kernel; }
 const void *kernel_entry_pair_sums() { return (const void *)pair_sums_kernel; }
-const void *kernel_entry_collect() { return (const void *)collect_kernel; }
+const void *kernel_entry_collect() { return (const void *)collect_windows_kernel; }
 
 }  // namespace es
