@@ -1,0 +1,195 @@
+// es_cambi_score_noalloc: the CAMBI score of one plane with no device allocation at all.
+//
+// Some callers must not allocate device memory when they score a picture: plugins whose host application owns the
+// device memory budget, and latency-critical paths where cudaMalloc's implicit device synchronization is not
+// acceptable. This entry point runs the same kernels as es_cambi_launch / es_cambi_finish, but every buffer they use
+// -- the five scale planes, the per-scale lists of positive c-values, the counters and the reciprocal table -- lives
+// in one file-scope device array of kScratchBytes (20 MiB), which every GPU that loads the library holds until the
+// process exits. The caller passes the input plane and a device double for the output.
+//
+// Host code cannot use the array's name as a device address (in host code it names a host-side stand-in), so the
+// first call on each device, with that device current, looks the address up with cudaGetSymbolAddress and fills the
+// reciprocal table; that first call should come before any stream capture. Every call shares the array: each call
+// clears what must start at zero, and calls whose work overlaps on the GPU race.
+#include <mutex>
+
+#include "es_internal.h"
+
+namespace es {
+namespace {
+
+constexpr size_t kScratchBytes = (size_t)20 << 20;
+constexpr int kNoAllocMaxPad = 32;                                                  // windows up to 65
+constexpr int kLutEntries = (2 * kNoAllocMaxPad + 1) * (2 * kNoAllocMaxPad + 1) + 1;  // 4226
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+constexpr size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+struct Carve {
+    size_t slots, score, lut, words[kScales], lists[kScales], end;
+    int sw[kScales], sh[kScales];
+};
+
+Carve carve(int w, int h)
+{
+    Carve c{};
+    size_t at = 0;
+    c.slots = at;
+    at = align256(at + kScales * sizeof(CvSlot));
+    c.score = at;
+    at = align256(at + (1 + kScales) * sizeof(double));
+    c.lut = at;
+    at = align256(at + kLutEntries * sizeof(float));
+    c.sw[0] = w;
+    c.sh[0] = h;
+    for (int s = 1; s < kScales; s++) {
+        c.sw[s] = (c.sw[s - 1] + 1) >> 1;
+        c.sh[s] = (c.sh[s - 1] + 1) >> 1;
+    }
+    for (int s = 0; s < kScales; s++) {
+        c.words[s] = at;
+        at = align256(at + (size_t)c.sw[s] * c.sh[s] * sizeof(uint16_t));
+    }
+    for (int s = 0; s < kScales; s++) {
+        c.lists[s] = at;
+        at = align256(at + (size_t)c.sw[s] * c.sh[s] * sizeof(float));
+    }
+    c.end = at;
+    return c;
+}
+
+// 1/i as float for i < kLutEntries (entry 0 unused), the same correctly rounded values as reciprocal_table().
+__global__ void noalloc_lut_kernel(float *lut)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kLutEntries; i += gridDim.x * blockDim.x)
+        lut[i] = i ? __double2float_rn(__ddiv_rn(1.0, (double)i)) : 0.0f;
+}
+
+struct SlotSetup {
+    float *list[kScales];
+    unsigned long long n[kScales], k[kScales];
+};
+
+// Clears the five counter slots and points them at their lists (blockIdx.x = scale).
+__global__ void noalloc_slots_kernel(CvSlot *slots, const __grid_constant__ SlotSetup st)
+{
+    CvSlot &S = slots[blockIdx.x];
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x) S.hist[i] = 0;
+    if (threadIdx.x == 0) {
+        S.sum_fx = S.count = S.list_n = 0;
+        S.n = st.n[blockIdx.x];
+        S.k = st.k[blockIdx.x];
+        S.remaining = S.k;
+        S.above_fx = S.above_n = 0;
+        S.prefix = S.mask = 0;
+        S.list = st.list[blockIdx.x];
+    }
+}
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+unsigned char *g_base[kMaxDevices] = {};
+
+// The array's device address on the current device, looked up (and the table filled) on the device's first call.
+unsigned char *scratch_on_current_device()
+{
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "finding the CUDA device");
+    require(dev >= 0 && dev < kMaxDevices, "es_cambi_score_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_base[dev]) {
+        void *p = nullptr;
+        cuda_check(cudaGetSymbolAddress(&p, g_scratch), "finding the no-allocation scratch array");
+        unsigned char *base = (unsigned char *)p;
+        noalloc_lut_kernel<<<8, 256>>>((float *)(base + carve(2, 2).lut));
+        cuda_check(cudaGetLastError(), "filling the reciprocal table");
+        cuda_check(cudaDeviceSynchronize(), "filling the reciprocal table");
+        g_base[dev] = base;
+    }
+    return g_base[dev];
+}
+
+}  // namespace
+}  // namespace es
+
+using namespace es;
+
+extern "C" int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int depth, double *score, void *stream)
+{
+    return guarded([&] {
+        require(img != 0 && score != nullptr, "es_cambi_score_noalloc: NULL plane or output");
+        require(w > 1 && h > 1, "es_cambi_score_noalloc: CAMBI needs a picture of at least 2 x 2 pixels");
+        require(depth == 8 || depth == 10, "es_cambi_score_noalloc: CAMBI takes 8- or 10-bit planes");
+        require(pitch >= w, "es_cambi_score_noalloc: pitch is smaller than the width");
+        const Carve c = carve(w, h);
+        if (c.end > kScratchBytes)
+            throw Error(ES_ERR_INVALID, "es_cambi_score_noalloc: a " + std::to_string(w) + " x " + std::to_string(h) +
+                                            " picture needs " + std::to_string(c.end) + " bytes of scratch; the fixed array holds " +
+                                            std::to_string(kScratchBytes) + " (about 1920 x 1080 at most)");
+        const es_cambi_params p = derive_params(w, h);
+        require(p.pad <= kNoAllocMaxPad, "es_cambi_score_noalloc: window wider than 65");
+        require(p.band_size > 0 && p.band_size <= kMaxBand, "es_cambi_score_noalloc: band out of range");
+        unsigned char *base = scratch_on_current_device();
+        cudaStream_t s = (cudaStream_t)stream;
+        CvSlot *slots = (CvSlot *)(base + c.slots);
+        double *rec = (double *)(base + c.score);
+
+        SlotSetup st{};
+        for (int k = 0; k < kScales; k++) {
+            st.list[k] = (float *)(base + c.lists[k]);
+            st.n[k] = (unsigned long long)c.sw[k] * c.sh[k];
+            st.k[k] = topk_count(st.n[k], p.topk);
+        }
+        noalloc_slots_kernel<<<kScales, 256, 0, s>>>(slots, st);
+        cuda_check(cudaGetLastError(), "clearing the counters");
+
+        Prep0Batch pb{};
+        pb.njobs = 1;
+        pb.job[0] = Prep0Job{(const uint16_t *)img, pitch, w, h, depth, p.mask_index, (uint16_t *)(base + c.words[0]), (w + 63) / 64, 0};
+        pb.total_tiles = pb.job[0].tiles_x * ((h + 31) / 32);
+        cuda_check(launch_prep0(pb, s), "cambi scale 0");
+        for (int k = 1; k < kScales; k++) {
+            DecBatch db{};
+            db.njobs = 1;
+            db.job[0] = DecJob{(const uint16_t *)(base + c.words[k - 1]), c.sw[k - 1], c.sh[k - 1], (uint16_t *)(base + c.words[k]),
+                               c.sw[k], c.sh[k], 0};
+            db.total_blocks = (c.sw[k] * c.sh[k] + 255) / 256;
+            cuda_check(launch_decimate_mode(db, s), "cambi scales");
+        }
+        CvBatch cb{};
+        cb.njobs = kScales;
+        int tiles = 0;
+        for (int k = 0; k < kScales; k++) {
+            CvJob &j = cb.job[k];
+            j.word = (const uint16_t *)(base + c.words[k]);
+            j.w = c.sw[k];
+            j.h = c.sh[k];
+            j.pad = p.pad;
+            j.tiles_x = (j.w + kCvTX - 1) / kCvTX;
+            j.first_tile = tiles;
+            j.slot = k;
+            j.plane = nullptr;
+            tiles += j.tiles_x * ((j.h + kCvTY - 1) / kCvTY);
+        }
+        cb.total_tiles = tiles;
+        cb.max_pad = p.pad;
+        cb.band = Band{p.band_base, p.band_size, p.vlt, {p.tvi[0], p.tvi[1], p.tvi[2], p.tvi[3]},
+                       {p.weight[0], p.weight[1], p.weight[2], p.weight[3]}};
+        cb.lut = (const float *)(base + c.lut);
+        cb.slots = slots;
+        cuda_check(launch_cvalues(cb, s), "cambi c-values");
+        static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+        for (int round = 0; round < 3; round++)
+            cuda_check(launch_select_round(slots, kScales, shifts[round], widths[round], s), "cambi top-k");
+        cuda_check(launch_sum_above(slots, kScales, s), "cambi top-k");
+        ScoreBatch sb{};
+        sb.njobs = 1;
+        sb.job[0].first_slot = 0;
+        sb.job[0].window = p.window;
+        sb.job[0].score = rec;
+        sb.slots = slots;
+        cuda_check(launch_score(sb, s), "cambi score");
+        cuda_check(cudaMemcpyAsync(score, rec, sizeof(double), cudaMemcpyDeviceToDevice, s), "writing the score");
+    });
+}

@@ -24,6 +24,7 @@ SYMBOLS = (
     "es_last_error", "es_version", "es_launch_count", "es_kernel_timing", "es_kernel_times", "es_module_load", "es_module_unload", "es_module_get", "es_module_launch",
     "es_cambi_create", "es_cambi_create_with", "es_cambi_derive_params", "es_cambi_get_params", "es_cambi_launch",
     "es_cambi_finish", "es_cambi_destroy", "es_cambi_scale_stats", "es_cambi_read_scale", "es_cambi_set_cvalue_planes",
+    "es_cambi_score_noalloc",
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
 )
@@ -107,6 +108,7 @@ def lib() -> ctypes.CDLL:
         L.es_cambi_scale_stats.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(U64), ctypes.POINTER(U64)]
         L.es_cambi_read_scale.argtypes = [P, I, P, P]
         L.es_cambi_set_cvalue_planes.argtypes = [P, ctypes.POINTER(P)]
+        L.es_cambi_score_noalloc.argtypes = [U64, I, I, I, I, P, P]
         L.es_histogram_add.argtypes = [ctypes.POINTER(Histogram), ctypes.c_double]
         L.es_histogram_quantile.argtypes = [ctypes.POINTER(Histogram), ctypes.c_double]
         L.es_histogram_quantile.restype = ctypes.c_double
@@ -230,6 +232,12 @@ class Cambi:
         if self.handle:
             lib().es_cambi_destroy(self.handle)
             self.handle = ctypes.c_void_p()
+
+
+def cambi_score_noalloc(img: int, pitch: int, w: int, h: int, depth: int, score_dev: int, stream: int = 0) -> None:
+    """es_cambi_score_noalloc: queues the CAMBI score of a device plane into the device double at `score_dev`,
+    allocating nothing (fixed internal scratch; pictures up to about 1920 x 1080)."""
+    check(lib().es_cambi_score_noalloc(img, pitch, w, h, depth, ctypes.c_void_p(score_dev), ctypes.c_void_p(stream)))
 
 
 def new_accum() -> Accum:

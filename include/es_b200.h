@@ -101,6 +101,18 @@ int es_cambi_read_scale(const es_cambi *c, int s, uint16_t *image, uint8_t *mask
  * computed c-value there (the buffer kernels.cu's cambi_cvalues fills). NULL entries switch it off per scale. */
 int es_cambi_set_cvalue_planes(es_cambi *c, float *const dev_planes[5]);
 
+/* No counterpart in the reference. The CAMBI score of one plane, like es_cambi_create + es_cambi_launch +
+ * es_cambi_finish, for callers that must not allocate device memory when they score a picture: plugins whose host
+ * application owns the device memory budget, and latency-critical paths where cudaMalloc's implicit device
+ * synchronization is not acceptable. It allocates nothing: its scratch is one fixed 20 MiB device array inside the
+ * library, which every GPU that loads the library holds until the process exits, so it takes pictures up to about
+ * 1920 x 1080 (larger ones fail with ES_ERR_INVALID and the size they would need). `img` is a device plane of w x h
+ * values at `depth` bits (8 or 10), `pitch` in pixels; the score is written to the device double `score`; all work is
+ * queued on `stream` and the call returns without waiting. The first call on each device (with that device current)
+ * looks up the array's address and fills a table, and should come before any stream capture. Every call shares the
+ * array: calls whose work overlaps on the GPU race, so serialize them (one stream, or events). */
+int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int depth, double *score, void *stream);
+
 /* ---------------------------------------------------------------------------------------------------------------
  * A decoded frame as the kernels read it: src/main.cpp:99-102 FrameView / src/kernels.cu:284-287 Frame. Planar or
  * semi-planar 4:2:0 (chroma interleaved in u when semi), `bytes` per sample (1 or 2), sample value >> shift (6 for
