@@ -117,4 +117,21 @@ def c4_step(frame: int, w: int = 3840, h: int = 2160, seed: int = 4, source: int
     return Step(_picture(src, 10), [_picture(enc, 10)])
 
 
-WORKLOADS = {"c1": c1_step, "c2": c2_step, "c4": c4_step}
+def texture_step(frame: int, w: int = 640, h: int = 360, seed: int = 7, source: int = 0) -> Step:
+    """Persistent texture for the lasting-texture measure: a static sum of 4 oriented sinusoids (periods 6-24 pixels)
+    around code 512 of a 10-bit picture plus fresh grain (sigma 6) every frame; the encode blurs it (sigma 0.9) and
+    requantises its left half to even codes."""
+    base = np.random.Generator(np.random.PCG64(seed + 1000 * source))
+    rng = np.random.Generator(np.random.PCG64(seed + 1000 * source + frame + 500))
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    tex = np.zeros((h, w), np.float32)
+    for _ in range(4):
+        a, period, phase = base.uniform(0, np.pi), base.uniform(6, 24), base.uniform(0, 2 * np.pi)
+        tex += np.sin(2 * np.pi * (xx * np.cos(a) + yy * np.sin(a)) / period + phase).astype(np.float32)
+    src = np.clip(np.rint(512 + 30 * tex + rng.normal(0, 6, (h, w))), 0, 1023)
+    enc = np.rint(ndimage.gaussian_filter(src.astype(np.float32), 0.9, mode="nearest"))
+    enc[:, : w // 2] = np.rint(enc[:, : w // 2] / 2) * 2
+    return Step(_picture(src, 10), [_picture(np.clip(enc, 0, 1023), 10)])
+
+
+WORKLOADS = {"c1": c1_step, "c2": c2_step, "c4": c4_step, "texture": texture_step}
