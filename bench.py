@@ -11,8 +11,9 @@ lasting-texture figures, PSNR and color, and the per-frame reduction into per-se
   for the CAMBI streams.
 * ``e2e``: the same through the C ABI with the inputs in pinned host memory, copied host-to-device every step on a copy
   stream (double-buffered) and the figures read back, inside the timed region.
-* ``roofline``: the kernel with the most device time in the timed region: its algorithmic bytes per launch (see
-  ALGORITHMIC_BYTES) over its mean event-timed duration, against the measured HBM copy bandwidth.
+* ``roofline``: the kernel with the most device time: its algorithmic bytes per launch (algorithmic_bytes) over its
+  mean duration, against the measured HBM copy bandwidth. Durations come from a pass over the pool after the timed
+  region with every kernel alone on the stream and bracketed by CUDA events (``kernels`` lists them all).
 * ``cpu_baseline``: the CPU oracle (plain-C restatement of the reference) on the host cores, one frame step per
   process, rank 0 at N = 1 only.
 
@@ -329,7 +330,6 @@ def main() -> None:
         clocks.start()
         time.sleep(0.25)
         launches0 = es_b200.launch_count()
-        es_b200.kernel_timing(True)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         first = f
@@ -343,14 +343,25 @@ def main() -> None:
         end.record(stream)
         end.synchronize()
         launches = es_b200.launch_count() - launches0
-        times = es_b200.kernel_times()
-        es_b200.kernel_timing(False)
         clk = clocks.stop()
     ms = start.elapsed_time(end)
     ms = max_over_ranks(ms)
     pairs = args.steps * n_enc * world
     value = pairs / (ms / 1000.0)
     assert f - first == args.steps
+
+    # ---- per-kernel leg: one pass over the pool with every kernel alone on the stream, each bracketed by events -
+    # (in the timed region the pictures' CAMBI streams overlap, so an event pair there would also time its neighbours)
+    es_b200.kernel_timing(True, serial=True)
+    with torch.cuda.stream(stream):
+        for _ in range(len(dev_pool)):
+            p = dev_pool[f % len(dev_pool)]
+            fr.queue(f, p[0][1], [x[1] for x in p[1:]], stream.cuda_stream)
+            fr.collect(f, acc, acc)
+            f += 1
+    times = es_b200.kernel_times()
+    es_b200.kernel_timing(False)
+    kernel_steps = len(dev_pool)
 
     # ---- end-to-end leg: host frames, copies inside the timed region ------------------------------------------
     e2e = None
@@ -420,7 +431,7 @@ def main() -> None:
         roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": read_traffic(top, args.workload),
                     "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "peak_source": peaks["source"]}
-    kernels = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps, "share": v[0] / total_kernel_ms}
+    kernels = {k: {"ms_per_step": v[0] / kernel_steps, "launches_per_step": v[1] / kernel_steps, "share": v[0] / total_kernel_ms}
                for k, v in sorted(times.items(), key=lambda kv: -kv[1][0])}
 
     # ---- CPU baseline (rank 0, one GPU) -------------------------------------------------------------------------

@@ -93,7 +93,7 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
     pb.total_tiles = pj.tiles_x * ((c->h + 31) / 32);
     cuda_check(launch_prep0(pb, caller), "cambi scale 0");
     cuda_check(cudaEventRecord(c->copied.e, caller), "cambi event");
-    cudaStream_t s = c->stream.s;
+    cudaStream_t s = serial_streams() ? caller : c->stream.s;
     cuda_check(cudaStreamWaitEvent(s, c->copied.e, 0), "cambi event");
     cuda_check(launch_slots_reset(c->slots.ptr, kScales, c->slot_n.ptr, c->slot_k.ptr, s), "cambi reset");
     for (int sc = 1; sc < kScales; sc++) {
@@ -229,7 +229,7 @@ int es_cambi_finish(es_cambi *c, double *score)
         require(c != nullptr && score != nullptr, "es_cambi_finish: NULL argument");
         if (!c->pending) throw Error(ES_ERR_STATE, "es_cambi_finish: nothing was launched");
         c->pending = false;
-        cuda_check(cudaStreamSynchronize(c->stream.s), "cambi");
+        cuda_check(cudaEventSynchronize(c->finished.e), "cambi");
         c->done = true;
         *score = c->host.ptr[0];
     });
@@ -277,7 +277,7 @@ int es_cambi_set_cvalue_planes(es_cambi *c, float *const dev_planes[5])
 void es_cambi_destroy(es_cambi *c)
 {
     if (!c) return;
-    if (c->pending) cudaStreamSynchronize(c->stream.s);
+    if (c->pending) cudaEventSynchronize(c->finished.e);
     delete c;
 }
 

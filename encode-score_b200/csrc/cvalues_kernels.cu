@@ -1,17 +1,19 @@
 // CAMBI c-values for sm_100a: src/kernels.cu:113-278 (cambi.c's c_value_pixel over the (2 pad + 1)^2 window of every
 // masked pixel in the band, histogram windows clipped at the picture's edges), bit-exact, with a different algorithm.
 //
-// One 256-thread block per 64 x 32 tile of any scale of any picture (a table of jobs):
-//  1. a pre-check of the tile's own pixels lets tiles with nothing to compute (most tiles of most pictures) leave
-//     after reading 2048 words;
+// One 256-thread block per 64 x 64 tile of any scale of any picture (a table of jobs):
+//  1. a pre-check of the tile's own pixels (16-byte loads) lets tiles with nothing to compute -- most tiles of most
+//     pictures -- leave after reading them;
 //  2. the tile and its window margins are staged in shared memory as band codes (value - band_base of a masked pixel
-//     in the band, kNone otherwise); the codes that can matter -- occurring within kDiffs of a code whose c-value is
-//     needed -- are ranked in order, and each such code gets a table of the rank offsets of its 8 neighbours;
-//  3. per pass over 32 ranks: column counts of the ranks over the window rows slide down the tile; per row, only the
-//     ranks some pixel of that row reads are turned into window counts, by a warp-parallel prefix sum over the
-//     columns (window count = difference of two prefix values), and two warps compute the row's c-values from them.
-// Positive c-values are summed exactly (they are multiples of 2^-24), counted, and appended to the scale's list for
-// the top-k selection; nothing per pixel is written unless the caller asks for the c-value planes.
+//     in the band, kNone otherwise) with 16-byte loads from an 8-pixel-aligned start; the codes that can matter --
+//     occurring within kDiffs of a code whose c-value is needed -- are ranked in order, and each needed code gets its
+//     8 neighbours' rank offsets and the mask of ranks it reads;
+//  3. per pass over 32 ranks: column counts (u8) of the ranks slide down the rows; per row, the rank pairs some pixel
+//     reads are prefix-summed over the columns (two ranks per 32-bit lane) and turned into window counts of the 64
+//     tile columns; every 4 rows all 8 warps compute the 256 c-values from those counts.
+// Positive c-values are summed exactly (they are multiples of 2^-24) and counted, and each block appends them to its
+// scale's list (for the top-k selection) through a bounded shared-memory buffer; nothing per pixel is written unless
+// the caller asks for the c-value planes.
 #include "es_kernels.h"
 
 namespace es {
@@ -19,47 +21,52 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCvChunk = kCvThreads / kCvTX;  // rows whose c-values are computed together
-
-__device__ __forceinline__ bool needs_cvalue(int code, const Band &bd)
-{
-    const int value = code + bd.band_base + kDiffs;
-    bool any = false;
-#pragma unroll
-    for (int d = 0; d < kDiffs; d++) any |= value <= bd.tvi[d] && value + d + 1 > bd.vlt;
-    return any;
-}
+constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
 
 __host__ __device__ constexpr int cv_rw(int pad) { return kCvTX + 2 * pad; }
+// the staged region starts at the multiple of 8 at or left of x0 - pad; its row stride is a whole number of vectors
+__host__ __device__ constexpr int cv_stride(int pad) { return (cv_rw(pad) + 7 + 7) & ~7; }
 __host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // column stride (scan width)
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 struct CvLayout {
-    size_t codes, rank, nbr, colcnt, prefix, wcount, list, total;
+    size_t codes, rank, nbr, relneed, colcnt, prefix, wcount, list, total;
 };
 __host__ __device__ inline CvLayout cv_layout(int pad)
 {
     CvLayout l;
     l.codes = 0;
-    l.rank = align16((size_t)cv_rw(pad) * (kCvTY + 2 * pad) * 2);
+    l.rank = align16((size_t)cv_stride(pad) * (kCvTY + 2 * pad) * 2);
     l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
-    l.colcnt = align16(l.nbr + (size_t)kMaxBand * 4);
+    l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
+    l.colcnt = align16(l.relneed + (size_t)kMaxBand * 2);
     l.prefix = align16(l.colcnt + (size_t)kCvBins * cv_cs(pad));
     l.wcount = align16(l.prefix + (size_t)(kCvThreads / 32) * cv_cs(pad) * 4);
     l.list = align16(l.wcount + (size_t)kCvChunk * (kCvBins / 2) * kCvTX * 4);
-    l.total = align16(l.list + (size_t)kCvTX * kCvTY * 4);
+    l.total = align16(l.list + (size_t)kListCap * 4);
     return l;
 }
 
-__device__ __forceinline__ uint16_t code_of(uint16_t word, const Band &bd)
+// the distances d + 1 at which a code's c-value looks (src/kernels.cu:195-197): bit d
+__host__ __device__ inline unsigned cvalue_dists(int code, const Band &bd)
 {
-    const unsigned u = (unsigned)(word & 0x7FFF) - (unsigned)bd.band_base;
+    const int value = code + bd.band_base + kDiffs;
+    unsigned m = 0;
+    for (int d = 0; d < kDiffs; d++) m |= (unsigned)(value <= bd.tvi[d] && value + d + 1 > bd.vlt) << d;
+    return m;
+}
+__device__ __forceinline__ bool needs_cvalue(int code, const Band &bd) { return cvalue_dists(code, bd) != 0; }
+
+__device__ __forceinline__ uint16_t code_of(unsigned word, const Band &bd)
+{
+    const unsigned u = (word & 0x7FFFu) - (unsigned)bd.band_base;
     return ((word & kMaskBit) && u < (unsigned)bd.band_size) ? (uint16_t)u : kNone;
 }
 
 __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_constant__ CvBatch b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t occ[32], srv[32], rel[32];
+    __shared__ uint32_t occ[32], srv[32], rel[32], needbits[32];
     __shared__ uint16_t relpre[33];
     __shared__ uint32_t rowneed[kCvTY];
     __shared__ unsigned list_n;
@@ -76,49 +83,102 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * kCvTY;
     const int w = J.w, h = J.h, P = J.pad;
     const int rows = min(kCvTY, h - y0), cols = min(kCvTX, w - x0);
+    const bool vec = (w & 7) == 0 && (((uintptr_t)J.word) & 15) == 0;  // rows of 16-byte vectors
+    // the codes whose c-value is needed (some d has value <= tvi[d] and value + d + 1 > vlt): warp w, words w + 8 k
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int code = (warp + 8 * k) * 32 + lane;
+        const unsigned m = __ballot_sync(kFull, code < bd.band_size && needs_cvalue(code, bd));
+        if (lane == 0) needbits[warp + 8 * k] = m;
+    }
+    __syncthreads();
+    auto needed = [&](unsigned code) { return (needbits[code >> 5] >> (code & 31)) & 1u; };
 
     // 1. does any pixel of the tile need a c-value?
     bool any = false;
-    for (int i = tid; i < kCvTX * kCvTY; i += kCvThreads) {
-        const int r = i >> 6, c = i & (kCvTX - 1);
-        if (r < rows && c < cols) {
-            const uint16_t code = code_of(J.word[(size_t)(y0 + r) * w + x0 + c], bd);
-            any |= code != kNone && needs_cvalue(code, bd);
+    if (vec && cols == kCvTX) {
+        for (int i = tid; i < kCvTY * (kCvTX / 8); i += kCvThreads) {
+            const int r = i >> 3, v = i & 7;
+            if (r >= rows) continue;
+            const uint4 q = __ldg((const uint4 *)(J.word + (size_t)(y0 + r) * w + x0) + v);
+            auto test = [&](unsigned word) {
+                const uint16_t c0 = code_of(word & 0xFFFFu, bd), c1 = code_of(word >> 16, bd);
+                any |= (c0 != kNone && needed(c0)) || (c1 != kNone && needed(c1));
+            };
+            test(q.x);
+            test(q.y);
+            test(q.z);
+            test(q.w);
+        }
+    } else {
+        for (int i = tid; i < kCvTX * kCvTY; i += kCvThreads) {
+            const int r = i >> 6, c = i & (kCvTX - 1);
+            if (r < rows && c < cols) {
+                const uint16_t code = code_of(J.word[(size_t)(y0 + r) * w + x0 + c], bd);
+                any |= code != kNone && needed(code);
+            }
         }
     }
     if (!__syncthreads_or(any)) return;
 
-    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P);
+    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P);
+    const int xs = ((x0 - P) >> 3) << 3, ox = (x0 - P) - xs;  // region start (aligned) and the offset of x0 - P in it
     const CvLayout L = cv_layout(P);
-    uint16_t *codes = (uint16_t *)(smem + L.codes);
+    uint16_t *codes = (uint16_t *)(smem + L.codes);           // [RH][S]: element e of row r is pixel (xs + e, y0 - P + r)
     uint16_t *rank = (uint16_t *)(smem + L.rank);
     uint32_t *nbr = (uint32_t *)(smem + L.nbr);
+    uint16_t *relneed = (uint16_t *)(smem + L.relneed);
     uint8_t *colcnt = smem + L.colcnt;
-    uint32_t *prefix = (uint32_t *)(smem + L.prefix);   // per-warp prefix rows
-    uint32_t *wcount = (uint32_t *)(smem + L.wcount);   // [chunk row][rank pair][column] packed window counts
+    uint32_t *prefix = (uint32_t *)(smem + L.prefix);        // per-warp prefix rows
+    uint32_t *wcount = (uint32_t *)(smem + L.wcount);        // [chunk row][rank pair][column] packed window counts
     float *blist = (float *)(smem + L.list);
     if (tid < 32) occ[tid] = srv[tid] = 0;
     if (tid == 0) list_n = 0;
     __syncthreads();
 
-    // 2. stage the region: threads cover 128 (or 256) columns of 2 (or 1) rows per iteration
+    // 2. stage the region, 8 elements per thread and step
     {
-        const int wide = RW > 128, c = wide ? tid : (tid & 127), dr = wide ? 0 : (tid >> 7), step = wide ? 1 : 2;
-        const int x = x0 - P + c;
-        const bool col_in = c < RW && x >= 0 && x < w;
-        const bool col_tile = c >= P && c < P + cols;
-        for (int r0 = 0; r0 < RH; r0 += step) {
-            const int r = r0 + dr, y = y0 - P + r;
-            uint16_t code = kNone;
-            if (col_in && r < RH && y >= 0 && y < h) code = code_of(J.word[(size_t)y * w + x], bd);
-            if (c < RW && r < RH) codes[r * RW + c] = code;
-            const bool served = code != kNone && col_tile && r >= P && r < P + rows && needs_cvalue(code, bd);
-            // mark each run of equal codes in the warp once
-            const unsigned prev = __shfl_up_sync(kFull, (unsigned)code, 1);
-            if (code != kNone && (lane == 0 || prev != code)) atomicOr(&occ[code >> 5], 1u << (code & 31));
-            const unsigned sv = served ? code : 0xFFFFu;
-            const unsigned sprev = __shfl_up_sync(kFull, sv, 1);
-            if (served && (lane == 0 || sprev != sv)) atomicOr(&srv[code >> 5], 1u << (code & 31));
+        const int nv = S >> 3, total = RH * nv;
+        for (int i = tid; i < total; i += kCvThreads) {
+            const int r = i / nv, v = i - r * nv, y = y0 - P + r, xv = xs + 8 * v;
+            uint16_t cs[8];
+            if (vec && y >= 0 && y < h && xv >= 0 && xv + 8 <= w) {
+                const uint4 q = __ldg((const uint4 *)(J.word + (size_t)y * w + xv));
+                cs[0] = code_of(q.x & 0xFFFFu, bd);
+                cs[1] = code_of(q.x >> 16, bd);
+                cs[2] = code_of(q.y & 0xFFFFu, bd);
+                cs[3] = code_of(q.y >> 16, bd);
+                cs[4] = code_of(q.z & 0xFFFFu, bd);
+                cs[5] = code_of(q.z >> 16, bd);
+                cs[6] = code_of(q.w & 0xFFFFu, bd);
+                cs[7] = code_of(q.w >> 16, bd);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int x = xv + k;
+                    cs[k] = (y >= 0 && y < h && x >= 0 && x < w) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
+                }
+            }
+            uint4 st;
+            st.x = cs[0] | ((unsigned)cs[1] << 16);
+            st.y = cs[2] | ((unsigned)cs[3] << 16);
+            st.z = cs[4] | ((unsigned)cs[5] << 16);
+            st.w = cs[6] | ((unsigned)cs[7] << 16);
+            *(uint4 *)(codes + r * S + 8 * v) = st;
+            const bool row_in_tile = r >= P && r < P + rows;
+            uint16_t prev = kNone, prev_srv = kNone;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint16_t code = cs[k];
+                if (code == kNone) continue;
+                if (code != prev) atomicOr(&occ[code >> 5], 1u << (code & 31));
+                prev = code;
+                const int x = xv + k;
+                if (row_in_tile && x >= x0 && x < x0 + cols && code != prev_srv && needed(code)) {
+                    atomicOr(&srv[code >> 5], 1u << (code & 31));
+                    prev_srv = code;
+                }
+            }
         }
     }
     __syncthreads();
@@ -148,23 +208,42 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
         rank[c] = (word & bit) ? (uint16_t)(relpre[c >> 5] + __popc(word & (bit - 1u))) : kNone;
     }
     __syncthreads();
-    // the rank offsets (+4) of the 8 neighbours u-4 .. u-1, u+1 .. u+4 of each served code; 15 = none
+    // for each served code: the rank offsets (+4) of its neighbours u-4 .. u-1, u+1 .. u+4 (15 = none), and the mask of
+    // the ranks rank-4 .. rank+4 it reads (bit 4 is its own)
     for (int c = tid; c < bd.band_size; c += kCvThreads) {
         if (!(srv[c >> 5] & (1u << (c & 31)))) continue;
         const int rc = rank[c];
+        const unsigned dists = cvalue_dists(c, bd);
         uint32_t packed = 0;
+        unsigned mask = 1u << 4;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const int q = c + (i < 4 ? i - 4 : i - 3);
+            const int d = i < 4 ? 3 - i : i - 4;  // distance d + 1
             unsigned nib = 15u;
-            if (q >= 0 && q < bd.band_size && rank[q] != kNone) nib = (unsigned)((int)rank[q] - rc + 4);
+            if (q >= 0 && q < bd.band_size && rank[q] != kNone) {
+                nib = (unsigned)((int)rank[q] - rc + 4);
+                if ((dists >> d) & 1u) mask |= 1u << nib;
+            }
             packed |= nib << (4 * i);
         }
         nbr[c] = packed;
+        relneed[c] = (uint16_t)mask;
     }
 
     unsigned long long my_sum = 0;
     unsigned my_cnt = 0;
+    CvSlot &SL = b.slots[J.slot];
+    // moves the block's buffered c-values to the scale's list (called by all threads, list_n > 0)
+    auto flush = [&]() {
+        if (tid == 0) list_base = atomicAdd(&SL.list_n, (unsigned long long)list_n);
+        __syncthreads();
+        const unsigned ln = list_n;
+        for (unsigned i = tid; i < ln; i += kCvThreads) SL.list[list_base + i] = blist[i];
+        __syncthreads();
+        if (tid == 0) list_n = 0;
+        __syncthreads();
+    };
 
     for (int b0 = 0;;) {
         const int B = min(kCvBins, R - b0);
@@ -177,17 +256,13 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             const int r = i >> 6, c = i & (kCvTX - 1);
             uint32_t need = 0;
             if (r < rows && c < cols) {
-                const uint16_t code = codes[(r + P) * RW + c + P];
+                const uint16_t code = codes[(r + P) * S + c + P + ox];
                 if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
                     const int rk = rank[code];
                     if (rk >= lo && rk < hi) {
-                        need = 1u << (rk - b0);
-                        const uint32_t nb = nbr[code];
-#pragma unroll
-                        for (int k = 0; k < 8; k++) {
-                            const unsigned o = (nb >> (4 * k)) & 15u;
-                            if (o != 15u) need |= 1u << (rk + (int)o - 4 - b0);
-                        }
+                        const int sh = rk - b0 - 4;
+                        const uint32_t m = relneed[code];
+                        need = sh >= 0 ? m << sh : m >> -sh;
                     }
                 }
             }
@@ -199,7 +274,7 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             uint8_t *col = colcnt + tid;
             const int last = min(2 * P, RH - 1);
             for (int r = 0; r <= last; r++) {
-                const uint16_t code = codes[r * RW + tid];
+                const uint16_t code = codes[r * S + tid + ox];
                 if (code != kNone) {
                     const int k = (int)rank[code] - b0;
                     if ((unsigned)k < (unsigned)B) col[k * CS]++;
@@ -214,13 +289,13 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
         auto slide = [&](int r) {
             if (tid >= RW) return;
             uint8_t *col = colcnt + tid;
-            const uint16_t cl = codes[(r - 1) * RW + tid];
+            const uint16_t cl = codes[(r - 1) * S + tid + ox];
             if (cl != kNone) {
                 const int k = (int)rank[cl] - b0;
                 if ((unsigned)k < (unsigned)B) col[k * CS]--;
             }
             if (r + 2 * P < RH) {
-                const uint16_t ce = codes[(r + 2 * P) * RW + tid];
+                const uint16_t ce = codes[(r + 2 * P) * S + tid + ox];
                 if (ce != kNone) {
                     const int k = (int)rank[ce] - b0;
                     if ((unsigned)k < (unsigned)B) col[k * CS]++;
@@ -231,9 +306,11 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             const uint32_t need = rowneed[r];
             uint32_t *wpre = prefix + warp * CS;
             const uint32_t pairs = (need | (need >> 1)) & 0x55555555u;  // bit 2p: pair p is read
-            const int npairs = __popc(pairs);
-            for (int n = warp; n < npairs; n += kCvThreads / 32) {  // warp w takes every 8th pair
-                const int p = (int)__fns(pairs, 0, n + 1) >> 1;
+            uint32_t pp = pairs;  // warp w takes pairs w, w + 8 (in the order of the read pairs)
+            for (int t = 0; t < warp && pp; t++) pp &= pp - 1u;
+            while (pp) {
+                const int p = (__ffs(pp) - 1) >> 1;
+                for (int t = 0; t < kCvThreads / 32 && pp; t++) pp &= pp - 1u;
                 const uint8_t *ca = colcnt + (2 * p) * CS, *cb = ca + CS;
                 unsigned carry = 0;
                 for (int base = 0; base < CS; base += 128) {
@@ -269,8 +346,7 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             for (int i = 0; i < n_rows; i++) {
                 const int r = r0 + i;
                 if (r > 0) slide(r);
-                const uint32_t need = rowneed[r];
-                if (!need) continue;
+                if (!rowneed[r]) continue;
                 chunk_any = true;
                 __syncthreads();
                 window_counts(r, i);
@@ -282,7 +358,7 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             bool served = false;
             const int r = r0 + ci;
             if (ci < n_rows && cc < cols) {
-                const uint16_t code = codes[(r + P) * RW + cc + P];
+                const uint16_t code = codes[(r + P) * S + cc + P + ox];
                 if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
                     const int rk = rank[code];
                     if (rk >= lo && rk < hi) {
@@ -321,13 +397,14 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
                 my_cnt++;
             }
             __syncthreads();
+            if (list_n > kListCap - kCvThreads) flush();
         }
         if (hi == R) break;
         b0 = hi - kDiffs;
         __syncthreads();
     }
 
-    // block totals, and this block's positive c-values appended to the scale's list
+    // block totals, and the rest of this block's positive c-values appended to the scale's list
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         my_sum += __shfl_down_sync(kFull, my_sum, o);
@@ -338,7 +415,6 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
         red_cnt[warp] = my_cnt;
     }
     __syncthreads();
-    CvSlot &S = b.slots[J.slot];
     if (tid == 0) {
         unsigned long long s = 0;
         unsigned c = 0;
@@ -346,16 +422,12 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             s += red_sum[k];
             c += red_cnt[k];
         }
-        list_base = 0;
         if (c) {
-            atomicAdd(&S.sum_fx, s);
-            atomicAdd(&S.count, (unsigned long long)c);
-            list_base = atomicAdd(&S.list_n, (unsigned long long)list_n);
+            atomicAdd(&SL.sum_fx, s);
+            atomicAdd(&SL.count, (unsigned long long)c);
         }
     }
-    __syncthreads();
-    const unsigned ln = list_n;
-    for (unsigned i = tid; i < ln; i += kCvThreads) S.list[list_base + i] = blist[i];
+    if (list_n) flush();
 }
 
 }  // namespace

@@ -27,6 +27,9 @@ struct LaunchTimer {
     ~LaunchTimer();
     LaunchTimer(const LaunchTimer &) = delete;
 };
+// True while es_kernel_timing(2) is in force: CAMBI instances then queue all their work on the caller's stream, so
+// that nothing runs beside a timed kernel and its events bracket that kernel alone.
+bool serial_streams();
 
 constexpr int kScales = 5;
 constexpr int kDiffs = 4;
@@ -100,7 +103,7 @@ struct CvBatch {
     const float *lut;  // lut[i] = 1/i as float, i < (2 max_pad + 1)^2 + 1
     CvSlot *slots;
 };
-constexpr int kCvTX = 64, kCvTY = 32, kCvThreads = 256, kCvBins = 32;
+constexpr int kCvTX = 64, kCvTY = 64, kCvThreads = 256, kCvBins = 32;
 size_t cvalues_smem_bytes(int max_pad);
 cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s);
 

@@ -25,7 +25,7 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 namespace {
 struct Timing {
     std::mutex m;
-    std::atomic<bool> on{false};
+    std::atomic<bool> on{false}, serial{false};
     struct Pending {
         std::string name;
         cudaEvent_t a, b;
@@ -68,6 +68,8 @@ LaunchTimer::~LaunchTimer()
     std::lock_guard<std::mutex> lock(t.m);
     if (slot < (int)t.pending.size()) cudaEventRecord(t.pending[slot].b, stream);
 }
+
+bool serial_streams() { return timing().serial.load(std::memory_order_relaxed); }
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }
@@ -211,7 +213,9 @@ int es_kernel_timing(int on)
     return guarded([&] {
         Timing &t = timing();
         std::lock_guard<std::mutex> lock(t.m);
+        require(on >= 0 && on <= 2, "es_kernel_timing: on must be 0, 1 or 2");
         t.on = on != 0;
+        t.serial = on == 2;
         if (on) t.totals.clear();
     });
 }

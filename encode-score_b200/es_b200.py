@@ -139,8 +139,10 @@ def launch_count() -> int:
     return int(lib().es_launch_count())
 
 
-def kernel_timing(on: bool) -> None:
-    check(lib().es_kernel_timing(int(on)))
+def kernel_timing(on: bool, serial: bool = False) -> None:
+    """Brackets each later kernel launch with CUDA events; with serial=True the CAMBI work also stays on the caller's
+    stream, so each event pair times one kernel running alone."""
+    check(lib().es_kernel_timing(2 if (on and serial) else int(bool(on))))
 
 
 def kernel_times() -> dict:

@@ -38,7 +38,9 @@ int es_version(void);
  * (all threads), so a caller can check how many GPU launches a piece of work took. */
 uint64_t es_launch_count(void);
 /* Diagnostics with no counterpart in the reference: with on != 0, each later kernel launch of the library is
- * bracketed by CUDA events on the stream it is launched on (and earlier totals are cleared); 0 stops it. */
+ * bracketed by CUDA events on the stream it is launched on (and earlier totals are cleared); 0 stops it. With on == 2
+ * the CAMBI work of es_cambi_launch and es_frame_queue also stays on the caller's stream instead of each instance's
+ * own, so kernels run one at a time and each event pair times one kernel alone. */
 int es_kernel_timing(int on);
 /* Waits for the device, then writes per kernel (up to `max` kernels): its name in names[32 i .. 32 i + 31]
  * (NUL-terminated), the summed event time in total_ms[i] and the number of timed launches in launches[i];
