@@ -6,11 +6,14 @@
 //     pictures -- leave after reading them;
 //  2. the tile and its window margins are staged in shared memory as band codes (value - band_base of a masked pixel
 //     in the band, kNone otherwise) with 16-byte loads from an 8-pixel-aligned start; the codes that can matter --
-//     occurring within kDiffs of a code whose c-value is needed -- are ranked in order, and each needed code gets its
-//     8 neighbours' rank offsets and the mask of ranks it reads;
-//  3. per pass over 32 ranks: column counts (u8) of the ranks slide down the rows; per row, the rank pairs some pixel
-//     reads are prefix-summed over the columns (two ranks per 32-bit lane) and turned into window counts of the 64
-//     tile columns; every 4 rows all 8 warps compute the 256 c-values from those counts.
+//     occurring within kDiffs of a code whose c-value is needed -- are ranked in order, each rank gets its code, the
+//     rank offsets of its 8 neighbour codes and the mask of ranks its c-value reads, and the region becomes a plane
+//     of 8-bit ranks;
+//  3. per pass over 32 ranks, rank pair p (two ranks) belongs to warp p % 8: the warp keeps the pair's column counts
+//     (ranks occurring in the 2 pad + 1 window rows of each column, 8 bits per column and rank, 4 columns per lane) in
+//     registers, slides them down the rows with byte-parallel compares of the leaving and entering rows, and on rows
+//     whose pixels read the pair turns them into window counts of the 64 tile columns (a prefix sum over the columns,
+//     two ranks per 32-bit lane). Every 4 rows all 8 warps compute the 256 c-values from those counts.
 // Positive c-values are summed exactly (they are multiples of 2^-24) and counted, and each block appends them to its
 // scale's list (for the top-k selection) through a bounded shared-memory buffer; nothing per pixel is written unless
 // the caller asks for the c-value planes.
@@ -22,28 +25,36 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCvChunk = kCvThreads / kCvTX;  // rows whose c-values are computed together
 constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
+constexpr int kWarps = kCvThreads / 32;
+constexpr unsigned kNoRank = 0xFFu;           // rank plane: no relevant code
+constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks can hold
 
 __host__ __device__ constexpr int cv_rw(int pad) { return kCvTX + 2 * pad; }
 // the staged region starts at the multiple of 8 at or left of x0 - pad; its row stride is a whole number of vectors
 __host__ __device__ constexpr int cv_stride(int pad) { return (cv_rw(pad) + 7 + 7) & ~7; }
-__host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // column stride (scan width)
+__host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // rank plane row (scan width)
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+__host__ __device__ constexpr size_t max_sz(size_t a, size_t b) { return a > b ? a : b; }
 
+// Shared memory: the rank plane and the per-code and per-rank tables, then a union of the staged codes (dead once
+// the rank plane is built) and the pass buffers.
 struct CvLayout {
-    size_t codes, rank, nbr, relneed, colcnt, prefix, wcount, list, total;
+    size_t rplane, rank, rcode, nbr, relneed, codes, wcount, prefix, list, total;
 };
 __host__ __device__ inline CvLayout cv_layout(int pad)
 {
+    const size_t rh = (size_t)kCvTY + 2 * pad;
     CvLayout l;
-    l.codes = 0;
-    l.rank = align16((size_t)cv_stride(pad) * (kCvTY + 2 * pad) * 2);
-    l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
+    l.rplane = 0;
+    l.rank = align16(l.rplane + rh * cv_cs(pad));
+    l.rcode = align16(l.rank + (size_t)kMaxBand * 2);
+    l.nbr = align16(l.rcode + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
-    l.colcnt = align16(l.relneed + (size_t)kMaxBand * 2);
-    l.prefix = align16(l.colcnt + (size_t)kCvBins * cv_cs(pad));
-    l.wcount = align16(l.prefix + (size_t)(kCvThreads / 32) * cv_cs(pad) * 4);
-    l.list = align16(l.wcount + (size_t)kCvChunk * (kCvBins / 2) * kCvTX * 4);
-    l.total = align16(l.list + (size_t)kListCap * 4);
+    l.codes = align16(l.relneed + (size_t)kMaxBand * 2);
+    l.wcount = l.codes;
+    l.prefix = align16(l.wcount + (size_t)kCvChunk * (kCvBins / 2) * kCvTX * 4);
+    l.list = align16(l.prefix + (size_t)kWarps * cv_cs(pad) * 4);
+    l.total = align16(max_sz(l.codes + (size_t)cv_stride(pad) * rh * 2, l.list + (size_t)kListCap * 4));
     return l;
 }
 
@@ -63,6 +74,16 @@ __device__ __forceinline__ uint16_t code_of(unsigned word, const Band &bd)
     return ((word & kMaskBit) && u < (unsigned)bd.band_size) ? (uint16_t)u : kNone;
 }
 
+// Bytes of `quad` equal to a (ma) and to a + 1 (mb), a even, ta4 = a in every byte: 1 per matching byte.
+__device__ __forceinline__ void pair_match(uint32_t quad, uint32_t ta4, uint32_t &ma, uint32_t &mb)
+{
+    const uint32_t z = quad ^ ta4;                                             // 0 for a, 1 for a + 1
+    const uint32_t t = ((z & 0x7E7E7E7Eu) + 0x7F7F7F7Fu) | (z & 0xFEFEFEFEu);  // bit 7 set: byte not in {a, a + 1}
+    const uint32_t hit = (~t >> 7) & 0x01010101u;
+    mb = hit & z;
+    ma = hit ^ mb;
+}
+
 __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_constant__ CvBatch b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -71,8 +92,8 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     __shared__ uint32_t rowneed[kCvTY];
     __shared__ unsigned list_n;
     __shared__ unsigned long long list_base;
-    __shared__ unsigned long long red_sum[kCvThreads / 32];
-    __shared__ unsigned red_cnt[kCvThreads / 32];
+    __shared__ unsigned long long red_sum[kWarps];
+    __shared__ unsigned red_cnt[kWarps];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int j = 0;
@@ -121,16 +142,17 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     }
     if (!__syncthreads_or(any)) return;
 
-    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P);
+    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P), NQ = CS / 128;
     const int xs = ((x0 - P) >> 3) << 3, ox = (x0 - P) - xs;  // region start (aligned) and the offset of x0 - P in it
     const CvLayout L = cv_layout(P);
-    uint16_t *codes = (uint16_t *)(smem + L.codes);           // [RH][S]: element e of row r is pixel (xs + e, y0 - P + r)
-    uint16_t *rank = (uint16_t *)(smem + L.rank);
-    uint32_t *nbr = (uint32_t *)(smem + L.nbr);
-    uint16_t *relneed = (uint16_t *)(smem + L.relneed);
-    uint8_t *colcnt = smem + L.colcnt;
-    uint32_t *prefix = (uint32_t *)(smem + L.prefix);        // per-warp prefix rows
-    uint32_t *wcount = (uint32_t *)(smem + L.wcount);        // [chunk row][rank pair][column] packed window counts
+    uint8_t *rplane = smem + L.rplane;                   // [RH][CS]: rank (- offset) of pixel (x0 - P + j, y0 - P + r)
+    uint16_t *rank = (uint16_t *)(smem + L.rank);        // code -> rank
+    uint16_t *rcode = (uint16_t *)(smem + L.rcode);      // rank -> code
+    uint32_t *nbr = (uint32_t *)(smem + L.nbr);          // rank -> neighbour rank offsets
+    uint16_t *relneed = (uint16_t *)(smem + L.relneed);  // rank -> ranks read (bit 4: itself); 0: not served
+    uint16_t *codes = (uint16_t *)(smem + L.codes);      // [RH][S]: element e of row r is pixel (xs + e, y0 - P + r)
+    uint32_t *wcount = (uint32_t *)(smem + L.wcount);    // [chunk row][rank pair][column] packed window counts
+    uint32_t *prefix = (uint32_t *)(smem + L.prefix);    // per-warp prefix rows
     float *blist = (float *)(smem + L.list);
     if (tid < 32) occ[tid] = srv[tid] = 0;
     if (tid == 0) list_n = 0;
@@ -208,11 +230,16 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
         rank[c] = (word & bit) ? (uint16_t)(relpre[c >> 5] + __popc(word & (bit - 1u))) : kNone;
     }
     __syncthreads();
-    // for each served code: the rank offsets (+4) of its neighbours u-4 .. u-1, u+1 .. u+4 (15 = none), and the mask of
-    // the ranks rank-4 .. rank+4 it reads (bit 4 is its own)
+    // per rank: its code; for a served code the rank offsets (+4) of its neighbours u-4 .. u-1, u+1 .. u+4 (15 = none)
+    // and the mask of the ranks rank-4 .. rank+4 its c-value reads (bit 4 is its own)
     for (int c = tid; c < bd.band_size; c += kCvThreads) {
-        if (!(srv[c >> 5] & (1u << (c & 31)))) continue;
         const int rc = rank[c];
+        if (rc == kNone) continue;
+        rcode[rc] = (uint16_t)c;
+        if (!(srv[c >> 5] & (1u << (c & 31)))) {
+            relneed[rc] = 0;
+            continue;
+        }
         const unsigned dists = cvalue_dists(c, bd);
         uint32_t packed = 0;
         unsigned mask = 1u << 4;
@@ -227,9 +254,39 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             }
             packed |= nib << (4 * i);
         }
-        nbr[c] = packed;
-        relneed[c] = (uint16_t)mask;
+        nbr[rc] = packed;
+        relneed[rc] = (uint16_t)mask;
     }
+    // the rank plane: absolute ranks once for the tile when they fit in a byte, else per pass relative to the pass
+    const bool per_pass = R > kMaxPlaneRank + 1;
+    auto build_plane = [&](int b0) {  // b0 < 0: absolute ranks from the staged codes; else pass ranks from the words
+        for (int i = tid; i < RH * (CS / 4); i += kCvThreads) {
+            const int r = i / (CS / 4), j0 = 4 * (i - r * (CS / 4));
+            uint32_t quad = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int jj = j0 + k;
+                unsigned v = kNoRank;
+                if (jj < RW) {
+                    uint16_t code;
+                    if (b0 < 0) {
+                        code = codes[r * S + jj + ox];
+                    } else {
+                        const int x = x0 - P + jj, y = y0 - P + r;
+                        code = (x >= 0 && x < w && y >= 0 && y < h) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
+                    }
+                    if (code != kNone && rank[code] != kNone) {
+                        const int rk = rank[code] - (b0 < 0 ? 0 : b0);
+                        if (b0 < 0 || (rk >= 0 && rk < kCvBins)) v = (unsigned)rk;
+                    }
+                }
+                quad |= v << (8 * k);
+            }
+            *(uint32_t *)(rplane + r * CS + j0) = quad;
+        }
+    };
+    if (!per_pass) build_plane(-1);
+    __syncthreads();  // the staged codes are dead from here: their space holds the pass buffers
 
     unsigned long long my_sum = 0;
     unsigned my_cnt = 0;
@@ -245,23 +302,24 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
         __syncthreads();
     };
 
+    uint32_t *wpre = prefix + warp * CS;
     for (int b0 = 0;;) {
-        const int B = min(kCvBins, R - b0);
         const int lo = b0 ? b0 + kDiffs : 0, hi = b0 + kCvBins >= R ? R : b0 + kCvBins - kDiffs;
+        const int off = per_pass ? 0 : b0;  // plane value of pass rank k: k + off
+        if (per_pass) build_plane(b0);
         if (tid < kCvTY) rowneed[tid] = 0;
-        for (int i = tid * 16; i < kCvBins * CS; i += kCvThreads * 16) *(uint4 *)(colcnt + i) = make_uint4(0, 0, 0, 0);
         __syncthreads();
-        // the ranks each row's pixels read in this pass: a warp covers 32 pixels of one row
+        // the pass ranks each row's pixels read: a warp covers 32 pixels of one row
         for (int i = tid; i < kCvTY * kCvTX; i += kCvThreads) {
             const int r = i >> 6, c = i & (kCvTX - 1);
             uint32_t need = 0;
             if (r < rows && c < cols) {
-                const uint16_t code = codes[(r + P) * S + c + P + ox];
-                if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
-                    const int rk = rank[code];
+                const unsigned v = rplane[(r + P) * CS + c + P];
+                if (v != kNoRank) {
+                    const int k = (int)v - off, rk = b0 + k;
                     if (rk >= lo && rk < hi) {
-                        const int sh = rk - b0 - 4;
-                        const uint32_t m = relneed[code];
+                        const uint32_t m = relneed[rk];
+                        const int sh = k - 4;
                         need = sh >= 0 ? m << sh : m >> -sh;
                     }
                 }
@@ -269,75 +327,75 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             need = __reduce_or_sync(kFull, need);
             if (lane == 0 && need) atomicOr(&rowneed[r], need);
         }
-        // column counts over the window rows of tile row 0 (region rows 0 .. 2P)
-        if (tid < RW) {
-            uint8_t *col = colcnt + tid;
-            const int last = min(2 * P, RH - 1);
-            for (int r = 0; r <= last; r++) {
-                const uint16_t code = codes[r * S + tid + ox];
-                if (code != kNone) {
-                    const int k = (int)rank[code] - b0;
-                    if ((unsigned)k < (unsigned)B) col[k * CS]++;
-                }
-            }
-        }
         __syncthreads();
-        // Rows go in chunks of kCvChunk. Per row: (a) slide the column counts down to it; (b) each warp turns every 8th
-        // pair of the ranks the row reads into a packed prefix sum over the columns (two ranks per 32-bit lane) and
-        // then into the window counts of the tile's 64 columns. Per chunk: (c) every thread computes one pixel's
-        // c-value from those counts.
-        auto slide = [&](int r) {
-            if (tid >= RW) return;
-            uint8_t *col = colcnt + tid;
-            const uint16_t cl = codes[(r - 1) * S + tid + ox];
-            if (cl != kNone) {
-                const int k = (int)rank[cl] - b0;
-                if ((unsigned)k < (unsigned)B) col[k * CS]--;
-            }
-            if (r + 2 * P < RH) {
-                const uint16_t ce = codes[(r + 2 * P) * S + tid + ox];
-                if (ce != kNone) {
-                    const int k = (int)rank[ce] - b0;
-                    if ((unsigned)k < (unsigned)B) col[k * CS]++;
+        // this warp's rank pairs w and w + 8, if some row reads them: column counts of 4 columns per lane and quad
+        const uint32_t pass_need = __reduce_or_sync(kFull, rowneed[lane] | rowneed[lane + 32]);
+        const uint32_t pairs_used = (pass_need | (pass_need >> 1)) & 0x55555555u;
+        bool act[2];
+        uint32_t t4[2];
+        uint32_t cnt[2][2][2];  // [owned pair][quad][rank a, a + 1]: 8-bit counts of 4 columns
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int p = warp + kWarps * s;
+            act[s] = (pairs_used >> (2 * p)) & 1u;
+            t4[s] = (unsigned)(2 * p + off) * 0x01010101u;
+#pragma unroll
+            for (int q = 0; q < 2; q++) cnt[s][q][0] = cnt[s][q][1] = 0;
+        }
+        auto count_row = [&](int r, bool enter) {  // adds (enter) or removes the ranks of region row r
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                if (q >= NQ) break;
+                const uint32_t quad = *(const uint32_t *)(rplane + r * CS + 128 * q + 4 * lane);
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    if (!act[s]) continue;
+                    uint32_t ma, mb;
+                    pair_match(quad, t4[s], ma, mb);
+                    if (enter) {
+                        cnt[s][q][0] += ma;
+                        cnt[s][q][1] += mb;
+                    } else {
+                        cnt[s][q][0] -= ma;
+                        cnt[s][q][1] -= mb;
+                    }
                 }
             }
         };
-        auto window_counts = [&](int r, int i) {  // row r into chunk slot i
-            const uint32_t need = rowneed[r];
-            uint32_t *wpre = prefix + warp * CS;
-            const uint32_t pairs = (need | (need >> 1)) & 0x55555555u;  // bit 2p: pair p is read
-            uint32_t pp = pairs;  // warp w takes pairs w, w + 8 (in the order of the read pairs)
-            for (int t = 0; t < warp && pp; t++) pp &= pp - 1u;
-            while (pp) {
-                const int p = (__ffs(pp) - 1) >> 1;
-                for (int t = 0; t < kCvThreads / 32 && pp; t++) pp &= pp - 1u;
-                const uint8_t *ca = colcnt + (2 * p) * CS, *cb = ca + CS;
-                unsigned carry = 0;
-                for (int base = 0; base < CS; base += 128) {
-                    const uint32_t fa = *(const uint32_t *)(ca + base + 4 * lane), fb = *(const uint32_t *)(cb + base + 4 * lane);
-                    const uint32_t a0 = fa & 0x00FF00FFu, c0 = fb & 0x00FF00FFu, a1 = (fa >> 8) & 0x00FF00FFu, c1 = (fb >> 8) & 0x00FF00FFu;
-                    // column 4 lane + i of rank 2p in the low 16 bits, of rank 2p + 1 in the high 16 bits
-                    const unsigned s1 = __byte_perm(a0, c0, 0x5410), s2 = s1 + __byte_perm(a1, c1, 0x5410),
-                                   s3 = s2 + __byte_perm(a0, c0, 0x7632), s4 = s3 + __byte_perm(a1, c1, 0x7632);
-                    unsigned incl = s4;
+        if (act[0] || act[1]) {
+            const int last = min(2 * P, RH - 1);
+            for (int r = 0; r <= last; r++) count_row(r, true);
+        }
+        // window counts of owned pair s at chunk row i into wcount
+        auto window_counts = [&](int s, int i) {
+            const int p = warp + kWarps * s;
+            unsigned carry = 0;
 #pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const unsigned v = __shfl_up_sync(kFull, incl, o);
-                        if (lane >= o) incl += v;
-                    }
-                    const unsigned ex = incl - s4 + carry;
-                    *(uint4 *)(wpre + base + 4 * lane) = make_uint4(ex + s1, ex + s2, ex + s3, ex + s4);
-                    carry += __shfl_sync(kFull, incl, 31);
-                }
-                __syncwarp();
-                uint32_t *wrow = wcount + (i * (kCvBins / 2) + p) * kCvTX;
+            for (int q = 0; q < 2; q++) {
+                if (q >= NQ) break;
+                const uint32_t fa = cnt[s][q][0], fb = cnt[s][q][1];
+                const uint32_t a0 = fa & 0x00FF00FFu, c0 = fb & 0x00FF00FFu, a1 = (fa >> 8) & 0x00FF00FFu, c1 = (fb >> 8) & 0x00FF00FFu;
+                // column 4 lane + i of rank 2p in the low 16 bits, of rank 2p + 1 in the high 16 bits
+                const unsigned s1 = __byte_perm(a0, c0, 0x5410), s2 = s1 + __byte_perm(a1, c1, 0x5410),
+                               s3 = s2 + __byte_perm(a0, c0, 0x7632), s4 = s3 + __byte_perm(a1, c1, 0x7632);
+                unsigned incl = s4;
 #pragma unroll
-                for (int h2 = 0; h2 < 2; h2++) {
-                    const int x = lane + 32 * h2;
-                    wrow[x] = wpre[x + 2 * P] - (x > 0 ? wpre[x - 1] : 0u);
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned v = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += v;
                 }
-                __syncwarp();
+                const unsigned ex = incl - s4 + carry;
+                *(uint4 *)(wpre + 128 * q + 4 * lane) = make_uint4(ex + s1, ex + s2, ex + s3, ex + s4);
+                carry += __shfl_sync(kFull, incl, 31);
             }
+            __syncwarp();
+            uint32_t *wrow = wcount + (i * (kCvBins / 2) + p) * kCvTX;
+#pragma unroll
+            for (int h2 = 0; h2 < 2; h2++) {
+                const int x = lane + 32 * h2;
+                wrow[x] = wpre[x + 2 * P] - (x > 0 ? wpre[x - 1] : 0u);
+            }
+            __syncwarp();
         };
         const int ci = tid >> 6, cc = tid & (kCvTX - 1);  // this thread's pixel in a chunk
         for (int r0 = 0; r0 < rows; r0 += kCvChunk) {
@@ -345,30 +403,34 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             bool chunk_any = false;
             for (int i = 0; i < n_rows; i++) {
                 const int r = r0 + i;
-                if (r > 0) slide(r);
-                if (!rowneed[r]) continue;
-                chunk_any = true;
-                __syncthreads();
-                window_counts(r, i);
-                __syncthreads();
+                if (r > 0 && (act[0] || act[1])) {
+                    count_row(r - 1, false);
+                    if (r + 2 * P < RH) count_row(r + 2 * P, true);
+                }
+                const uint32_t need = rowneed[r];
+                chunk_any |= need != 0;
+#pragma unroll
+                for (int s = 0; s < 2; s++)
+                    if (act[s] && ((need >> (2 * (warp + kWarps * s))) & 3u)) window_counts(s, i);
             }
             if (!chunk_any) continue;
-            // (c) the chunk's c-values, one pixel per thread
+            __syncthreads();
+            // the chunk's c-values, one pixel per thread
             float c = 0.0f;
             bool served = false;
             const int r = r0 + ci;
             if (ci < n_rows && cc < cols) {
-                const uint16_t code = codes[(r + P) * S + cc + P + ox];
-                if (code != kNone && (srv[code >> 5] & (1u << (code & 31)))) {
-                    const int rk = rank[code];
-                    if (rk >= lo && rk < hi) {
+                const unsigned v = rplane[(r + P) * CS + cc + P];
+                if (v != kNoRank) {
+                    const int k = (int)v - off, rk = b0 + k;
+                    if (rk >= lo && rk < hi && relneed[rk]) {
                         served = true;
-                        const uint32_t nb = nbr[code];
-                        const int base = rk - b0 - 4;
+                        const uint32_t nb = nbr[rk];
+                        const int base = k - 4;
                         const uint32_t *wc = wcount + ci * (kCvBins / 2) * kCvTX + cc;
-                        auto count = [&](int k) -> unsigned { return (wc[(k >> 1) * kCvTX] >> ((k & 1) * 16)) & 0xFFFFu; };
-                        const int value = code + bd.band_base + kDiffs;
-                        const unsigned p0 = count(rk - b0);
+                        auto count = [&](int kk) -> unsigned { return (wc[(kk >> 1) * kCvTX] >> ((kk & 1) * 16)) & 0xFFFFu; };
+                        const int value = rcode[rk] + bd.band_base + kDiffs;
+                        const unsigned p0 = count(k);
 #pragma unroll
                         for (int d = 0; d < kDiffs; d++) {
                             if (value <= bd.tvi[d] && value + d + 1 > bd.vlt) {
@@ -418,7 +480,7 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     if (tid == 0) {
         unsigned long long s = 0;
         unsigned c = 0;
-        for (int k = 0; k < kCvThreads / 32; k++) {
+        for (int k = 0; k < kWarps; k++) {
             s += red_sum[k];
             c += red_cnt[k];
         }

@@ -133,41 +133,128 @@ __device__ __forceinline__ float oriented_of(long long jxx, long long jyy, long 
 
 // ---------------------------------------------------------------------------------------------------------------
 // Window statistics of one source frame against every encode: src/kernels.cu:346-428, exact.
+//
+// A block of 256 threads takes a 64 x 64 tile (4 x 4 windows) of every picture in turn. Per picture: the 72 x 72 region
+// (4-pixel margin, coordinates clamped) is staged in shared memory with 8-byte loads; each thread then builds the
+// horizontal 3- and 9-sums of 8 columns of a region row from two 16-byte reads; then thread (c, g) walks tile column c
+// down rows 16 g .. 16 g + 15 (one window's column) with running vertical sums, so the 3 x 3 and 9 x 9 sums of a pixel
+// cost a few additions. The 16 lanes of a window reduce its sums with shuffles.
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) window_stats_kernel(const __grid_constant__ WindowJob J)
+constexpr int kWT = 64;             // tile side
+constexpr int kWR = kWT + 2 * kM;   // region side, 72
+constexpr int kWS = 72;             // row stride of the region planes (144 bytes, a multiple of 16)
+
+struct WinSmem {
+    uint16_t y[kWR][kWS];   // y[r][j]: pixel (x0 - 4 + j, y0 - 4 + r), coordinates clamped
+    uint16_t h3[kWR][kWS];  // h3[r][k]: 3-sum of row r centred at x0 - 1 + k, k < 66
+    uint16_t h9[kWR][kWT];  // h9[r][c]: 9-sum of row r centred at x0 + c
+};
+
+// Stages the region of `src` (w x h, values shifted left by `up`; null reads 0) at tile (x0, y0).
+__device__ __forceinline__ void stage_window_region(WinSmem &sm, const uint16_t *src, int w, int h, int up, int x0, int y0)
 {
-    __shared__ BoxSmem sm;
+    if (src && x0 >= kM && x0 + kWT + kM <= w && (w & 3) == 0 && ((uintptr_t)src & 7) == 0) {
+        // interior columns: 18 loads of 4 pixels per row (x0 - 4 is a multiple of 4)
+        for (int i = threadIdx.x; i < kWR * 18; i += 256) {
+            const int r = i / 18, q = i - r * 18;
+            const int y = min(max(y0 - kM + r, 0), h - 1);
+            uint2 v = __ldg((const uint2 *)(src + (size_t)y * w + (x0 - kM)) + q);
+            v.x <<= up;  // both 16-bit samples: they stay below 2^10 after the shift
+            v.y <<= up;
+            *(uint2 *)&sm.y[r][4 * q] = v;
+        }
+    } else {
+        for (int i = threadIdx.x; i < kWR * kWR; i += 256) {
+            const int r = i / kWR, j = i - r * kWR;
+            const int x = min(max(x0 - kM + j, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
+            sm.y[r][j] = src ? (uint16_t)(src[(size_t)y * w + x] << up) : (uint16_t)0;
+        }
+    }
+}
+
+// h3 and h9 of every region row: item (r, s) covers columns 8 s .. 8 s + 7 from y[r][8 s .. 8 s + 15].
+__device__ __forceinline__ void window_horizontal_sums(WinSmem &sm)
+{
+    for (int i = threadIdx.x; i < kWR * 8; i += 256) {
+        const int r = i >> 3, c0 = 8 * (i & 7);
+        const uint4 a = *(const uint4 *)&sm.y[r][c0], b = *(const uint4 *)&sm.y[r][c0 + 8];
+        const unsigned wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        int v[16];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            v[2 * k] = (int)(wv[k] & 0xFFFFu);
+            v[2 * k + 1] = (int)(wv[k] >> 16);
+        }
+        int s9 = 0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) s9 += v[k];
+        int h9[8], h3[10];
+        h9[0] = s9;
+#pragma unroll
+        for (int k = 1; k < 8; k++) {
+            s9 += v[k + 8] - v[k - 1];
+            h9[k] = s9;
+        }
+#pragma unroll
+        for (int k = 0; k < 10; k++) h3[k] = v[k + 2] + v[k + 3] + v[k + 4];
+        *(uint4 *)&sm.h9[r][c0] = make_uint4(h9[0] | (h9[1] << 16), h9[2] | (h9[3] << 16), h9[4] | (h9[5] << 16), h9[6] | (h9[7] << 16));
+        *(uint4 *)&sm.h3[r][c0] = make_uint4(h3[0] | (h3[1] << 16), h3[2] | (h3[3] << 16), h3[4] | (h3[5] << 16), h3[6] | (h3[7] << 16));
+        if (c0 == 56) *(uint32_t *)&sm.h3[r][64] = h3[8] | (h3[9] << 16);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T half_warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 8; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_constant__ WindowJob J)
+{
+    __shared__ __align__(16) WinSmem sm;
     const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
     const int tiles_x = (ww + 3) / 4;
-    const int x0 = (blockIdx.x % tiles_x) * kTW, y0 = (blockIdx.x / tiles_x) * kTH;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wx = x0 / kWin + (warp & 3), wy = y0 / kWin + (warp >> 2);
+    const int x0 = (blockIdx.x % tiles_x) * kWT, y0 = (blockIdx.x / tiles_x) * kWT;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int c = tid & (kWT - 1), r0 = (tid >> 6) * kWin;  // tile column, first tile row
+    const int wx = (x0 + c) / kWin, wy = (y0 + r0) / kWin;
     const bool inside = wx < ww && wy < wh;
-    const int c = (warp & 3) * kWin + (lane & 15), r0 = (warp >> 2) * kWin + (lane >> 4) * 8;  // tile coordinates
     const int x = x0 + c;
     const bool gx_on = x > 0 && x < w - 1;
-    int fr[8], mr[8];
-    long long src_f = 0, src_m = 0, src_jxx = 0, src_jyy = 0, src_jxy = 0;
+    int fr[kWin], mr[kWin];
+    unsigned long long src_f = 0, src_m = 0, src_xx = 0, src_yy = 0;
+    long long src_xy = 0;
     for (int p = 0; p <= J.nenc; p++) {
         const uint16_t *plane = p == 0 ? J.yr : J.yd[p - 1];
         __syncthreads();
-        load_region(sm.y, plane, w, h, J.up, x0, y0);
+        stage_window_region(sm, plane, w, h, J.up, x0, y0);
         __syncthreads();
-        horizontal_sums(sm);
+        window_horizontal_sums(sm);
         __syncthreads();
-        int s3[10], s3l[8], s3r[8], s9[8];
-        column_s3<10>(sm, c, 0, r0 - 1, s3);
-        column_s3<8>(sm, c, -1, r0, s3l);
-        column_s3<8>(sm, c, 1, r0, s3r);
-        column_s9(sm, c, r0, s9);
-        int fine_sq = 0, jxx = 0, jyy = 0, jxy = 0, fine_x = 0;
-        long long mid_sq = 0, mid_x = 0;
+        // tile row t is region row t + 4; h3 column c + 1 is centred at x, c and c + 2 at x -+ 1
+        auto h3c = [&](int t) { return (int)sm.h3[t + kM][c + 1]; };
+        auto h3l = [&](int t) { return (int)sm.h3[t + kM][c]; };
+        auto h3r = [&](int t) { return (int)sm.h3[t + kM][c + 2]; };
+        auto h9c = [&](int t) { return (int)sm.h9[t + kM][c]; };
+        int s3_prev = h3c(r0 - 2) + h3c(r0 - 1) + h3c(r0);      // S3 at row r0 - 1
+        int s3 = s3_prev - h3c(r0 - 2) + h3c(r0 + 1);            // S3 at row r0
+        int s3l = h3l(r0 - 1) + h3l(r0) + h3l(r0 + 1), s3r = h3r(r0 - 1) + h3r(r0) + h3r(r0 + 1);
+        int s9 = 0;
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int y = y0 + r0 + i;
-            const int f = 9 * (int)sm.y[r0 + i + kM][c + kM] - s3[i + 1], m = 9 * s3[i + 1] - s9[i];
-            const int gx = gx_on ? s3r[i] - s3l[i] : 0;
-            const int gy = (y > 0 && y < h - 1) ? s3[i + 2] - s3[i] : 0;
+        for (int k = -4; k <= 4; k++) s9 += h9c(r0 + k);
+        unsigned fine_sq = 0, jxx = 0, jyy = 0;
+        int jxy = 0, fine_x = 0;
+        unsigned long long mid_sq = 0;
+        long long mid_x = 0;
+#pragma unroll
+        for (int i = 0; i < kWin; i++) {
+            const int t = r0 + i, y = y0 + t;
+            const int s3_next = s3 - h3c(t - 1) + h3c(t + 2);
+            const int f = 9 * (int)sm.y[t + kM][c + kM] - s3, m = 9 * s3 - s9;
+            const int gx = gx_on ? s3r - s3l : 0;
+            const int gy = (y > 0 && y < h - 1) ? s3_next - s3_prev : 0;
             if (p == 0) {
                 fr[i] = f;
                 mr[i] = m;
@@ -175,29 +262,37 @@ __global__ void __launch_bounds__(256) window_stats_kernel(const __grid_constant
                 fine_x += f * fr[i];
                 mid_x += (long long)m * mr[i];
             }
-            fine_sq += f * f;
-            mid_sq += (long long)m * m;
-            jxx += gx * gx;
-            jyy += gy * gy;
+            fine_sq += (unsigned)(f * f);
+            mid_sq += (unsigned long long)((long long)m * m);
+            jxx += (unsigned)(gx * gx);
+            jyy += (unsigned)(gy * gy);
             jxy += gx * gy;
+            if (i + 1 < kWin) {
+                s3_prev = s3;
+                s3 = s3_next;
+                s3l += h3l(t + 2) - h3l(t - 1);
+                s3r += h3r(t + 2) - h3r(t - 1);
+                s9 += h9c(t + 5) - h9c(t - 4);
+            }
         }
-        const long long sf = warp_sum((long long)fine_sq), sm2 = warp_sum(mid_sq), sxx = warp_sum((long long)jxx),
-                        syy = warp_sum((long long)jyy), sxy = warp_sum((long long)jxy);
+        const unsigned long long sf = half_warp_sum((unsigned long long)fine_sq), sm2 = half_warp_sum(mid_sq),
+                                 sxx = half_warp_sum((unsigned long long)jxx), syy = half_warp_sum((unsigned long long)jyy);
+        const long long sxy = half_warp_sum((long long)jxy);
         if (p == 0) {
-            src_f = sf; src_m = sm2; src_jxx = sxx; src_jyy = syy; src_jxy = sxy;
+            src_f = sf; src_m = sm2; src_xx = sxx; src_yy = syy; src_xy = sxy;
             continue;
         }
-        const long long cf = warp_sum((long long)fine_x), cm = warp_sum(mid_x);
-        if (inside && lane == 0) {
+        const long long cf = half_warp_sum((long long)fine_x), cm = half_warp_sum(mid_x);
+        if (inside && (lane & 15) == 0) {
             float *o = J.stats[p - 1] + ((size_t)wy * ww + wx) * 8;
-            o[0] = exact_ratio(src_f, 81.0);
-            o[1] = exact_ratio(src_m, 6561.0);
-            o[2] = exact_ratio(sf, 81.0);
-            o[3] = exact_ratio(sm2, 6561.0);
+            o[0] = exact_ratio((long long)src_f, 81.0);
+            o[1] = exact_ratio((long long)src_m, 6561.0);
+            o[2] = exact_ratio((long long)sf, 81.0);
+            o[3] = exact_ratio((long long)sm2, 6561.0);
             o[4] = exact_ratio(cf, 81.0);
             o[5] = exact_ratio(cm, 6561.0);
-            o[6] = oriented_of(src_jxx, src_jyy, src_jxy);
-            o[7] = oriented_of(sxx, syy, sxy);
+            o[6] = oriented_of((long long)src_xx, (long long)src_yy, src_xy);
+            o[7] = oriented_of((long long)sxx, (long long)syy, sxy);
         }
     }
 }
@@ -554,7 +649,7 @@ cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s)
 {
     const int ww = j.w / kWin, wh = j.h / kWin;
     if (ww <= 0 || wh <= 0 || j.nenc <= 0) return cudaSuccess;
-    const int blocks = ((ww + 3) / 4) * ((wh + 1) / 2);
+    const int blocks = ((ww + 3) / 4) * ((wh + 3) / 4);
     LaunchTimer t("window_stats", s);
     window_stats_kernel<<<blocks, 256, 0, s>>>(j);
     return after_launch();

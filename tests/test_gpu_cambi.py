@@ -34,6 +34,20 @@ def stripes(w, h, v0=120, period=10):
     return (v0 + ((xx // period) % 2)).astype(np.uint16)
 
 
+def plateaus(w, h, size=4, seed=11):
+    """size x size plateaus of 10-bit values 60 .. 559 (a seeded permutation, block (bx, by) takes entry bx + 16 by
+    mod 500): the 16 x 16 plateaus of an aligned 64 x 64 tile all differ, so with a window of 65 a tile has more than
+    255 codes whose c-values are needed, more than a byte of ranks can hold."""
+    perm = np.random.default_rng(seed).permutation(500) + 60
+    by, bx = np.mgrid[0:(h + size - 1) // size, 0:(w + size - 1) // size]
+    b = perm[(bx + 16 * by) % 500]
+    return np.kron(b, np.ones((size, size), np.int64))[:h, :w].astype(np.uint16)
+
+
+def test_plateaus_hold_more_than_255_codes_in_one_tile():
+    assert len(np.unique(plateaus(320, 256)[64:128, 64:128])) > 255
+
+
 CASES = [
     # (name, image, depth, params override)
     ("banded-1080-like", lambda: banded(320, 180, 1, step=2), 10, {"window": 33}),
@@ -46,6 +60,7 @@ CASES = [
     ("tiny", lambda: banded(7, 5, 7), 10, None),
     ("window65", lambda: banded(400, 260, 8, step=2), 10, {"window": 65}),
     ("derived", lambda: banded(640, 360, 9, step=1, grain=0.2), 10, None),
+    ("plateaus-many-ranks", lambda: plateaus(320, 256), 10, {"window": 65}),
 ]
 
 
