@@ -55,15 +55,16 @@ def scale_pixels(w: int, h: int) -> list[int]:
     return out
 
 
-def algorithmic_bytes(name: str, wl: dict) -> float | None:
-    """Bytes a launch of `name` must move at least: inputs read once, outputs written once (per launch)."""
+def algorithmic_bytes(name: str, wl: dict, pics: int = 1) -> float | None:
+    """Bytes a launch of `name` must move at least: inputs read once, outputs written once (per launch). `pics` is the
+    number of pictures one CAMBI launch covers (1 in the plain form, every picture of the step in the batched one)."""
     w, h, e = wl["w"], wl["h"], wl["n_enc"]
     n, windows = w * h, (w // 16) * (h // 16)
     sp = scale_pixels(w, h)
     table = {
-        "cambi_cvalues": 2.0 * sum(sp),                      # one picture's 5 scale planes (16-bit words)
-        "cambi_prep0": 2.0 * n + 2.0 * n,                    # plane in, scale-0 words out
-        "cambi_decimate_mode": 4.0 * sum(sp[1:]) / 4,        # mean over the 4 scale launches
+        "cambi_cvalues": 2.0 * sum(sp) * pics,               # the pictures' 5 scale planes (16-bit words)
+        "cambi_prep0": (2.0 * n + 2.0 * n) * pics,           # plane in, scale-0 words out
+        "cambi_decimate_mode": 4.0 * sum(sp[1:]) / 4 * pics, # mean over the 4 scale launches
         "window_stats": 2.0 * n * (1 + e) + 32.0 * windows * e,
         "persist_stats": 2.0 * n * (2 + 4 + 2 + e) + 20.0 * windows * e,
         "pair_sums": 3.0 * n * (1 + e),
@@ -313,54 +314,107 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident leg -----------------------------------------------------------------------------------
-    fr = es_b200.Frame(module, w, h, pd, n_enc)
-    acc = [es_b200.new_accum() for _ in range(n_enc)]
-    f = 0
-    with torch.cuda.stream(stream):
-        sh = stream.cuda_stream
-        for _ in range(args.warmup):
-            p = dev_pool[f % len(dev_pool)]
-            fr.queue(f, p[0][1], [x[1] for x in p[1:]], sh)
-            fr.collect(f, acc, acc)
-            f += 1
-        barrier()
-        torch.cuda.synchronize()
-        clocks = Clocks(local)
-        clocks.start()
-        time.sleep(0.25)
-        launches0 = es_b200.launch_count()
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        first = f
-        for k in range(args.steps):
-            p = dev_pool[f % len(dev_pool)]
-            fr.queue(f, p[0][1], [x[1] for x in p[1:]], sh)
-            if k > 0:
-                fr.collect(f - 1, acc, acc)
-            f += 1
-        fr.collect(f - 1, acc, acc)
-        end.record(stream)
-        end.synchronize()
-        launches = es_b200.launch_count() - launches0
-        clk = clocks.stop()
-    ms = start.elapsed_time(end)
-    ms = max_over_ranks(ms)
+    # ---- device-resident legs: the plain form (es_frame) and the batched form (es_batch, CUDA graphs) -------------
+    class PlainForm:
+        name = "plain (es_frame queue/collect, one launch set per picture, CAMBI on per-picture streams)"
+
+        def __init__(self):
+            self.fr = es_b200.Frame(module, w, h, pd, n_enc)
+
+        def queue(self, f, pics, sh):
+            self.fr.queue(f, pics[0], pics[1:], sh)
+
+        def collect(self, f, acc):
+            self.fr.collect(f, acc, acc)
+
+        def close(self):
+            self.fr.close()
+
+    class BatchedForm:
+        name = "batched (es_batch: one launch per stage for all pictures, steps replayed from CUDA graphs)"
+
+        def __init__(self):
+            self.b = es_b200.Batch(module, [(w, h, pd, n_enc)])
+
+        def queue(self, f, pics, sh):
+            self.b.queue(f, pics, sh)
+
+        def collect(self, f, acc):
+            self.b.collect(f, acc, acc)
+
+        def close(self):
+            self.b.close()
+
+    def time_form(form, f0: int) -> tuple[float, int, dict | None, int]:
+        """Warm-up, then args.steps timed steps of `form` over the device pool; returns (ms, launches, clocks, next f).
+        The warm-up covers the first 14 frames, so the batched form replays graphs in the timed region."""
+        acc = [es_b200.new_accum() for _ in range(n_enc)]
+        f = f0
+        with torch.cuda.stream(stream):
+            sh = stream.cuda_stream
+            for _ in range(max(args.warmup, 15)):
+                p = dev_pool[f % len(dev_pool)]
+                form.queue(f, [x[1] for x in p], sh)
+                form.collect(f, acc)
+                f += 1
+            barrier()
+            torch.cuda.synchronize()
+            clocks = Clocks(local)
+            clocks.start()
+            time.sleep(0.25)
+            launches0 = es_b200.launch_count()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            for k in range(args.steps):
+                p = dev_pool[f % len(dev_pool)]
+                form.queue(f, [x[1] for x in p], sh)
+                if k > 0:
+                    form.collect(f - 1, acc)
+                f += 1
+            form.collect(f - 1, acc)
+            end.record(stream)
+            end.synchronize()
+            launches = es_b200.launch_count() - launches0
+            clk = clocks.stop()
+        return max_over_ranks(start.elapsed_time(end)), launches, clk, f
+
     pairs = args.steps * n_enc * world
-    value = pairs / (ms / 1000.0)
-    assert f - first == args.steps
+    forms = {}
+    plain = PlainForm()
+    ms_plain, launches_plain, clk_plain, f = time_form(plain, 0)
+    forms["plain"] = {"value": pairs / (ms_plain / 1000.0), "ms_per_step": ms_plain / args.steps, "form": plain.name,
+                      "gpu_launches": int(launches_plain)}
+    plain.close()
+    batched = BatchedForm()
+    ms_b, launches_b, clk, _ = time_form(batched, 0)
+    batched.close()
+    forms["batched"] = {"value": pairs / (ms_b / 1000.0), "ms_per_step": ms_b / args.steps, "form": batched.name,
+                        "gpu_launches": int(launches_b)}
+    head = "batched"
+    ms, launches = ms_b, launches_b
+    value = forms[head]["value"]
 
     # ---- per-kernel leg: one pass over the pool with every kernel alone on the stream, each bracketed by events -
-    # (in the timed region the pictures' CAMBI streams overlap, so an event pair there would also time its neighbours)
-    es_b200.kernel_timing(True, serial=True)
+    # (in the timed region kernels of a step overlap, so an event pair there would also time its neighbours; kernel
+    # timing also switches graph replay off, so each kernel is launched and timed on its own)
+    kform = BatchedForm() if head == "batched" else PlainForm()
+    kacc = [es_b200.new_accum() for _ in range(n_enc)]
     with torch.cuda.stream(stream):
+        kf = 0
+        for _ in range(14):
+            p = dev_pool[kf % len(dev_pool)]
+            kform.queue(kf, [x[1] for x in p], stream.cuda_stream)
+            kform.collect(kf, kacc)
+            kf += 1
+        es_b200.kernel_timing(True, serial=True)
         for _ in range(len(dev_pool)):
-            p = dev_pool[f % len(dev_pool)]
-            fr.queue(f, p[0][1], [x[1] for x in p[1:]], stream.cuda_stream)
-            fr.collect(f, acc, acc)
-            f += 1
+            p = dev_pool[kf % len(dev_pool)]
+            kform.queue(kf, [x[1] for x in p], stream.cuda_stream)
+            kform.collect(kf, kacc)
+            kf += 1
     times = es_b200.kernel_times()
     es_b200.kernel_timing(False)
+    kform.close()
     kernel_steps = len(dev_pool)
 
     # ---- end-to-end leg: host frames, copies inside the timed region ------------------------------------------
@@ -378,7 +432,7 @@ def main() -> None:
         h2d = sum(t.numel() * t.element_size() for pic in host_pool[0] for t in pic)
         windows = (w // 16) * (h // 16)
         d2h = 8 * (3 * n_enc + 3 * (n_enc + 1)) + 136 * n_enc + 2 * 6 * windows * n_enc + 48 * (1 + n_enc)
-        fr2 = es_b200.Frame(module, w, h, pd, n_enc)
+        fr2 = BatchedForm() if head == "batched" else PlainForm()
         acc2 = [es_b200.new_accum() for _ in range(n_enc)]
         copy_stream = torch.cuda.Stream()
         copied = [torch.cuda.Event() for _ in range(2)]
@@ -394,24 +448,25 @@ def main() -> None:
                         d.copy_(hsrc, non_blocking=True)
                 copied[s].record(copy_stream)
             stream.wait_event(copied[s])
-            fr2.queue(g, views[s][0], views[s][1:], stream.cuda_stream)
+            fr2.queue(g, views[s], stream.cuda_stream)
             free[s].record(stream)
             if collect_prev:
-                fr2.collect(g - 1, acc2, acc2)
+                fr2.collect(g - 1, acc2)
 
         with torch.cuda.stream(stream):
-            for g in range(args.warmup):
+            warm = max(args.warmup, 15)
+            for g in range(warm):
                 e2e_step(g, g > 0)
-            fr2.collect(args.warmup - 1, acc2, acc2)
+            fr2.collect(warm - 1, acc2)
             barrier()
             torch.cuda.synchronize()
             t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t_start.record(stream)
             copy_stream.wait_event(t_start)
-            g0 = args.warmup
+            g0 = warm
             for k in range(args.steps):
                 e2e_step(g0 + k, k > 0)
-            fr2.collect(g0 + args.steps - 1, acc2, acc2)
+            fr2.collect(g0 + args.steps - 1, acc2)
             t_end.record(stream)
             t_end.synchronize()
         e2e_ms = max_over_ranks(t_start.elapsed_time(t_end))
@@ -426,10 +481,10 @@ def main() -> None:
     peaks = read_peaks()
     if top:
         per_launch_ms = times[top][0] / times[top][1]
-        alg = algorithmic_bytes(top, wl)
+        alg = algorithmic_bytes(top, wl, pics=(1 + n_enc) if head == "batched" else 1)
         achieved = alg / (per_launch_ms / 1000.0) / 1e9 if alg else None
         roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": read_traffic(top, args.workload),
+                    "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": read_traffic(top, f"{args.workload}:{head}"),
                     "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "peak_source": peaks["source"]}
     kernels = {k: {"ms_per_step": v[0] / kernel_steps, "launches_per_step": v[1] / kernel_steps, "share": v[0] / total_kernel_ms}
                for k, v in sorted(times.items(), key=lambda kv: -kv[1][0])}
@@ -446,7 +501,6 @@ def main() -> None:
         cpu = {"value": statistics.median(v for v, _ in vals), "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "3 rounds of " + vals[-1][1]}
 
-    fr.close()
     module.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -454,9 +508,9 @@ def main() -> None:
                 "dtype": "u16/int64", "data": "synthetic (seeded es_synth frames, no video decode)",
                 "config": {"workload": wl["desc"], "frame_pairs_per_step": n_enc, "pool_steps": args.pool,
                            "l2": "inputs larger than L2: 6 distinct steps of ~100 MB input each cycled",
-                           "form": "plain (es_frame queue/collect, one launch set per picture)", "parallelism": f"replicas x{world}"},
+                           "form": forms[head]["form"], "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
-                "kernels": kernels}
+                "forms": forms, "kernels": kernels}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -1,0 +1,594 @@
+// es_batch: the per-frame measures of several sources at once, each with its own encodes, picture size and depth.
+//
+// The reference scores one source per process, with one launch per kernel and picture and a host round trip per
+// top-k radix round (src/main.cpp:518-643, src/cambi.cpp:88-184). Here a frame step of every source is one launch per
+// stage for all pictures: unpacking, scale 0, the decimation of each scale, the c-values of every scale of every
+// picture, the top-k rounds of every slot and the scores form one chain; PSNR / color, window figures, lasting texture
+// and the per-frame reduction of every source form a second chain that runs beside it. Once a source's rings are full
+// (frame 14 on), a step is replayed from a CUDA graph captured per ring phase, so queueing a step costs one small copy
+// of the input addresses and one graph launch.
+//
+// Per source the device state is that of es_frame (luma rings, running texture sums, structure masks, figures); per
+// picture the CAMBI state is one word plane and one positive c-value list per scale. The figures of step f are copied
+// to page-locked memory indexed by f % 2, so collect(f) reads them while step f + 1 runs.
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "es_internal.h"
+
+using namespace es;
+
+namespace {
+constexpr int kRing = 14, kEncRing = 7, kRadius = 6, kStats = 8, kPersist = 5, kBinArrays = 6;
+constexpr int kMaxBatchPictures = kMaxJobs / kScales;  // c-value jobs of one launch
+
+struct Source {
+    int w = 0, h = 0, pd = 10, nenc = 0, ww = 0, wh = 0, windows = 0;
+    size_t n = 0, slot = 0;
+    int picture = 0;  // index of its own picture; its encodes' pictures follow
+    DeviceBuffer<uint16_t> src_ring, src_u, src_v;
+    std::vector<std::unique_ptr<DeviceBuffer<uint16_t>>> enc_ring, enc_u, enc_v;
+    DeviceBuffer<uint16_t> run_e[2], run_o[2];
+    DeviceBuffer<float> stats[2], persist[2];
+    DeviceBuffer<uint8_t> masks;
+    DeviceBuffer<unsigned long long> sums[2];
+    DeviceBuffer<FrameFigures> figs[2];
+    DeviceBuffer<uint16_t> bins[2];
+    DeviceBuffer<float> threshold;
+    DeviceBuffer<double> partials;
+    PinnedBuffer<unsigned long long> h_sums[2];
+    PinnedBuffer<FrameFigures> h_figs[2];
+    PinnedBuffer<uint16_t> h_bins[2];
+    uint16_t *src_plane(long f) const { return src_ring.ptr + (size_t)(f % kRing) * slot; }
+    uint16_t *enc_plane(int e, long f) const { return enc_ring[e]->ptr + (size_t)(f % kEncRing) * slot; }
+};
+
+struct Picture {
+    int source = 0, encode = -1;  // encode -1: the source's own picture
+    int w = 0, h = 0, depth = 10;
+    es_cambi_params p{};
+    int sw[kScales], sh[kScales];
+    DeviceBuffer<uint16_t> words[kScales];
+    DeviceBuffer<float> lists[kScales];
+};
+}  // namespace
+
+struct es_batch {
+    std::vector<std::unique_ptr<Source>> sources;
+    std::vector<std::unique_ptr<Picture>> pictures;
+    int max_pad = 0;
+    DeviceBuffer<CvSlot> slots;  // pictures x kScales
+    DeviceBuffer<unsigned long long> slot_n, slot_k;
+    DeviceBuffer<float> lut;
+    DeviceBuffer<double> scores;  // pictures x (1 + kScales): score, then pooled per scale
+    PinnedBuffer<double> h_scores[2];
+    DeviceBuffer<UnpackView> views;
+    PinnedBuffer<UnpackView> h_views[2];
+    Stream main, side;
+    Event start, fork, join, done[2];
+    bool use_graphs = true;
+    std::map<std::pair<int, uint32_t>, cudaGraphExec_t> graphs;  // (ring phase, skipped sources) -> step
+    uint32_t skipped[2] = {0, 0};
+    long queued[2] = {-1, -1};
+    long next = 0, last_collected = -1;
+    uint64_t graph_launches = 0;
+
+    ~es_batch()
+    {
+        for (auto &g : graphs) cudaGraphExecDestroy(g.second);
+    }
+    int encode_picture(int s, int e) const { return sources[s]->picture + 1 + e; }
+};
+
+namespace {
+
+void check_view(const es_frame_view &v, int pd, const char *what)
+{
+    require(v.y != nullptr && v.u != nullptr && (v.semi || v.v != nullptr), std::string(what) + ": missing plane");
+    require(v.bytes == 1 || v.bytes == 2, std::string(what) + ": samples must be 1 or 2 bytes");
+    require(v.depth == 8 || v.depth == 10, std::string(what) + ": depth must be 8 or 10");
+    require(v.depth <= pd, std::string(what) + ": deeper than the pipeline");
+    require(v.shift >= 0 && v.shift < 16, std::string(what) + ": bad shift");
+}
+
+void init_source(Source &S, const es_batch_source &d)
+{
+    S.w = d.w;
+    S.h = d.h;
+    S.pd = d.pd;
+    S.nenc = d.n_encodes;
+    S.n = (size_t)d.w * d.h;
+    S.slot = (S.n + 127) & ~(size_t)127;
+    S.ww = d.w / kWin;
+    S.wh = d.h / kWin;
+    S.windows = S.ww * S.wh;
+    const size_t n = S.n, cn = n / 4, win = (size_t)S.windows;
+    S.src_ring.reset(S.slot * kRing);
+    S.src_u.reset(cn);
+    S.src_v.reset(cn);
+    for (int e = 0; e < S.nenc; e++) {
+        S.enc_ring.push_back(std::make_unique<DeviceBuffer<uint16_t>>(S.slot * kEncRing));
+        S.enc_u.push_back(std::make_unique<DeviceBuffer<uint16_t>>(cn));
+        S.enc_v.push_back(std::make_unique<DeviceBuffer<uint16_t>>(cn));
+    }
+    for (int i = 0; i < 2; i++) {
+        S.run_e[i].reset(n);
+        S.run_o[i].reset(n);
+        cuda_check(cudaMemset(S.run_e[i].ptr, 0, n * 2), "clearing");
+        cuda_check(cudaMemset(S.run_o[i].ptr, 0, n * 2), "clearing");
+        S.stats[i].reset(std::max<size_t>(1, win * kStats * S.nenc));
+        S.persist[i].reset(std::max<size_t>(1, win * kPersist * S.nenc));
+        S.sums[i].reset((size_t)3 * S.nenc + 3 * (S.nenc + 1));
+        S.figs[i].reset(S.nenc);
+        S.bins[i].reset(std::max<size_t>(1, win * kBinArrays * S.nenc));
+        S.h_sums[i].reset(S.sums[i].count);
+        S.h_figs[i].reset(S.nenc);
+        S.h_bins[i].reset(S.bins[i].count);
+        std::memset(S.h_figs[i].ptr, 0, sizeof(FrameFigures) * S.nenc);
+    }
+    S.threshold.reset(1);
+    S.partials.reset(std::max<size_t>(1, (size_t)S.nenc * collect_blocks(S.windows) * kCollectSums));
+    S.masks.reset(std::max<size_t>(1, win * kEncRing));
+    cuda_check(cudaMemset(S.masks.ptr, 0, S.masks.bytes()), "clearing");
+}
+
+void init_cambi(es_batch &b)
+{
+    const int P = (int)b.pictures.size();
+    std::vector<unsigned long long> n(P * kScales), k(P * kScales);
+    std::vector<CvSlot> init(P * kScales);
+    std::memset(init.data(), 0, sizeof(CvSlot) * init.size());
+    for (int i = 0; i < P; i++) {
+        Picture &pic = *b.pictures[i];
+        pic.sw[0] = pic.w;
+        pic.sh[0] = pic.h;
+        for (int s = 1; s < kScales; s++) {
+            pic.sw[s] = (pic.sw[s - 1] + 1) >> 1;
+            pic.sh[s] = (pic.sh[s - 1] + 1) >> 1;
+        }
+        for (int s = 0; s < kScales; s++) {
+            const size_t m = (size_t)pic.sw[s] * pic.sh[s];
+            pic.words[s].reset(m);
+            pic.lists[s].reset(m);
+            n[i * kScales + s] = m;
+            k[i * kScales + s] = topk_count(m, pic.p.topk);
+            init[i * kScales + s].list = pic.lists[s].ptr;
+        }
+        b.max_pad = std::max(b.max_pad, pic.p.pad);
+    }
+    b.slots.reset(init.size());
+    b.slot_n.reset(n.size());
+    b.slot_k.reset(k.size());
+    cuda_check(cudaMemcpy(b.slots.ptr, init.data(), sizeof(CvSlot) * init.size(), cudaMemcpyHostToDevice), "batch set-up");
+    cuda_check(cudaMemcpy(b.slot_n.ptr, n.data(), n.size() * 8, cudaMemcpyHostToDevice), "batch set-up");
+    cuda_check(cudaMemcpy(b.slot_k.ptr, k.data(), k.size() * 8, cudaMemcpyHostToDevice), "batch set-up");
+    const size_t lut_n = (size_t)(2 * b.max_pad + 1) * (2 * b.max_pad + 1) + 1;
+    std::vector<float> lut(lut_n);
+    reciprocal_table(b.max_pad, lut.data(), lut_n);
+    b.lut.reset(lut_n);
+    cuda_check(cudaMemcpy(b.lut.ptr, lut.data(), lut_n * 4, cudaMemcpyHostToDevice), "batch set-up");
+    b.scores.reset((size_t)P * (1 + kScales));
+    for (int i = 0; i < 2; i++) {
+        b.h_scores[i].reset((size_t)P * (1 + kScales));
+        std::memset(b.h_scores[i].ptr, 0, sizeof(double) * P * (1 + kScales));
+        b.h_views[i].reset(P);
+    }
+    b.views.reset(P);
+}
+
+uint16_t *luma_of(const es_batch &b, int picture, long f)
+{
+    const Picture &pic = *b.pictures[picture];
+    const Source &S = *b.sources[pic.source];
+    return pic.encode < 0 ? S.src_plane(f) : S.enc_plane(pic.encode, f);
+}
+
+// The CAMBI chain of step f for the pictures whose CAMBI runs, on stream s.
+void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
+{
+    std::vector<int> run;
+    for (int i = 0; i < (int)b.pictures.size(); i++) {
+        const Picture &pic = *b.pictures[i];
+        if (pic.encode >= 0 || !((skip >> pic.source) & 1u)) run.push_back(i);
+    }
+    if (run.empty()) return;
+    Prep0Batch pb{};
+    int tiles = 0;
+    for (int i : run) {
+        const Picture &pic = *b.pictures[i];
+        Prep0Job &j = pb.job[pb.njobs++];
+        j.img = luma_of(b, i, f);
+        j.pitch = pic.w;
+        j.w = pic.w;
+        j.h = pic.h;
+        j.depth = pic.depth;
+        j.mask_index = pic.p.mask_index;
+        j.word = pic.words[0].ptr;
+        j.tiles_x = (pic.w + 63) / 64;
+        j.first_tile = tiles;
+        tiles += j.tiles_x * ((pic.h + 31) / 32);
+    }
+    pb.total_tiles = tiles;
+    cuda_check(launch_prep0(pb, s), "batch scale 0");
+    const int nslots = (int)b.pictures.size() * kScales;
+    cuda_check(launch_slots_reset(b.slots.ptr, nslots, b.slot_n.ptr, b.slot_k.ptr, s), "batch reset");
+    for (int sc = 1; sc < kScales; sc++) {
+        DecBatch db{};
+        int blocks = 0;
+        for (int i : run) {
+            const Picture &pic = *b.pictures[i];
+            DecJob &dj = db.job[db.njobs++];
+            dj.src = pic.words[sc - 1].ptr;
+            dj.sw = pic.sw[sc - 1];
+            dj.sh = pic.sh[sc - 1];
+            dj.dst = pic.words[sc].ptr;
+            dj.w = pic.sw[sc];
+            dj.h = pic.sh[sc];
+            dj.first_block = blocks;
+            blocks += (dj.w * dj.h + 255) / 256;
+        }
+        db.total_blocks = blocks;
+        cuda_check(launch_decimate_mode(db, s), "batch scales");
+    }
+    CvBatch cb{};
+    tiles = 0;
+    for (int i : run) {
+        const Picture &pic = *b.pictures[i];
+        for (int sc = 0; sc < kScales; sc++) {
+            CvJob &j = cb.job[cb.njobs++];
+            j.word = pic.words[sc].ptr;
+            j.w = pic.sw[sc];
+            j.h = pic.sh[sc];
+            j.pad = pic.p.pad;
+            j.tiles_x = (j.w + kCvTX - 1) / kCvTX;
+            j.first_tile = tiles;
+            j.slot = i * kScales + sc;
+            j.plane = nullptr;
+            tiles += j.tiles_x * ((j.h + kCvTY - 1) / kCvTY);
+        }
+    }
+    cb.total_tiles = tiles;
+    cb.max_pad = b.max_pad;
+    const es_cambi_params &p0 = b.pictures[0]->p;
+    cb.band.band_base = p0.band_base;
+    cb.band.band_size = p0.band_size;
+    cb.band.vlt = p0.vlt;
+    for (int d = 0; d < kDiffs; d++) {
+        cb.band.tvi[d] = p0.tvi[d];
+        cb.band.weight[d] = p0.weight[d];
+    }
+    cb.lut = b.lut.ptr;
+    cb.slots = b.slots.ptr;
+    cuda_check(launch_cvalues(cb, s), "batch c-values");
+    static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+    for (int round = 0; round < 3; round++)
+        cuda_check(launch_select_round(b.slots.ptr, nslots, shifts[round], widths[round], s), "batch top-k");
+    cuda_check(launch_sum_above(b.slots.ptr, nslots, s), "batch top-k");
+    ScoreBatch sb{};
+    for (int i : run) {
+        ScoreJob &j = sb.job[sb.njobs++];
+        j.first_slot = i * kScales;
+        j.window = b.pictures[i]->p.window;
+        j.score = b.scores.ptr + (size_t)i * (1 + kScales);
+    }
+    sb.slots = b.slots.ptr;
+    cuda_check(launch_score(sb, s), "batch score");
+    cuda_check(cudaMemcpyAsync(b.h_scores[f % 2].ptr, b.scores.ptr, b.scores.bytes(), cudaMemcpyDeviceToHost, s),
+               "reading scores");
+}
+
+// The texture chain of step f (PSNR / color, window figures, lasting texture, reduction) for every source.
+void record_texture(es_batch &b, long f, cudaStream_t s)
+{
+    const int at = (int)(f % 2);
+    const bool texture = f >= 2 * kRadius;
+    PairSumsBatch pb{};
+    WindowBatch wb{};
+    PersistBatch qb{};
+    CollectBatch cb{};
+    for (auto &sp : b.sources) {
+        Source &S = *sp;
+        const int up = 10 - S.pd;
+        cuda_check(cudaMemsetAsync(S.sums[at].ptr, 0, S.sums[at].bytes(), s), "clearing");
+        PairSumsJob &pj = pb.job[pb.njobs++];
+        pj.ry = S.src_plane(f);
+        pj.ru = S.src_u.ptr;
+        pj.rv = S.src_v.ptr;
+        for (int e = 0; e < S.nenc; e++) {
+            pj.dy[e] = S.enc_plane(e, f);
+            pj.du[e] = S.enc_u[e]->ptr;
+            pj.dv[e] = S.enc_v[e]->ptr;
+        }
+        pj.sse = S.sums[at].ptr;
+        pj.color = S.sums[at].ptr + 3 * S.nenc;
+        pj.nenc = S.nenc;
+        pj.w = S.w;
+        pj.h = S.h;
+        pj.up = up;
+
+        WindowJob &wj = wb.job[wb.njobs++];
+        wj.yr = S.src_plane(f);
+        for (int e = 0; e < S.nenc; e++) {
+            wj.yd[e] = S.enc_plane(e, f);
+            wj.stats[e] = S.stats[at].ptr + (size_t)e * S.windows * kStats;
+        }
+        wj.nenc = S.nenc;
+        wj.w = S.w;
+        wj.h = S.h;
+        wj.up = up;
+
+        PersistJob &qj = qb.job[qb.njobs++];
+        qj.e_old = S.run_e[at ^ 1].ptr;
+        qj.o_old = S.run_o[at ^ 1].ptr;
+        qj.e_new = S.run_e[at].ptr;
+        qj.o_new = S.run_o[at].ptr;
+        qj.y_m13 = f >= 13 ? S.src_plane(f - 13) : nullptr;
+        qj.y_m7 = f >= 7 ? S.src_plane(f - 7) : nullptr;
+        qj.y_c = f >= 6 ? S.src_plane(f - 6) : nullptr;
+        qj.y_f = S.src_plane(f);
+        for (int e = 0; e < S.nenc; e++) {
+            qj.yd[e] = f >= 6 ? S.enc_plane(e, f - 6) : nullptr;
+            qj.out[e] = S.persist[at].ptr + (size_t)e * S.windows * kPersist;
+        }
+        qj.nenc = S.nenc;
+        qj.w = S.w;
+        qj.h = S.h;
+        qj.up = up;
+        qj.stats = texture ? 1 : 0;
+
+        if (S.windows > 0) {
+            CollectJob &cj = cb.job[cb.njobs++];
+            for (int e = 0; e < S.nenc; e++) {
+                cj.stats[e] = wj.stats[e];
+                cj.persist[e] = texture ? qj.out[e] : nullptr;
+                cj.fig[e] = S.figs[at].ptr + e;
+                cj.bins[e] = S.bins[at].ptr + (size_t)e * kBinArrays * S.windows;
+            }
+            cj.centre_mask = S.masks.ptr + (size_t)((f + kEncRing - kRadius) % kEncRing) * S.windows;
+            cj.mask = S.masks.ptr + (size_t)(f % kEncRing) * S.windows;
+            cj.nenc = S.nenc;
+            cj.windows = S.windows;
+            cj.threshold = S.threshold.ptr;
+            cj.partials = S.partials.ptr;
+        }
+    }
+    cuda_check(launch_pair_sums(pb, s), "batch squared errors and colors");
+    cuda_check(launch_window_stats(wb, s), "batch window figures");
+    cuda_check(launch_persist(qb, s), "batch lasting texture");
+    if (cb.njobs) cuda_check(launch_collect(cb, s), "batch collecting figures");
+    for (auto &sp : b.sources) {
+        Source &S = *sp;
+        cuda_check(cudaMemcpyAsync(S.h_sums[at].ptr, S.sums[at].ptr, S.sums[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
+        if (S.windows > 0) {
+            cuda_check(cudaMemcpyAsync(S.h_figs[at].ptr, S.figs[at].ptr, S.figs[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
+            cuda_check(cudaMemcpyAsync(S.h_bins[at].ptr, S.bins[at].ptr, S.bins[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
+        }
+    }
+}
+
+// The whole step f on b.main: unpacking, then the CAMBI chain on main beside the texture chain on side.
+void record_step(es_batch &b, long f, uint32_t skip)
+{
+    cudaStream_t s = b.main.s;
+    UnpackBatch ub{};
+    ub.views = b.views.ptr;
+    int first = 0;
+    for (int i = 0; i < (int)b.pictures.size(); i++) {
+        const Picture &pic = *b.pictures[i];
+        const Source &S = *b.sources[pic.source];
+        UnpackJob &j = ub.job[ub.njobs++];
+        j.y16 = luma_of(b, i, f);
+        j.u16 = pic.encode < 0 ? S.src_u.ptr : S.enc_u[pic.encode]->ptr;
+        j.v16 = pic.encode < 0 ? S.src_v.ptr : S.enc_v[pic.encode]->ptr;
+        j.w = S.w;
+        j.h = S.h;
+        j.pd = S.pd;
+        j.first_block = first;
+        first += (int)(((size_t)(S.w / 2) * (S.h / 2) + 255) / 256);
+    }
+    ub.total_blocks = first;
+    cuda_check(launch_unpack(ub, s), "batch unpacking");
+    const bool split = !serial_streams();
+    cudaStream_t t = split ? b.side.s : s;
+    if (split) {
+        cuda_check(cudaEventRecord(b.fork.e, s), "event");
+        cuda_check(cudaStreamWaitEvent(t, b.fork.e, 0), "event");
+    }
+    record_cambi(b, f, skip, s);
+    record_texture(b, f, t);
+    if (split) {
+        cuda_check(cudaEventRecord(b.join.e, t), "event");
+        cuda_check(cudaStreamWaitEvent(s, b.join.e, 0), "event");
+    }
+}
+
+void queue_step(es_batch &b, long f, uint32_t skip)
+{
+    const bool graph = b.use_graphs && f >= kRing && !kernel_timing_on();
+    if (!graph) {
+        record_step(b, f, skip);
+        return;
+    }
+    const auto key = std::make_pair((int)(f % kRing), skip);
+    auto it = b.graphs.find(key);
+    if (it == b.graphs.end()) {
+        cudaGraph_t g = nullptr;
+        cuda_check(cudaStreamBeginCapture(b.main.s, cudaStreamCaptureModeThreadLocal), "capturing a step");
+        try {
+            record_step(b, f, skip);
+        } catch (...) {
+            cudaStreamEndCapture(b.main.s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        cuda_check(cudaStreamEndCapture(b.main.s, &g), "capturing a step");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        cuda_check(e, "instantiating a step graph");
+        it = b.graphs.emplace(key, exec).first;
+    }
+    cuda_check(cudaGraphLaunch(it->second, b.main.s), "launching a step graph");
+    b.graph_launches++;
+}
+
+}  // namespace
+
+extern "C" {
+
+int es_batch_create(const es_module *m, int n_sources, const es_batch_source *sources, const es_batch_options *options,
+                    es_batch **out)
+{
+    return guarded([&] {
+        require(m != nullptr && sources != nullptr && out != nullptr, "es_batch_create: NULL argument");
+        require(n_sources >= 1 && n_sources <= kMaxSources, "es_batch_create: 1 to 16 sources");
+        int pictures = 0;
+        for (int i = 0; i < n_sources; i++) {
+            const es_batch_source &d = sources[i];
+            require(d.w >= 16 && d.h >= 16 && d.w % 2 == 0 && d.h % 2 == 0,
+                    "es_batch_create: every picture must be even and at least 16 x 16");
+            require(d.pd == 8 || d.pd == 10, "es_batch_create: pipeline depth must be 8 or 10");
+            require(d.n_encodes >= 1 && d.n_encodes <= kMaxEncodes, "es_batch_create: 1 to 16 encodes per source");
+            pictures += 1 + d.n_encodes;
+        }
+        require(pictures <= kMaxBatchPictures, "es_batch_create: at most 32 pictures (sources and encodes) per batch");
+        check_device();
+        auto b = std::make_unique<es_batch>();
+        if (options) b->use_graphs = options->use_graphs != 0;
+        for (int i = 0; i < n_sources; i++) {
+            auto S = std::make_unique<Source>();
+            init_source(*S, sources[i]);
+            S->picture = (int)b->pictures.size();
+            const es_cambi_params p = derive_params(sources[i].w, sources[i].h);
+            for (int e = -1; e < sources[i].n_encodes; e++) {
+                auto pic = std::make_unique<Picture>();
+                pic->source = i;
+                pic->encode = e;
+                pic->w = sources[i].w;
+                pic->h = sources[i].h;
+                pic->depth = sources[i].pd;
+                pic->p = p;
+                b->pictures.push_back(std::move(pic));
+            }
+            b->sources.push_back(std::move(S));
+        }
+        init_cambi(*b);
+        cuda_check(cudaDeviceSynchronize(), "batch set-up");
+        *out = b.release();
+    });
+}
+
+int es_batch_queue(es_batch *b, long f, const es_frame_view *views, const int *crops, const int *source_cambi,
+                   void *stream)
+{
+    return guarded([&] {
+        require(b != nullptr && views != nullptr, "es_batch_queue: NULL argument");
+        require(f == b->next, "es_batch_queue: frames must be queued in order from 0");
+        const int at = (int)(f % 2);
+        if (b->queued[at] > b->last_collected)
+            throw Error(ES_ERR_STATE, "es_batch_queue: frame " + std::to_string(b->queued[at]) + " has not been collected");
+        uint32_t skip = 0;
+        const int P = (int)b->pictures.size();
+        for (int i = 0; i < P; i++) {
+            const Picture &pic = *b->pictures[i];
+            check_view(views[i], b->sources[pic.source]->pd, pic.encode < 0 ? "source" : "encode");
+            UnpackView &u = b->h_views[at].ptr[i];
+            u.f = FrameViewDev{views[i].y, views[i].u, views[i].v, views[i].ypitch, views[i].cpitch, views[i].semi,
+                               views[i].bytes, views[i].shift, views[i].depth};
+            u.x0 = crops ? crops[2 * i] : 0;
+            u.y0 = crops ? crops[2 * i + 1] : 0;
+            require(u.x0 >= 0 && u.y0 >= 0 && u.x0 % 2 == 0 && u.y0 % 2 == 0, "es_batch_queue: crop offsets must be even and >= 0");
+        }
+        for (int s = 0; s < (int)b->sources.size(); s++)
+            if (source_cambi && !source_cambi[s]) skip |= 1u << s;
+        cudaStream_t caller = (cudaStream_t)stream;
+        cuda_check(cudaEventRecord(b->start.e, caller), "event");
+        cuda_check(cudaStreamWaitEvent(b->main.s, b->start.e, 0), "event");
+        cuda_check(cudaMemcpyAsync(b->views.ptr, b->h_views[at].ptr, sizeof(UnpackView) * P, cudaMemcpyHostToDevice, b->main.s),
+                   "input addresses");
+        queue_step(*b, f, skip);
+        cuda_check(cudaEventRecord(b->done[at].e, b->main.s), "event");
+        cuda_check(cudaStreamWaitEvent(caller, b->done[at].e, 0), "event");
+        b->skipped[at] = skip;
+        b->queued[at] = f;
+        b->next = f + 1;
+    });
+}
+
+int es_batch_collect(es_batch *b, long f, const double *cached_source_cambi, es_accum *const *frame_acc,
+                     es_accum *const *centre_acc, es_frame_result *out)
+{
+    return guarded([&] {
+        require(b != nullptr, "es_batch_collect: NULL batch");
+        const int at = (int)(f % 2);
+        if (b->queued[at] != f) throw Error(ES_ERR_STATE, "es_batch_collect: frame " + std::to_string(f) + " was not queued");
+        if (f <= b->last_collected) throw Error(ES_ERR_STATE, "es_batch_collect: frame collected twice");
+        cuda_check(cudaEventSynchronize(b->done[at].e), "waiting for a frame step");
+        const bool texture = f >= 2 * kRadius;
+        const double *sc = b->h_scores[at].ptr;
+        int k = 0;
+        for (int s = 0; s < (int)b->sources.size(); s++) {
+            const Source &S = *b->sources[s];
+            double source_banding;
+            if ((b->skipped[at] >> s) & 1u) {
+                require(cached_source_cambi != nullptr, "es_batch_collect: a source's CAMBI was skipped and no cached value given");
+                source_banding = cached_source_cambi[s];
+            } else {
+                source_banding = sc[(size_t)S.picture * (1 + kScales)];
+            }
+            const unsigned long long *sse = S.h_sums[at].ptr, *color = sse + 3 * S.nenc, *scol = color + 3 * S.nenc;
+            for (int e = 0; e < S.nenc; e++, k++) {
+                const double banding = sc[(size_t)b->encode_picture(s, e) * (1 + kScales)];
+                const es_frame_result res = collect_encode(
+                    EncodeFigures{banding, source_banding, sse + 3 * e, scol, color + 3 * e, S.n, S.pd, S.windows,
+                                  &S.h_figs[at].ptr[e], S.h_bins[at].ptr + (size_t)e * kBinArrays * S.windows, texture},
+                    frame_acc ? frame_acc[k] : nullptr, centre_acc ? centre_acc[k] : nullptr);
+                if (out) out[k] = res;
+            }
+        }
+        b->last_collected = f;
+    });
+}
+
+int es_batch_read_windows(es_batch *b, int source, int encode, float *stats, float *persist)
+{
+    return guarded([&] {
+        require(b != nullptr, "es_batch_read_windows: NULL batch");
+        require(source >= 0 && source < (int)b->sources.size(), "es_batch_read_windows: source out of range");
+        const Source &S = *b->sources[source];
+        require(encode >= 0 && encode < S.nenc, "es_batch_read_windows: encode out of range");
+        if (b->last_collected < 0) throw Error(ES_ERR_STATE, "es_batch_read_windows: no frame collected");
+        const int at = (int)(b->last_collected % 2);
+        const size_t win = (size_t)S.windows;
+        if (stats && win)
+            cuda_check(cudaMemcpy(stats, S.stats[at].ptr + (size_t)encode * win * kStats, win * kStats * 4, cudaMemcpyDeviceToHost), "reading");
+        if (persist && win) {
+            require(b->last_collected >= 2 * kRadius, "es_batch_read_windows: no lasting texture before frame 12");
+            cuda_check(cudaMemcpy(persist, S.persist[at].ptr + (size_t)encode * win * kPersist, win * kPersist * 4, cudaMemcpyDeviceToHost), "reading");
+        }
+    });
+}
+
+int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5])
+{
+    return guarded([&] {
+        require(b != nullptr && pooled != nullptr, "es_batch_scale_pooled: NULL argument");
+        require(picture >= 0 && picture < (int)b->pictures.size(), "es_batch_scale_pooled: picture out of range");
+        if (b->last_collected < 0) throw Error(ES_ERR_STATE, "es_batch_scale_pooled: no frame collected");
+        const double *sc = b->h_scores[b->last_collected % 2].ptr + (size_t)picture * (1 + kScales);
+        for (int s = 0; s < kScales; s++) pooled[s] = sc[1 + s];
+    });
+}
+
+uint64_t es_batch_graph_launches(const es_batch *b) { return b ? b->graph_launches : 0; }
+
+void es_batch_destroy(es_batch *b)
+{
+    if (!b) return;
+    cudaDeviceSynchronize();
+    delete b;
+}
+
+}  // extern "C"

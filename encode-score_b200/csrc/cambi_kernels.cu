@@ -170,43 +170,47 @@ __global__ void slots_reset_kernel(CvSlot *slots, int nslots, const unsigned lon
     }
 }
 
-__global__ void __launch_bounds__(256) select_hist_kernel(CvSlot *slots, int shift, int width)
+// One radix round over every slot whose positive count exceeds k; block b takes the b-th share of each such slot's list.
+__global__ void __launch_bounds__(256) select_hist_kernel(CvSlot *slots, int nslots, int shift, int width)
 {
-    CvSlot &S = slots[blockIdx.y];
-    if (S.count <= S.k) return;
     __shared__ unsigned hist[2048];
     const int nb = 1 << width;
-    for (int i = threadIdx.x; i < nb; i += 256) hist[i] = 0;
-    __syncthreads();
-    const unsigned *v = (const unsigned *)S.list;
-    const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
-    const unsigned mask = S.mask, prefix = S.prefix;
-    // neighbouring c-values of the list are often equal (they come from the same tile), so each thread adds runs of
-    // equal digits at once; 4 values per 16-byte load
-    unsigned last = 0, run = 0;
-    auto add = [&](unsigned bits) {
-        if ((bits & mask) != prefix) return;
-        const unsigned d = (bits >> shift) & (unsigned)(nb - 1);
-        if (run && d == last) {
-            run++;
-            return;
+    for (int sl = 0; sl < nslots; sl++) {
+        CvSlot &S = slots[sl];
+        if (S.count <= S.k) continue;  // the same for the whole block
+        for (int i = threadIdx.x; i < nb; i += 256) hist[i] = 0;
+        __syncthreads();
+        const unsigned *v = (const unsigned *)S.list;
+        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
+        const unsigned mask = S.mask, prefix = S.prefix;
+        // neighbouring c-values of the list are often equal (they come from the same tile), so each thread adds runs
+        // of equal digits at once; 4 values per 16-byte load
+        unsigned last = 0, run = 0;
+        auto add = [&](unsigned bits) {
+            if ((bits & mask) != prefix) return;
+            const unsigned d = (bits >> shift) & (unsigned)(nb - 1);
+            if (run && d == last) {
+                run++;
+                return;
+            }
+            if (run) atomicAdd(&hist[last], run);
+            last = d;
+            run = 1;
+        };
+        for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+            const uint4 q = __ldg((const uint4 *)v + i);
+            add(q.x);
+            add(q.y);
+            add(q.z);
+            add(q.w);
         }
+        for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(v[i]);
         if (run) atomicAdd(&hist[last], run);
-        last = d;
-        run = 1;
-    };
-    for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
-        const uint4 q = __ldg((const uint4 *)v + i);
-        add(q.x);
-        add(q.y);
-        add(q.z);
-        add(q.w);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nb; i += 256)
+            if (hist[i]) atomicAdd(&S.hist[i], hist[i]);
+        __syncthreads();
     }
-    for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(v[i]);
-    if (run) atomicAdd(&hist[last], run);
-    __syncthreads();
-    for (int i = threadIdx.x; i < nb; i += 256)
-        if (hist[i]) atomicAdd(&S.hist[i], hist[i]);
 }
 
 __global__ void __launch_bounds__(256) select_pick_kernel(CvSlot *slots, int shift, int width)
@@ -241,35 +245,37 @@ __global__ void __launch_bounds__(256) select_pick_kernel(CvSlot *slots, int shi
     for (int i = t; i < nb; i += 256) S.hist[i] = 0;
 }
 
-__global__ void __launch_bounds__(256) sum_above_kernel(CvSlot *slots)
+__global__ void __launch_bounds__(256) sum_above_kernel(CvSlot *slots, int nslots)
 {
-    CvSlot &S = slots[blockIdx.y];
-    if (S.count <= S.k) return;
-    const float threshold = __uint_as_float(S.prefix);
-    const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
-    unsigned long long s = 0, c = 0;
-    auto add = [&](float v) {
-        if (v > threshold) {
-            s += __float2ull_rn(__fmul_rn(v, 16777216.0f));
-            c++;
+    for (int sl = 0; sl < nslots; sl++) {
+        CvSlot &S = slots[sl];
+        if (S.count <= S.k) continue;
+        const float threshold = __uint_as_float(S.prefix);
+        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
+        unsigned long long s = 0, c = 0;
+        auto add = [&](float v) {
+            if (v > threshold) {
+                s += __float2ull_rn(__fmul_rn(v, 16777216.0f));
+                c++;
+            }
+        };
+        for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+            const float4 q = __ldg((const float4 *)S.list + i);
+            add(q.x);
+            add(q.y);
+            add(q.z);
+            add(q.w);
         }
-    };
-    for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
-        const float4 q = __ldg((const float4 *)S.list + i);
-        add(q.x);
-        add(q.y);
-        add(q.z);
-        add(q.w);
-    }
-    for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(S.list[i]);
+        for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(S.list[i]);
 #pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        s += __shfl_down_sync(0xffffffffu, s, o);
-        c += __shfl_down_sync(0xffffffffu, c, o);
-    }
-    if ((threadIdx.x & 31) == 0 && c) {
-        atomicAdd(&S.above_fx, s);
-        atomicAdd(&S.above_n, c);
+        for (int o = 16; o; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o);
+            c += __shfl_down_sync(0xffffffffu, c, o);
+        }
+        if ((threadIdx.x & 31) == 0 && c) {
+            atomicAdd(&S.above_fx, s);
+            atomicAdd(&S.above_n, c);
+        }
     }
 }
 
@@ -331,7 +337,7 @@ cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width,
     if (nslots <= 0) return cudaSuccess;
     {
         LaunchTimer t("cambi_select_hist", s);
-        select_hist_kernel<<<dim3(296, nslots), 256, 0, s>>>(slots, shift, width);
+        select_hist_kernel<<<296, 256, 0, s>>>(slots, nslots, shift, width);
     }
     cudaError_t e = after_launch();
     if (e != cudaSuccess) return e;
@@ -344,7 +350,7 @@ cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s)
 {
     if (nslots <= 0) return cudaSuccess;
     LaunchTimer t("cambi_sum_above", s);
-    sum_above_kernel<<<dim3(296, nslots), 256, 0, s>>>(slots);
+    sum_above_kernel<<<296, 256, 0, s>>>(slots, nslots);
     return after_launch();
 }
 
@@ -352,7 +358,7 @@ cudaError_t launch_score(const ScoreBatch &b, cudaStream_t s)
 {
     if (b.njobs <= 0) return cudaSuccess;
     LaunchTimer t("cambi_score", s);
-    score_kernel<<<1, 32, 0, s>>>(b);
+    score_kernel<<<1, kScoreMaxJobs, 0, s>>>(b);
     return after_launch();
 }
 

@@ -133,6 +133,24 @@ unsigned long long topk_count(unsigned long long n, double topk);
 // the caller's stream marks the end of a whole frame step).
 void cambi_join(es_cambi *c, cudaStream_t stream);
 
+namespace es {
+// The figures of one encode in a collected frame step, as the device left them in page-locked memory.
+struct EncodeFigures {
+    double banding, source_banding;
+    const unsigned long long *sse;           // Y, Cb, Cr squared errors
+    const unsigned long long *source_color;  // sum U, sum V, strength in 2^-30 units
+    const unsigned long long *encode_color;
+    size_t n;                                // luma samples
+    int pd, windows;
+    const FrameFigures *fig;
+    const uint16_t *bins;                    // 6 arrays of `windows` bins
+    bool texture;                            // the lasting texture of frame f - 6 is in `fig` / `bins`
+};
+// src/main.cpp:584-641 for one encode: adds the figures into frame_acc and, with texture, the lasting texture into
+// centre_acc (either may be null), and returns the frame's result.
+es_frame_result collect_encode(const EncodeFigures &in, es_accum *frame_acc, es_accum *centre_acc);
+}  // namespace es
+
 struct es_module {
     int device = 0;
 };

@@ -30,6 +30,8 @@ struct LaunchTimer {
 // True while es_kernel_timing(2) is in force: CAMBI instances then queue all their work on the caller's stream, so
 // that nothing runs beside a timed kernel and its events bracket that kernel alone.
 bool serial_streams();
+// True while es_kernel_timing is on (its events need plain launches, so graphs are not used then).
+bool kernel_timing_on();
 
 constexpr int kScales = 5;
 constexpr int kDiffs = 4;
@@ -37,7 +39,8 @@ constexpr uint16_t kNone = 0xFFFF;
 constexpr uint16_t kMaskBit = 0x8000;  // a scale's plane holds value | mask << 15
 constexpr int kMaxBand = 1024;         // codes of a 10-bit pipeline
 constexpr int kMaxPad = 64;            // window 129
-constexpr int kMaxJobs = 80;           // pictures x scales in one c-value launch
+constexpr int kMaxPictures = 64;       // pictures in one batched launch
+constexpr int kMaxJobs = 160;          // pictures x scales in one c-value launch
 constexpr int kWin = 16;               // detail window side (src/kernels.cu:331)
 
 // CAMBI's band parameters (src/kernels.cu:65-69 CambiParams without the per-scale size).
@@ -54,7 +57,7 @@ struct Prep0Job {
     uint16_t *word;       // out: w x h, mode-filtered value | mask << 15
     int tiles_x, first_tile;
 };
-constexpr int kPrep0MaxJobs = 32;
+constexpr int kPrep0MaxJobs = kMaxPictures;
 struct Prep0Batch {
     Prep0Job job[kPrep0MaxJobs];
     int njobs, total_tiles;
@@ -69,7 +72,7 @@ struct DecJob {
     int w, h;
     int first_block;      // blocks of 256 pixels
 };
-constexpr int kDecMaxJobs = 32;
+constexpr int kDecMaxJobs = kMaxPictures;
 struct DecBatch {
     DecJob job[kDecMaxJobs];
     int njobs, total_blocks;
@@ -120,7 +123,7 @@ struct ScoreJob {
     int window;
     double *score;   // out
 };
-constexpr int kScoreMaxJobs = 32;
+constexpr int kScoreMaxJobs = kMaxPictures;
 struct ScoreBatch {
     ScoreJob job[kScoreMaxJobs];
     int njobs;
@@ -137,12 +140,20 @@ struct UnpackJob {
     FrameViewDev f;
     int x0, y0;
     uint16_t *y16, *u16, *v16;  // w x h, w/2 x h/2
+    int w, h, pd;               // common picture area and pipeline depth of this picture's source
     int first_block;            // blocks of 2 x 2-pixel groups
 };
-constexpr int kUnpackMaxJobs = 32;
+constexpr int kUnpackMaxJobs = kMaxPictures;
+struct UnpackView {
+    FrameViewDev f;
+    int x0, y0;
+};
 struct UnpackBatch {
     UnpackJob job[kUnpackMaxJobs];
-    int njobs, total_blocks, w, h, pd;
+    int njobs, total_blocks;
+    // optional: job j's frame view and crop are views[j] in device memory instead of job[j].f, x0, y0 (so a captured
+    // graph can take new input addresses each step)
+    const UnpackView *views;
 };
 cudaError_t launch_unpack(const UnpackBatch &b, cudaStream_t s);
 
@@ -153,8 +164,15 @@ struct WindowJob {
     const uint16_t *yd[kMaxEncodes];    // encode luma
     float *stats[kMaxEncodes];          // per encode: windows x 8
     int nenc, w, h, up;
+    int first_block;                    // set by the launcher
 };
-cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s);
+// Per-source work of a frame step for up to kMaxSources sources in one launch.
+constexpr int kMaxSources = 16;
+struct WindowBatch {
+    WindowJob job[kMaxSources];
+    int njobs;
+};
+cudaError_t launch_window_stats(WindowBatch &b, cudaStream_t s);
 
 // ---- lasting texture ------------------------------------------------------------------------------------------------
 // Running sums of the source's luma over the even and odd frame offsets of the centre frame c = f - 6:
@@ -168,8 +186,13 @@ struct PersistJob {
     float *out[kMaxEncodes];                   // per encode: windows x 5
     int nenc, w, h, up;
     int stats;  // 0: only advance the running sums
+    int first_block;  // set by the launcher
 };
-cudaError_t launch_persist(const PersistJob &j, cudaStream_t s);
+struct PersistBatch {
+    PersistJob job[kMaxSources];
+    int njobs;
+};
+cudaError_t launch_persist(PersistBatch &b, cudaStream_t s);
 
 // ---- PSNR squared errors and color sums --------------------------------------------------------------------------
 struct PairSumsJob {
@@ -178,8 +201,13 @@ struct PairSumsJob {
     unsigned long long *sse;       // [nenc][3]
     unsigned long long *color;     // [nenc + 1][3]: sum U, sum V, strength in 2^-30 units; source last
     int nenc, w, h, up;
+    int first_pic;  // set by the launcher: this job's pictures are grid rows first_pic .. first_pic + nenc
 };
-cudaError_t launch_pair_sums(const PairSumsJob &j, cudaStream_t s);
+struct PairSumsBatch {
+    PairSumsJob job[kMaxSources];
+    int njobs;
+};
+cudaError_t launch_pair_sums(PairSumsBatch &b, cudaStream_t s);
 
 // ---- per-frame reduction of the window figures (src/main.cpp:606-641) -------------------------------------------
 struct FrameFigures {
@@ -200,9 +228,14 @@ struct CollectJob {
     float *threshold;                   // scratch: the frame's structure threshold
     double *partials;                   // scratch: [nenc][collect_blocks(windows)][kCollectSums]
     int nenc, windows;
+    int first_enc;  // set by the launcher: this job's encodes are grid rows first_enc .. first_enc + nenc - 1
+};
+struct CollectBatch {
+    CollectJob job[kMaxSources];
+    int njobs;
 };
 constexpr int kCollectSums = 20;  // 18 double sums and 2 counts per block
 int collect_blocks(int windows);
-cudaError_t launch_collect(const CollectJob &j, cudaStream_t s);
+cudaError_t launch_collect(CollectBatch &b, cudaStream_t s);
 
 }  // namespace es

@@ -89,9 +89,6 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     const int at = (int)(f % 2), up = 10 - fr->pd;
     // unpack every picture of the step in one launch
     UnpackBatch ub{};
-    ub.w = fr->w;
-    ub.h = fr->h;
-    ub.pd = fr->pd;
     const int blocks = (int)(((size_t)(fr->w / 2) * (fr->h / 2) + 255) / 256);
     int first = 0;
     for (int p = 0; p <= fr->nenc; p++) {
@@ -111,6 +108,9 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
             j.u16 = fr->enc_u[p - 1]->ptr;
             j.v16 = fr->enc_v[p - 1]->ptr;
         }
+        j.w = fr->w;
+        j.h = fr->h;
+        j.pd = fr->pd;
         j.first_block = first;
         first += blocks;
     }
@@ -146,7 +146,10 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     pj.w = fr->w;
     pj.h = fr->h;
     pj.up = up;
-    cuda_check(launch_pair_sums(pj, s), "squared errors and colors");
+    PairSumsBatch pb{};
+    pb.job[0] = pj;
+    pb.njobs = 1;
+    cuda_check(launch_pair_sums(pb, s), "squared errors and colors");
 
     // detail window figures of frame f
     WindowJob wj{};
@@ -159,7 +162,10 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     wj.w = fr->w;
     wj.h = fr->h;
     wj.up = up;
-    cuda_check(launch_window_stats(wj, s), "window figures");
+    WindowBatch wb{};
+    wb.job[0] = wj;
+    wb.njobs = 1;
+    cuda_check(launch_window_stats(wb, s), "window figures");
 
     // lasting texture of frame f - 6, once frames f - 12 .. f are in
     const bool texture = f >= 2 * kRadius;
@@ -182,7 +188,10 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     qj.h = fr->h;
     qj.up = up;
     qj.stats = texture ? 1 : 0;
-    cuda_check(launch_persist(qj, s), "lasting texture");
+    PersistBatch qb{};
+    qb.job[0] = qj;
+    qb.njobs = 1;
+    cuda_check(launch_persist(qb, s), "lasting texture");
 
     // per-frame reduction on the device
     CollectJob cj{};
@@ -198,7 +207,12 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     cj.windows = fr->windows;
     cj.threshold = fr->threshold.ptr;
     cj.partials = fr->partials.ptr;
-    if (fr->windows > 0) cuda_check(launch_collect(cj, s), "collecting figures");
+    if (fr->windows > 0) {
+        CollectBatch cb{};
+        cb.job[0] = cj;
+        cb.njobs = 1;
+        cuda_check(launch_collect(cb, s), "collecting figures");
+    }
 
     cuda_check(cudaMemcpyAsync(fr->h_sums[at].ptr, fr->sums[at].ptr, fr->sums[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
     if (fr->windows > 0) {
@@ -224,6 +238,61 @@ void add_bins(es_histogram &hist, const uint16_t *bins, int n)
 }
 
 }  // namespace
+
+// src/main.cpp:584-641 for one encode of a collected frame step.
+es_frame_result es::collect_encode(const EncodeFigures &in, es_accum *frame_acc, es_accum *centre_acc)
+{
+    const size_t cn = in.n / 4;
+    auto color_of = [](const unsigned long long *c, int i) { return i < 2 ? (double)c[i] : (double)c[2] * (1.0 / 1073741824.0); };
+    const FrameFigures &fg = *in.fig;
+    es_frame_result res{};
+    res.cambi = in.banding;
+    res.cambi_source = in.source_banding;
+    res.psnr[0] = es_psnr(in.sse[0], in.n, in.pd);
+    res.psnr[1] = es_psnr(in.sse[1], cn, in.pd);
+    res.psnr[2] = es_psnr(in.sse[2], cn, in.pd);
+    for (int i = 0; i < 3; i++) {
+        res.color_source[i] = color_of(in.source_color, i) / (double)cn;
+        res.color_encode[i] = color_of(in.encode_color, i) / (double)cn;
+    }
+    res.texture = in.texture;
+    res.structure_windows = in.windows > 0 ? fg.n_structure : 0;
+    res.lasting_windows = in.texture && in.windows > 0 ? fg.n_lasting : 0;
+    if (frame_acc) {
+        es_accum &acc = *frame_acc;
+        acc.frames++;
+        acc.cambi += in.banding;
+        acc.cambi_source += in.source_banding;
+        for (int i = 0; i < 3; i++) {
+            acc.psnr[i] += res.psnr[i];
+            acc.color_r[i] += color_of(in.source_color, i) / (double)cn;
+            acc.color_d[i] += color_of(in.encode_color, i) / (double)cn;
+        }
+        if (in.windows > 0) {
+            for (int k = 0; k < 3; k++) {
+                acc.all_r[k] += fg.all_r[k];
+                acc.all_d[k] += fg.all_d[k];
+                acc.st_r[k] += fg.st_r[k];
+                acc.st_d[k] += fg.st_d[k];
+            }
+            for (int k = 0; k < 2; k++) {
+                acc.sh_all_r[k] += fg.all_r[k];
+                acc.sh_all_x[k] += fg.sh_all_x[k];
+                acc.sh_st_r[k] += fg.st_r[k];
+                acc.sh_st_x[k] += fg.sh_st_x[k];
+            }
+            for (int k = 0; k < 3; k++) add_bins(acc.amount[k], in.bins + (size_t)k * in.windows, in.windows);
+            for (int k = 0; k < 2; k++) add_bins(acc.matching[k], in.bins + (size_t)(3 + k) * in.windows, in.windows);
+        }
+    }
+    if (in.texture && in.windows > 0 && centre_acc) {
+        es_accum &cacc = *centre_acc;
+        cacc.own += fg.own;
+        cacc.mine += fg.mine;
+        add_bins(cacc.lasting, in.bins + (size_t)5 * in.windows, in.windows);
+    }
+    return res;
+}
 
 extern "C" {
 
@@ -323,65 +392,16 @@ int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es
             source_banding = *cached_source_cambi;
         }
         const bool texture = f >= 2 * kRadius;
-        const size_t cn = fr->n / 4;
         const unsigned long long *sse = fr->h_sums[at].ptr, *color = sse + 3 * fr->nenc;
         const unsigned long long *scol = color + 3 * fr->nenc;
-        auto color_of = [](const unsigned long long *c, int i) {
-            return i < 2 ? (double)c[i] : (double)c[2] * (1.0 / 1073741824.0);
-        };
         for (int e = 0; e < fr->nenc; e++) {
             double banding = 0;
             const int r = es_cambi_finish(fr->enc_cambi[at][e], &banding);
             if (r) throw Error(r, es_last_error());
-            es_frame_result res{};
-            res.cambi = banding;
-            res.cambi_source = source_banding;
-            res.psnr[0] = es_psnr(sse[3 * e + 0], fr->n, fr->pd);
-            res.psnr[1] = es_psnr(sse[3 * e + 1], cn, fr->pd);
-            res.psnr[2] = es_psnr(sse[3 * e + 2], cn, fr->pd);
-            for (int i = 0; i < 3; i++) {
-                res.color_source[i] = color_of(scol, i) / (double)cn;
-                res.color_encode[i] = color_of(color + 3 * e, i) / (double)cn;
-            }
-            const FrameFigures &fg = fr->h_figs[at].ptr[e];
-            res.texture = texture;
-            res.structure_windows = fr->windows > 0 ? fg.n_structure : 0;
-            res.lasting_windows = texture && fr->windows > 0 ? fg.n_lasting : 0;
-            if (frame_acc && frame_acc[e]) {
-                es_accum &acc = *frame_acc[e];
-                acc.frames++;
-                acc.cambi += banding;
-                acc.cambi_source += source_banding;
-                for (int i = 0; i < 3; i++) {
-                    acc.psnr[i] += res.psnr[i];
-                    acc.color_r[i] += color_of(scol, i) / (double)cn;
-                    acc.color_d[i] += color_of(color + 3 * e, i) / (double)cn;
-                }
-                if (fr->windows > 0) {
-                    for (int k = 0; k < 3; k++) {
-                        acc.all_r[k] += fg.all_r[k];
-                        acc.all_d[k] += fg.all_d[k];
-                        acc.st_r[k] += fg.st_r[k];
-                        acc.st_d[k] += fg.st_d[k];
-                    }
-                    for (int k = 0; k < 2; k++) {
-                        acc.sh_all_r[k] += fg.all_r[k];
-                        acc.sh_all_x[k] += fg.sh_all_x[k];
-                        acc.sh_st_r[k] += fg.st_r[k];
-                        acc.sh_st_x[k] += fg.sh_st_x[k];
-                    }
-                    const uint16_t *b = fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows;
-                    for (int k = 0; k < 3; k++) add_bins(acc.amount[k], b + (size_t)k * fr->windows, fr->windows);
-                    for (int k = 0; k < 2; k++) add_bins(acc.matching[k], b + (size_t)(3 + k) * fr->windows, fr->windows);
-                }
-            }
-            if (texture && fr->windows > 0 && centre_acc && centre_acc[e]) {
-                es_accum &cacc = *centre_acc[e];
-                cacc.own += fg.own;
-                cacc.mine += fg.mine;
-                const uint16_t *b = fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows;
-                add_bins(cacc.lasting, b + (size_t)5 * fr->windows, fr->windows);
-            }
+            const es_frame_result res = collect_encode(
+                EncodeFigures{banding, source_banding, sse + 3 * e, scol, color + 3 * e, fr->n, fr->pd, fr->windows,
+                              &fr->h_figs[at].ptr[e], fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows, texture},
+                frame_acc ? frame_acc[e] : nullptr, centre_acc ? centre_acc[e] : nullptr);
             if (out) out[e] = res;
         }
         fr->last_collected = f;

@@ -28,20 +28,22 @@ __global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ Unp
     int j = 0;
     while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
     const UnpackJob &J = b.job[j];
-    const int cw = b.w / 2, ch = b.h / 2;
+    const FrameViewDev f = b.views ? b.views[j].f : J.f;
+    const int x0 = b.views ? b.views[j].x0 : J.x0, y0 = b.views ? b.views[j].y0 : J.y0;
+    const int cw = J.w / 2, ch = J.h / 2;
     const int i = (blockIdx.x - J.first_block) * 256 + threadIdx.x;
     if (i >= cw * ch) return;
-    const int cx = i % cw, cy = i / cw, up = b.pd - J.f.depth;
+    const int cx = i % cw, cy = i / cw, up = J.pd - f.depth;
 #pragma unroll
     for (int dy = 0; dy < 2; dy++) {
         const int y = 2 * cy + dy;
-        const unsigned a = sample_at(J.f.y, J.f.ypitch, 2 * cx + J.x0, y + J.y0, J.f);
-        const unsigned c = sample_at(J.f.y, J.f.ypitch, 2 * cx + 1 + J.x0, y + J.y0, J.f);
-        *(uint32_t *)(J.y16 + (size_t)y * b.w + 2 * cx) = (a << up) | ((c << up) << 16);
+        const unsigned a = sample_at(f.y, f.ypitch, 2 * cx + x0, y + y0, f);
+        const unsigned c = sample_at(f.y, f.ypitch, 2 * cx + 1 + x0, y + y0, f);
+        *(uint32_t *)(J.y16 + (size_t)y * J.w + 2 * cx) = (a << up) | ((c << up) << 16);
     }
-    const int sx = (2 * cx + J.x0) / 2, sy = (2 * cy + J.y0) / 2;
-    const unsigned u = J.f.semi ? sample_at(J.f.u, J.f.cpitch, 2 * sx, sy, J.f) : sample_at(J.f.u, J.f.cpitch, sx, sy, J.f);
-    const unsigned v = J.f.semi ? sample_at(J.f.u, J.f.cpitch, 2 * sx + 1, sy, J.f) : sample_at(J.f.v, J.f.cpitch, sx, sy, J.f);
+    const int sx = (2 * cx + x0) / 2, sy = (2 * cy + y0) / 2;
+    const unsigned u = f.semi ? sample_at(f.u, f.cpitch, 2 * sx, sy, f) : sample_at(f.u, f.cpitch, sx, sy, f);
+    const unsigned v = f.semi ? sample_at(f.u, f.cpitch, 2 * sx + 1, sy, f) : sample_at(f.v, f.cpitch, sx, sy, f);
     J.u16[(size_t)cy * cw + cx] = (uint16_t)(u << up);
     J.v16[(size_t)cy * cw + cx] = (uint16_t)(v << up);
 }
@@ -211,12 +213,16 @@ __device__ __forceinline__ T half_warp_sum(T v)
     return v;
 }
 
-__global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_constant__ WindowJob J)
+__global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_constant__ WindowBatch B)
 {
     __shared__ __align__(16) WinSmem sm;
+    int jb = 0;
+    while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_block) jb++;
+    const WindowJob &J = B.job[jb];
+    const int bid = blockIdx.x - J.first_block;
     const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
     const int tiles_x = (ww + 3) / 4;
-    const int x0 = (blockIdx.x % tiles_x) * kWT, y0 = (blockIdx.x / tiles_x) * kWT;
+    const int x0 = (bid % tiles_x) * kWT, y0 = (bid / tiles_x) * kWT;
     const int tid = threadIdx.x, lane = tid & 31;
     const int c = tid & (kWT - 1), r0 = (tid >> 6) * kWin;  // tile column, first tile row
     const int wx = (x0 + c) / kWin, wy = (y0 + r0) / kWin;
@@ -310,13 +316,17 @@ __device__ __forceinline__ void mids_of(BoxSmem &sm, int c, int r0, int (&mid)[8
     for (int i = 0; i < 8; i++) mid[i] = 9 * s3[i] - s9[i];
 }
 
-__global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ PersistJob J)
+__global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ PersistBatch B)
 {
     __shared__ BoxSmem sm;
     __shared__ uint16_t o_reg[kRH][kRW];
+    int jb = 0;
+    while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_block) jb++;
+    const PersistJob &J = B.job[jb];
+    const int bid = blockIdx.x - J.first_block;
     const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
     const int tiles_x = (w + kTW - 1) / kTW;
-    const int x0 = (blockIdx.x % tiles_x) * kTW, y0 = (blockIdx.x / tiles_x) * kTH;
+    const int x0 = (bid % tiles_x) * kTW, y0 = (bid / tiles_x) * kTH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // advance the running sums over the region (clamped coordinates, so the margins repeat the edges)
     for (int i = threadIdx.x; i < kRH * kRW; i += 256) {
@@ -395,9 +405,12 @@ __global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ Pe
 // sample sqrt(du^2 + dv^2) is rounded to units of 2^-30 so its sum is exact too. blockIdx.y picks the picture:
 // 0 .. nenc-1 the encodes (squared errors against the source, and their colors), nenc the source's colors.
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ PairSumsJob J)
+__global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ PairSumsBatch B)
 {
-    const int p = blockIdx.y;
+    int jb = 0;
+    while (jb + 1 < B.njobs && (int)blockIdx.y >= B.job[jb + 1].first_pic) jb++;
+    const PairSumsJob &J = B.job[jb];
+    const int p = blockIdx.y - J.first_pic;
     const bool src_only = p == J.nenc;
     const size_t n = (size_t)J.w * J.h, cn = n / 4;
     const size_t stride = (size_t)gridDim.x * 256, i0 = (size_t)blockIdx.x * 256 + threadIdx.x;
@@ -474,6 +487,7 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kCT = 1024;  // threshold block
 constexpr int kCW = 256;   // windows per block
+__host__ __device__ inline int collect_blocks_dev(int windows) { return (windows + kCW - 1) / kCW; }
 
 __device__ __forceinline__ uint16_t hist_bin(double pct)
 {
@@ -528,9 +542,10 @@ __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, un
     return s_prefix;
 }
 
-__global__ void __launch_bounds__(kCT) collect_threshold_kernel(const __grid_constant__ CollectJob J)
+__global__ void __launch_bounds__(kCT) collect_threshold_kernel(const __grid_constant__ CollectBatch B)
 {
     __shared__ unsigned hist[2048];
+    const CollectJob &J = B.job[blockIdx.x];
     const float *st = J.stats[0];  // the source's oriented figures are the same in every encode's array
     const int n = J.windows;
     // numpy's linear quantile at 0.8 of exact order statistics, in the reference's float / double arithmetic
@@ -550,10 +565,15 @@ __global__ void __launch_bounds__(kCT) collect_threshold_kernel(const __grid_con
     }
 }
 
-__global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_constant__ CollectJob J)
+__global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_constant__ CollectBatch B)
 {
     __shared__ double part[kCW / 32][kCollectSums];
-    const int e = blockIdx.y, n = J.windows, i = blockIdx.x * kCW + threadIdx.x;
+    int jb = 0;
+    while (jb + 1 < B.njobs && (int)blockIdx.y >= B.job[jb + 1].first_enc) jb++;
+    const CollectJob &J = B.job[jb];
+    const int nb = collect_blocks_dev(J.windows);
+    if ((int)blockIdx.x >= nb) return;  // the grid covers the job with the most windows
+    const int e = blockIdx.y - J.first_enc, n = J.windows, i = blockIdx.x * kCW + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // sums: all_r[3] all_d[3] st_r[3] st_d[3] sh_all_x[2] sh_st_x[2] own mine n_structure n_lasting
     double v[kCollectSums];
@@ -611,13 +631,16 @@ __global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_const
     if (threadIdx.x < kCollectSums) {
         double s = 0.0;
         for (int k = 0; k < kCW / 32; k++) s += part[k][threadIdx.x];
-        J.partials[((size_t)e * gridDim.x + blockIdx.x) * kCollectSums + threadIdx.x] = s;
+        J.partials[((size_t)e * nb + blockIdx.x) * kCollectSums + threadIdx.x] = s;
     }
 }
 
-__global__ void collect_final_kernel(const __grid_constant__ CollectJob J, int nblocks)
+__global__ void collect_final_kernel(const __grid_constant__ CollectBatch B)
 {
-    const int e = blockIdx.x, k = threadIdx.x;
+    int jb = 0;
+    while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_enc) jb++;
+    const CollectJob &J = B.job[jb];
+    const int e = blockIdx.x - J.first_enc, k = threadIdx.x, nblocks = collect_blocks_dev(J.windows);
     if (k >= kCollectSums) return;
     double s = 0.0;
     for (int b = 0; b < nblocks; b++) s += J.partials[((size_t)e * nblocks + b) * kCollectSums + k];
@@ -645,51 +668,74 @@ cudaError_t launch_unpack(const UnpackBatch &b, cudaStream_t s)
     return after_launch();
 }
 
-cudaError_t launch_window_stats(const WindowJob &j, cudaStream_t s)
+cudaError_t launch_window_stats(WindowBatch &b, cudaStream_t s)
 {
-    const int ww = j.w / kWin, wh = j.h / kWin;
-    if (ww <= 0 || wh <= 0 || j.nenc <= 0) return cudaSuccess;
-    const int blocks = ((ww + 3) / 4) * ((wh + 3) / 4);
+    int blocks = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        WindowJob &J = b.job[j];
+        J.first_block = blocks;
+        const int ww = J.w / kWin, wh = J.h / kWin;
+        if (ww > 0 && wh > 0 && J.nenc > 0) blocks += ((ww + 3) / 4) * ((wh + 3) / 4);
+    }
+    if (blocks == 0) return cudaSuccess;
     LaunchTimer t("window_stats", s);
-    window_stats_kernel<<<blocks, 256, 0, s>>>(j);
+    window_stats_kernel<<<blocks, 256, 0, s>>>(b);
     return after_launch();
 }
 
-cudaError_t launch_persist(const PersistJob &j, cudaStream_t s)
+cudaError_t launch_persist(PersistBatch &b, cudaStream_t s)
 {
-    const int blocks = ((j.w + kTW - 1) / kTW) * ((j.h + kTH - 1) / kTH);
+    int blocks = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        PersistJob &J = b.job[j];
+        J.first_block = blocks;
+        blocks += ((J.w + kTW - 1) / kTW) * ((J.h + kTH - 1) / kTH);
+    }
+    if (blocks == 0) return cudaSuccess;
     LaunchTimer t("persist_stats", s);
-    persist_kernel<<<blocks, 256, 0, s>>>(j);
+    persist_kernel<<<blocks, 256, 0, s>>>(b);
     return after_launch();
 }
 
-cudaError_t launch_pair_sums(const PairSumsJob &j, cudaStream_t s)
+cudaError_t launch_pair_sums(PairSumsBatch &b, cudaStream_t s)
 {
+    int pics = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        b.job[j].first_pic = pics;
+        pics += b.job[j].nenc + 1;
+    }
+    if (pics == 0) return cudaSuccess;
     LaunchTimer t("pair_sums", s);
-    pair_sums_kernel<<<dim3(148, j.nenc + 1), 256, 0, s>>>(j);
+    pair_sums_kernel<<<dim3(pics <= 4 ? 148 : 64, pics), 256, 0, s>>>(b);
     return after_launch();
 }
 
-int collect_blocks(int windows) { return (windows + kCW - 1) / kCW; }
+int collect_blocks(int windows) { return collect_blocks_dev(windows); }
 
-cudaError_t launch_collect(const CollectJob &j, cudaStream_t s)
+cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
 {
-    if (j.nenc <= 0 || j.windows <= 0) return cudaSuccess;
-    const int nb = collect_blocks(j.windows);
+    int encs = 0, nb = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        b.job[j].first_enc = encs;
+        encs += b.job[j].nenc;
+        nb = nb > collect_blocks(b.job[j].windows) ? nb : collect_blocks(b.job[j].windows);
+        if (b.job[j].nenc <= 0 || b.job[j].windows <= 0) return cudaErrorInvalidValue;
+    }
+    if (encs == 0) return cudaSuccess;
     {
         LaunchTimer t("frame_collect_threshold", s);
-        collect_threshold_kernel<<<1, kCT, 0, s>>>(j);
+        collect_threshold_kernel<<<b.njobs, kCT, 0, s>>>(b);
     }
     cudaError_t e = after_launch();
     if (e != cudaSuccess) return e;
     {
         LaunchTimer t("frame_collect_windows", s);
-        collect_windows_kernel<<<dim3(nb, j.nenc), kCW, 0, s>>>(j);
+        collect_windows_kernel<<<dim3(nb, encs), kCW, 0, s>>>(b);
     }
     e = after_launch();
     if (e != cudaSuccess) return e;
     LaunchTimer t("frame_collect_final", s);
-    collect_final_kernel<<<j.nenc, 32, 0, s>>>(j, nb);
+    collect_final_kernel<<<encs, 32, 0, s>>>(b);
     return after_launch();
 }
 

@@ -70,6 +70,7 @@ LaunchTimer::~LaunchTimer()
 }
 
 bool serial_streams() { return timing().serial.load(std::memory_order_relaxed); }
+bool kernel_timing_on() { return timing().on.load(std::memory_order_relaxed); }
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }

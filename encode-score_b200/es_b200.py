@@ -27,6 +27,8 @@ SYMBOLS = (
     "es_cambi_score_noalloc",
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
+    "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
+    "es_batch_graph_launches", "es_batch_destroy",
 )
 
 
@@ -82,6 +84,14 @@ class FrameResult(ctypes.Structure):
 _lib = None
 
 
+class BatchSource(ctypes.Structure):
+    _fields_ = [("w", ctypes.c_int), ("h", ctypes.c_int), ("pd", ctypes.c_int), ("n_encodes", ctypes.c_int)]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("use_graphs", ctypes.c_int)]
+
+
 def lib() -> ctypes.CDLL:
     """The loaded library (raises OSError with the path if it was not built)."""
     global _lib
@@ -126,6 +136,15 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.POINTER(Accum)), ctypes.POINTER(FrameResult)]
         L.es_frame_read_windows.argtypes = [P, I, P, P]
         L.es_frame_destroy.argtypes = [P]
+        L.es_batch_create.argtypes = [P, I, ctypes.POINTER(BatchSource), ctypes.POINTER(BatchOptions), ctypes.POINTER(P)]
+        L.es_batch_queue.argtypes = [P, ctypes.c_long, ctypes.POINTER(FrameView), ctypes.POINTER(I), ctypes.POINTER(I), P]
+        L.es_batch_collect.argtypes = [P, ctypes.c_long, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.POINTER(Accum)),
+                                       ctypes.POINTER(ctypes.POINTER(Accum)), ctypes.POINTER(FrameResult)]
+        L.es_batch_read_windows.argtypes = [P, I, I, P, P]
+        L.es_batch_scale_pooled.argtypes = [P, I, ctypes.POINTER(ctypes.c_double)]
+        L.es_batch_graph_launches.argtypes = [P]
+        L.es_batch_graph_launches.restype = U64
+        L.es_batch_destroy.argtypes = [P]
         _lib = L
     return _lib
 
@@ -295,4 +314,56 @@ class Frame:
     def close(self) -> None:
         if self.handle:
             lib().es_frame_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+class Batch:
+    """Batched frame steps of several sources (es_batch_*): one launch per stage for all pictures, CUDA graphs from
+    frame 14 on. ``sources`` is a list of (w, h, pd, n_encodes); pictures and encodes are numbered source by source."""
+
+    def __init__(self, module: Module, sources: list, use_graphs: bool = True):
+        self.handle = ctypes.c_void_p()
+        self.sources = [tuple(s) for s in sources]
+        self.n_pictures = sum(1 + s[3] for s in self.sources)
+        self.n_encodes = sum(s[3] for s in self.sources)
+        arr = (BatchSource * len(self.sources))(*[BatchSource(*s) for s in self.sources])
+        opt = BatchOptions(int(use_graphs))
+        check(lib().es_batch_create(module.handle, len(self.sources), arr, ctypes.byref(opt), ctypes.byref(self.handle)))
+
+    def queue(self, f: int, views: list, stream: int = 0, crops: list | None = None, source_cambi: list | None = None) -> None:
+        va = (FrameView * self.n_pictures)(*views)
+        ca = (ctypes.c_int * (2 * self.n_pictures))(*[c for xy in crops for c in xy]) if crops else None
+        sa = (ctypes.c_int * len(self.sources))(*[int(x) for x in source_cambi]) if source_cambi is not None else None
+        check(lib().es_batch_queue(self.handle, f, va, ca, sa, ctypes.c_void_p(stream)))
+
+    def collect(self, f: int, frame_acc: list | None = None, centre_acc: list | None = None,
+                cached_source_cambi: list | None = None) -> list:
+        n = self.n_encodes
+        out = (FrameResult * n)()
+        fa = (ctypes.POINTER(Accum) * n)(*[ctypes.pointer(a) for a in frame_acc]) if frame_acc else None
+        ca = (ctypes.POINTER(Accum) * n)(*[ctypes.pointer(a) for a in centre_acc]) if centre_acc else None
+        cached = (ctypes.c_double * len(self.sources))(*cached_source_cambi) if cached_source_cambi is not None else None
+        check(lib().es_batch_collect(self.handle, f, cached, fa, ca, out))
+        return list(out)
+
+    def read_windows(self, source: int, encode: int, persist: bool = False):
+        import numpy as np
+        w, h = self.sources[source][0], self.sources[source][1]
+        windows = (w // 16) * (h // 16)
+        st = np.zeros((windows, 8), np.float32)
+        ps = np.zeros((windows, 5), np.float32) if persist else None
+        check(lib().es_batch_read_windows(self.handle, source, encode, st.ctypes.data, ps.ctypes.data if persist else None))
+        return st, ps
+
+    def scale_pooled(self, picture: int) -> list:
+        out = (ctypes.c_double * SCALES)()
+        check(lib().es_batch_scale_pooled(self.handle, picture, out))
+        return list(out)
+
+    def graph_launches(self) -> int:
+        return int(lib().es_batch_graph_launches(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_batch_destroy(self.handle)
             self.handle = ctypes.c_void_p()

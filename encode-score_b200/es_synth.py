@@ -7,6 +7,9 @@ Each workload is a source and its encodes as 4:2:0 planes (uint16 arrays holding
 * ``c2``  3840x2160 10-bit dark content: low-frequency gradients over codes 64-300 plus grain (sigma 8); three encodes
   blurred with sigma 0.8 / 1.5 / 2.5, the third also de-grained by a 7x7 box, each requantised to steps of 8 / 16 / 32
   codes on random rectangles covering 30% of the picture.
+* ``c3``  16 sources of uneven sizes scored together (6 x 1280x720 8-bit, 6 x 1920x800 10-bit cropped from
+  1920x1080 frames with black bars, 4 x 3840x1600 10-bit), each made like ``c1`` with its own grain sigma (uniform in
+  1-12 codes) and banding step (one of 4, 8, 16, 32 codes).
 * ``c4``  bright 10-bit gradient (codes 600-940) with heavy grain (sigma 20), for the precision checks.
 
 Chroma is the luma halved and downsampled 2x2. Frame i of source s draws from numpy's PCG64 seeded with
@@ -106,6 +109,26 @@ def c2_step(frame: int, w: int = 3840, h: int = 2160, seed: int = 2, source: int
         enc = np.where(region, np.rint(enc / step) * step, np.rint(enc))
         encodes.append(_picture(np.clip(enc, 64, 300), 10))
     return Step(_picture(src, 10), encodes)
+
+
+C3_SOURCES = [(1280, 720, 8)] * 6 + [(1920, 800, 10)] * 6 + [(3840, 1600, 10)] * 4
+C3_BARS = {(1920, 800): (1920, 1080)}  # decoded frame size of a cropped source: the picture sits centred in black bars
+
+
+def c3_step(frame: int, source: int, w: int, h: int, depth: int, seed: int = 3) -> Step:
+    """One source of the uneven batch and its encode: c1's recipe at (w, h, depth) with this source's grain sigma and
+    banding step."""
+    base = np.random.Generator(np.random.PCG64(seed + 1000 * source))
+    rng = np.random.Generator(np.random.PCG64(seed + 1000 * source + frame + 500))
+    sigma = float(base.uniform(1, 12))
+    step = int(base.choice([4, 8, 16, 32]))
+    lo, hi = (16, 235) if depth == 8 else (64, 940)
+    luma = lo + (hi - lo) * _field(base, w, h, frame)
+    src = np.clip(np.rint(luma + rng.normal(0, sigma, (h, w))), lo, hi)
+    blur = ndimage.gaussian_filter(src.astype(np.float32), 1.2, truncate=2.0 / 1.2, mode="nearest")
+    enc = np.clip(np.rint(blur), lo, hi)
+    enc[:, : w // 2] = np.clip(np.rint(enc[:, : w // 2] / step) * step, lo, hi)
+    return Step(_picture(src, depth), [_picture(enc, depth)])
 
 
 def c4_step(frame: int, w: int = 3840, h: int = 2160, seed: int = 4, source: int = 0) -> Step:

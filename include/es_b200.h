@@ -195,6 +195,43 @@ int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es
 int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist);
 void es_frame_destroy(es_frame *fr);
 
+/* ---------------------------------------------------------------------------------------------------------------
+ * Batched frame steps: no counterpart in the reference, which scores one source per process with one launch per
+ * kernel and picture (src/main.cpp:518-643). A batch holds up to 16 sources, each with its own encodes, picture size
+ * and pipeline depth (at most 32 pictures in all), and scores a frame step of all of them with one launch per stage;
+ * CAMBI runs beside the texture figures, and from frame 14 on a step is replayed from a CUDA graph per ring phase.
+ * queue / collect keep es_frame_queue / es_frame_collect's contract (double-buffered by f % 2, frames in order).
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct es_batch es_batch;
+typedef struct {
+    int w, h;      /* common picture area of the source and its encodes (even) */
+    int pd;        /* pipeline depth, 8 or 10 */
+    int n_encodes; /* 1 to 16 */
+} es_batch_source;
+typedef struct {
+    int use_graphs; /* replay steps from CUDA graphs once the rings are full (frame 14 on) */
+} es_batch_options;
+
+/* options NULL = {use_graphs = 1}. Pictures are numbered source by source: the source, then its encodes. */
+int es_batch_create(const es_module *m, int n_sources, const es_batch_source *sources, const es_batch_options *options,
+                    es_batch **out);
+/* views[i]: picture i's device frame (numbered as above); crops: (x, y) per picture (even), or NULL for none;
+ * source_cambi: per source, 0 to skip its CAMBI this step (a cached value is given to collect), or NULL for all.
+ * The step runs after the work already queued on `stream`, and `stream` waits for it. */
+int es_batch_queue(es_batch *b, long f, const es_frame_view *views, const int *crops, const int *source_cambi,
+                   void *stream);
+/* Waits for step f and adds its figures; frame_acc / centre_acc / out are indexed by encode, numbered source by
+ * source (any may be NULL or hold NULL entries); cached_source_cambi[s] is read for sources skipped at queue time. */
+int es_batch_collect(es_batch *b, long f, const double *cached_source_cambi, es_accum *const *frame_acc,
+                     es_accum *const *centre_acc, es_frame_result *out);
+/* Introspection for tests: as es_frame_read_windows for encode `encode` of source `source`. */
+int es_batch_read_windows(es_batch *b, int source, int encode, float *stats, float *persist);
+/* Introspection for tests: the pooled value of each scale of picture `picture` in the last collected step. */
+int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5]);
+/* Diagnostics: how many steps were replayed from CUDA graphs. */
+uint64_t es_batch_graph_launches(const es_batch *b);
+void es_batch_destroy(es_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

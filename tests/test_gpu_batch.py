@@ -1,0 +1,138 @@
+"""The batched frame step (es_batch_*) against one plain es_frame per source: sources of uneven sizes and depths,
+scored together with one launch per stage and, from frame 14 on, replayed from CUDA graphs, must give the same
+per-frame results, window and lasting-texture figures and segment accumulators as scoring each source alone (which
+the frame tests pin to the CPU oracle)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import es_b200
+import es_synth
+from gpu_util import step_to_dev
+
+pytestmark = pytest.mark.gpu
+
+SOURCES = [(160, 96, 8, 1), (192, 128, 10, 2), (128, 80, 10, 1)]
+FRAMES = 17
+
+
+def make_step(f, s, w, h, pd, n):
+    if n == 1:
+        return es_synth.c3_step(f, s, w, h, pd)
+    return es_synth.c2_step(f, w=w, h=h, source=s, n_encodes=n)
+
+
+def accum_bytes(a):
+    return bytes(memoryview(ctypes.string_at(ctypes.addressof(a), ctypes.sizeof(a))))
+
+
+def run_plain(cuda, module, steps, source_cambi=None):
+    stream = cuda.cuda.current_stream().cuda_stream
+    out = []
+    accs = []
+    for s, (w, h, pd, n) in enumerate(SOURCES):
+        fr = es_b200.Frame(module, w, h, pd, n)
+        acc = [es_b200.new_accum() for _ in range(n)]
+        res, wins = [], []
+        cached = None
+        for f in range(FRAMES):
+            keep, sv, ev = step_to_dev(cuda, es_b200, steps[f][s])
+            run = source_cambi is None or source_cambi[f][s]
+            fr.queue(f, sv, ev, stream, source_cambi=run)
+            r = fr.collect(f, acc, acc, cached_source_cambi=None if run else 1.25)
+            res.append([(x.cambi, x.cambi_source, tuple(x.psnr), tuple(x.color_source), tuple(x.color_encode), x.texture,
+                         x.structure_windows, x.lasting_windows) for x in r])
+            wins.append([fr.read_windows(e, persist=f >= 12) for e in range(n)])
+        fr.close()
+        out.append((res, wins))
+        accs.append(acc)
+    return out, accs
+
+
+def run_batch(cuda, module, steps, use_graphs=True, source_cambi=None):
+    stream = cuda.cuda.current_stream().cuda_stream
+    b = es_b200.Batch(module, SOURCES, use_graphs=use_graphs)
+    accs = [es_b200.new_accum() for _ in range(b.n_encodes)]
+    per_source = [([], []) for _ in SOURCES]
+    for f in range(FRAMES):
+        keep, views = [], []
+        for s in range(len(SOURCES)):
+            k, sv, ev = step_to_dev(cuda, es_b200, steps[f][s])
+            keep.append(k)
+            views += [sv] + ev
+        flags = source_cambi[f] if source_cambi is not None else None
+        b.queue(f, views, stream, source_cambi=flags)
+        r = b.collect(f, accs, accs, cached_source_cambi=[1.25] * len(SOURCES))
+        k = 0
+        for s, (w, h, pd, n) in enumerate(SOURCES):
+            per_source[s][0].append([(x.cambi, x.cambi_source, tuple(x.psnr), tuple(x.color_source), tuple(x.color_encode),
+                                      x.texture, x.structure_windows, x.lasting_windows) for x in r[k:k + n]])
+            per_source[s][1].append([b.read_windows(s, e, persist=f >= 12) for e in range(n)])
+            k += n
+    graphs = b.graph_launches()
+    b.close()
+    return per_source, accs, graphs
+
+
+@pytest.fixture(scope="module")
+def steps():
+    return [[make_step(f, s, *src) for s, src in enumerate(SOURCES)] for f in range(FRAMES)]
+
+
+def compare(plain, plain_acc, batch, batch_acc):
+    k = 0
+    for s, (w, h, pd, n) in enumerate(SOURCES):
+        (pres, pwin), (bres, bwin) = plain[s], batch[s]
+        for f in range(FRAMES):
+            assert bres[f] == pres[f], (s, f, bres[f], pres[f])
+            for e in range(n):
+                assert np.array_equal(bwin[f][e][0].view(np.uint32), pwin[f][e][0].view(np.uint32)), (s, f, e)
+                if f >= 12:
+                    assert np.array_equal(bwin[f][e][1].view(np.uint32), pwin[f][e][1].view(np.uint32)), (s, f, e)
+        for e in range(n):
+            assert accum_bytes(batch_acc[k + e]) == accum_bytes(plain_acc[s][e]), (s, e)
+        k += n
+
+
+def test_batch_equals_one_frame_per_source(cuda, module, steps):
+    plain, pacc = run_plain(cuda, module, steps)
+    batch, bacc, graphs = run_batch(cuda, module, steps)
+    assert graphs == FRAMES - 14
+    compare(plain, pacc, batch, bacc)
+    # banding is exercised: some encode has a positive CAMBI
+    assert max(r[0] for res, _ in plain for fr in res for r in fr) > 0
+
+
+def test_batch_without_graphs_equals_with(cuda, module, steps):
+    a, aacc, ga = run_batch(cuda, module, steps, use_graphs=False)
+    b, bacc, gb = run_batch(cuda, module, steps, use_graphs=True)
+    assert ga == 0 and gb == FRAMES - 14
+    for s in range(len(SOURCES)):
+        assert a[s][0] == b[s][0]
+    assert [accum_bytes(x) for x in aacc] == [accum_bytes(x) for x in bacc]
+
+
+def test_batch_skipped_source_cambi_uses_the_cached_value(cuda, module, steps):
+    rng = np.random.default_rng(5)
+    flags = [[bool(rng.integers(0, 2)) for _ in SOURCES] for _ in range(FRAMES)]
+    flags[15] = [False] * len(SOURCES)  # a graph with every source skipped
+    plain, pacc = run_plain(cuda, module, steps, source_cambi=flags)
+    batch, bacc, graphs = run_batch(cuda, module, steps, source_cambi=flags)
+    compare(plain, pacc, batch, bacc)
+    for s in range(len(SOURCES)):
+        for f in range(FRAMES):
+            if not flags[f][s]:
+                assert all(r[1] == 1.25 for r in batch[s][0][f])
+
+
+def test_batch_rejects_bad_arguments(cuda, module):
+    with pytest.raises(es_b200.EsError):
+        es_b200.Batch(module, [(15, 16, 10, 1)])
+    with pytest.raises(es_b200.EsError):
+        es_b200.Batch(module, [(64, 64, 10, 16)] * 2)  # 34 pictures
+    b = es_b200.Batch(module, [(64, 64, 10, 1)])
+    with pytest.raises(es_b200.EsError):
+        b.collect(0)
+    b.close()
