@@ -28,6 +28,7 @@ struct es_cambi {
     Stream stream;
     Event copied, finished;
     float *planes[kScales] = {};
+    unsigned long long *tile_mass = nullptr;
     bool pending = false, done = false;
 };
 
@@ -136,6 +137,7 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
     }
     cb.lut = c->lut.ptr;
     cb.slots = c->slots.ptr;
+    cb.tile_mass = c->tile_mass;
     // the slots carry their list buffers
     {
         static_assert(sizeof(CvSlot) % 8 == 0, "slot layout");
@@ -271,6 +273,37 @@ int es_cambi_set_cvalue_planes(es_cambi *c, float *const dev_planes[5])
     return guarded([&] {
         require(c != nullptr, "es_cambi_set_cvalue_planes: NULL instance");
         for (int s = 0; s < kScales; s++) c->planes[s] = dev_planes ? dev_planes[s] : nullptr;
+    });
+}
+
+int es_cambi_tile_count(int w, int h, int *count)
+{
+    return guarded([&] {
+        require(w > 0 && h > 0 && count != nullptr, "es_cambi_tile_count: bad argument");
+        int n = 0;
+        for (int s = 0; s < kScales; s++) {
+            n += ((w + kCvTX - 1) / kCvTX) * ((h + kCvTY - 1) / kCvTY);
+            w = (w + 1) >> 1;
+            h = (h + 1) >> 1;
+        }
+        *count = n;
+    });
+}
+
+int es_cambi_set_tile_mass(es_cambi *c, uint64_t *dev_mass)
+{
+    return guarded([&] {
+        require(c != nullptr, "es_cambi_set_tile_mass: NULL instance");
+        c->tile_mass = (unsigned long long *)dev_mass;
+    });
+}
+
+int es_cambi_scale_words(const es_cambi *c, int s, uint64_t *address)
+{
+    return guarded([&] {
+        require(c != nullptr && address != nullptr, "es_cambi_scale_words: NULL argument");
+        require(s >= 0 && s < kScales, "es_cambi_scale_words: scale out of range");
+        *address = (uint64_t)c->words[s].ptr;
     });
 }
 

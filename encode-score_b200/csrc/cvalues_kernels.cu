@@ -17,6 +17,7 @@
 // Positive c-values are summed exactly (they are multiples of 2^-24) and counted, and each block appends them to its
 // scale's list (for the top-k selection) through a bounded shared-memory buffer; nothing per pixel is written unless
 // the caller asks for the c-value planes.
+#include "cambi_codes.h"
 #include "es_kernels.h"
 
 namespace es {
@@ -58,21 +59,6 @@ __host__ __device__ inline CvLayout cv_layout(int pad)
     return l;
 }
 
-// the distances d + 1 at which a code's c-value looks (src/kernels.cu:195-197): bit d
-__host__ __device__ inline unsigned cvalue_dists(int code, const Band &bd)
-{
-    const int value = code + bd.band_base + kDiffs;
-    unsigned m = 0;
-    for (int d = 0; d < kDiffs; d++) m |= (unsigned)(value <= bd.tvi[d] && value + d + 1 > bd.vlt) << d;
-    return m;
-}
-__device__ __forceinline__ bool needs_cvalue(int code, const Band &bd) { return cvalue_dists(code, bd) != 0; }
-
-__device__ __forceinline__ uint16_t code_of(unsigned word, const Band &bd)
-{
-    const unsigned u = (word & 0x7FFFu) - (unsigned)bd.band_base;
-    return ((word & kMaskBit) && u < (unsigned)bd.band_size) ? (uint16_t)u : kNone;
-}
 
 // Bytes of `quad` equal to a (ma) and to a + 1 (mb), a even, ta4 = a in every byte: 1 per matching byte.
 __device__ __forceinline__ void pair_match(uint32_t quad, uint32_t ta4, uint32_t &ma, uint32_t &mb)
@@ -95,16 +81,9 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     __shared__ unsigned long long red_sum[kWarps];
     __shared__ unsigned red_cnt[kWarps];
 
+    __shared__ unsigned next_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int j = 0;
-    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
-    const CvJob &J = b.job[j];
     const Band &bd = b.band;
-    const int tile = blockIdx.x - J.first_tile;
-    const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * kCvTY;
-    const int w = J.w, h = J.h, P = J.pad;
-    const int rows = min(kCvTY, h - y0), cols = min(kCvTX, w - x0);
-    const bool vec = (w & 7) == 0 && (((uintptr_t)J.word) & 15) == 0;  // rows of 16-byte vectors
     // the codes whose c-value is needed (some d has value <= tvi[d] and value + d + 1 > vlt): warp w, words w + 8 k
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -114,6 +93,18 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     }
     __syncthreads();
     auto needed = [&](unsigned code) { return (needbits[code >> 5] >> (code & 31)) & 1u; };
+
+  // one tile, gt its global number; all threads return together
+  auto tile_body = [&](const int gt) {
+    int j = 0;
+    while (j + 1 < b.njobs && gt >= b.job[j + 1].first_tile) j++;
+    const CvJob &J = b.job[j];
+    if (b.run && !b.run[J.run_index]) return;
+    const int tile = gt - J.first_tile;
+    const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * kCvTY;
+    const int w = J.w, h = J.h, P = J.pad;
+    const int rows = min(kCvTY, h - y0), cols = min(kCvTX, w - x0);
+    const bool vec = (w & 7) == 0 && (((uintptr_t)J.word) & 15) == 0;  // rows of 16-byte vectors
 
     // 1. does any pixel of the tile need a c-value?
     bool any = false;
@@ -140,7 +131,10 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             }
         }
     }
-    if (!__syncthreads_or(any)) return;
+    if (!__syncthreads_or(any)) {
+        if (b.tile_mass && tid == 0) b.tile_mass[gt] = 0;
+        return;
+    }
 
     const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P), NQ = CS / 128;
     const int xs = ((x0 - P) >> 3) << 3, ox = (x0 - P) - xs;  // region start (aligned) and the offset of x0 - P in it
@@ -488,8 +482,24 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
             atomicAdd(&SL.sum_fx, s);
             atomicAdd(&SL.count, (unsigned long long)c);
         }
+        if (b.tile_mass) b.tile_mass[gt] = s;
     }
     if (list_n) flush();
+  };
+
+    if (!b.tiles) {
+        tile_body((int)blockIdx.x);
+        return;
+    }
+    const unsigned count = *b.tile_count;
+    for (;;) {
+        if (tid == 0) next_tile = atomicAdd(b.tile_next, 1u);
+        __syncthreads();
+        const unsigned i = next_tile;
+        if (i >= count) break;
+        tile_body((int)b.tiles[i]);
+        __syncthreads();
+    }
 }
 
 }  // namespace
@@ -503,7 +513,8 @@ cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s)
     cudaError_t e = cudaFuncSetAttribute(cvalues_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     LaunchTimer t("cambi_cvalues", s);
-    cvalues_kernel<<<b.total_tiles, kCvThreads, smem, s>>>(b);
+    const int grid = b.tiles ? (b.total_tiles < kCvListBlocks ? b.total_tiles : kCvListBlocks) : b.total_tiles;
+    cvalues_kernel<<<grid, kCvThreads, smem, s>>>(b);
     return after_launch();
 }
 

@@ -98,6 +98,7 @@ struct CvJob {
     int tiles_x, first_tile;
     int slot;       // index into the CvSlot array
     float *plane;   // optional: every computed c-value at its pixel
+    int run_index;  // the entry of CvBatch::run that gates this job (with a run table)
 };
 struct CvBatch {
     CvJob job[kMaxJobs];
@@ -105,7 +106,18 @@ struct CvBatch {
     Band band;
     const float *lut;  // lut[i] = 1/i as float, i < (2 max_pad + 1)^2 + 1
     CvSlot *slots;
+    // Optional tile list: the launch then has a fixed grid whose blocks take tiles[*tile_next++] (global tile ids, job
+    // by job as first_tile numbers them) while the counter is below *tile_count; *tile_next must be 0 at launch.
+    const unsigned *tiles;
+    const unsigned *tile_count;
+    unsigned *tile_next;
+    // Optional: per global tile, the exact sum of its positive c-values in 2^-24 units (0 for a tile with none).
+    unsigned long long *tile_mass;
+    // Optional: run[job.run_index] == 0 skips the job's tiles.
+    const int *run;
 };
+// Blocks of a tile-list launch.
+constexpr int kCvListBlocks = 148 * 4;
 constexpr int kCvTX = 64, kCvTY = 64, kCvThreads = 256, kCvBins = 32;
 size_t cvalues_smem_bytes(int max_pad);
 cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s);
@@ -237,5 +249,93 @@ struct CollectBatch {
 constexpr int kCollectSums = 20;  // 18 double sums and 2 counts per block
 int collect_blocks(int windows);
 cudaError_t launch_collect(CollectBatch &b, cudaStream_t s);
+
+// ---- learned tile proposal -------------------------------------------------------------------------------------
+// A 4-layer network of valid 3 x 3 convolutions (2 -> 16 -> 16 -> 16 -> 1, ReLU after the first three) on 4 x 4
+// block features of scale 0 predicts log1p(mean positive c-value) of each 64 x 64 scale-0 tile. Parameters are one
+// float array: per layer the weights [co][ci][3][3], then the biases.
+constexpr int kNetParams = 5089;
+__host__ __device__ constexpr int net_w(int l) { return l == 0 ? 0 : l == 1 ? 304 : l == 2 ? 2624 : 4944; }   // weights of layer l
+__host__ __device__ constexpr int net_b(int l) { return l == 0 ? 288 : l == 1 ? 2608 : l == 2 ? 4928 : 5088; }  // its biases
+constexpr int kFeatTile = 24;  // feature pixels per side around one tile (16 + 2 x 4 halo)
+// mma B fragments of the two 16 -> 16 layers: [layer 1, 2][tap][n tile][register][lane]
+constexpr int kNetFrags = 2 * 9 * 2 * 2 * 32;
+
+struct PredJob {
+    const uint16_t *word;  // scale-0 words of a picture
+    int w, h, tiles_x, tiles_y, first_tile;
+};
+struct PredBatch {
+    PredJob job[kMaxPictures];
+    int njobs, total_tiles;
+    Band band;
+    const float *params;    // bfloat16-rounded parameters (as floats)
+    const uint32_t *frags;  // B fragments of layers 1 and 2
+    float *pred;            // per scale-0 tile: the prediction, -inf where no pixel needs a c-value
+};
+cudaError_t launch_predict(const PredBatch &b, cudaStream_t s);
+
+// Features of n crops: crop i covers scale-0 pixels from (xy[2 i], xy[2 i + 1]) on, fw x fh feature pixels of 4 x 4.
+cudaError_t launch_net_features(const uint16_t *word, int w, int h, const int *xy, int n, int fw, int fh, float *out,
+                                cudaStream_t s);
+// Training on crops (NCHW float): forward of layer l (input n x ci x h x w, output n x co x (h - 2) x (w - 2), ReLU
+// for l < 3); backward of layer l (gradients of its weights and biases into grads and, for l > 0, the gradient of its
+// input times the ReLU mask of that input into gin); the tile loss of the last layer (n x 1 x 16a x 16b against
+// n x a x b labels: per-tile squared differences into loss_parts, the gradient of the last layer's output into gz);
+// and Adam (master weights, their bfloat16-rounded copy, moments).
+cudaError_t launch_net_forward(int layer, const float *in, int n, int h, int w, const float *params, float *out,
+                               cudaStream_t s);
+cudaError_t launch_net_backward(int layer, const float *gout, const float *in, int n, int h, int w, const float *params,
+                                float *gin, float *grads, cudaStream_t s);
+cudaError_t launch_net_loss(const float *z, const float *labels, int n, int ta, int tb, float *gz, float *loss_parts,
+                            cudaStream_t s);
+cudaError_t launch_net_adam(float *params, float *rounded, const float *grads, float *m, float *v, int count, float lr,
+                            float b1, float b2, float eps, int t, cudaStream_t s);
+// The mma B fragments of layers 1 and 2 (kNetFrags words) from the bfloat16-rounded parameters.
+cudaError_t launch_net_pack(const float *rounded, uint32_t *frags, cudaStream_t s);
+
+// The proposal of one frame step over the c-value job table: which tiles of scales 0 and 1 run now (proposed or
+// audited) and which wait for the fallback; scales 2-4 always run.
+constexpr uint8_t kTileSkip = 0, kTileRun = 1, kTileAudit = 2, kTileEmpty = 3;
+struct ProposeJob {
+    int first_tile, tiles_x, tiles_y, scale, picture;
+    int pred_first, pred_tiles_x, pred_tiles_y;  // the picture's scale-0 tile predictions
+};
+struct ProposeBatch {
+    ProposeJob job[kMaxJobs];
+    int njobs, total_tiles;
+    const float *pred;
+    float threshold;
+    unsigned audit_permille[2];           // per scale 0, 1
+    const unsigned long long *frame;      // device: the step's frame number (seeds the audit sample)
+    unsigned *list_a, *count_a;           // tiles to run now
+    unsigned *list_b, *count_b;           // tiles of the fallback
+    uint8_t *kind;                        // per global tile
+    unsigned *n_audit, *n_skip;           // per job (zeroed before the launch, with the counts)
+};
+cudaError_t launch_propose(const ProposeBatch &b, cudaStream_t s);
+struct AuditJob {
+    int job[2];         // the picture's scale-0 and scale-1 jobs in the propose table
+    int first_tile[2];  // their global tile ranges
+    int tiles[2];
+    double k[2];        // their top-k counts
+    int window;
+};
+struct ProposalStats {
+    float estimate;     // estimated change of the score from the skipped tiles
+    int fallback;       // 1: the skipped tiles ran too
+    unsigned run[2], audited[2], skipped[2];
+};
+struct AuditBatch {
+    AuditJob job[kMaxPictures];
+    int njobs;
+    const unsigned long long *tile_mass;
+    const uint8_t *kind;
+    const unsigned *n_audit, *n_skip;
+    double tolerance;
+    int *run;                 // out: per picture, 1 when the fallback runs
+    ProposalStats *stats;     // out: per picture
+};
+cudaError_t launch_audit(const AuditBatch &b, cudaStream_t s);
 
 }  // namespace es

@@ -1,0 +1,601 @@
+// Learned tile proposal for sm_100a: a small network predicts which 64 x 64 tiles of scale 0 carry CAMBI c-values, so
+// the exact c-value kernel runs only on those tiles (and their covering tiles of scale 1) plus a random audit sample,
+// with a fallback to every tile when the audit estimates that the skipped tiles matter. The reference has no
+// counterpart: it computes c-values of every tile (src/kernels.cu:224-278).
+//
+//  * features: per 4 x 4 block of scale-0 words (value | mask << 15), the mean value as (mean - 512) / 256 and the
+//    share of masked pixels (blocks outside the picture are 0);
+//  * training kernels (FP32, SIMT): valid 3 x 3 convolutions forward and backward on crops, the tile loss and Adam;
+//    weights are used rounded to bfloat16;
+//  * predict_kernel: one 128-thread block per scale-0 tile runs all four layers on the tile's 24 x 24 feature window
+//    in shared memory; the two 16 -> 16 layers are bfloat16 tensor-core products (mma.sync m16n8k16, FP32
+//    accumulation, A fragments by ldmatrix from [pixel][16 channel] planes), the first and last layers FP32 SIMT;
+//    tiles with no pixel that needs a c-value get -inf;
+//  * propose_kernel / audit_kernel: the per-step tile lists and the audit's estimate, all on the device.
+#include <cuda_bf16.h>
+
+#include "cambi_codes.h"
+#include "es_kernels.h"
+
+namespace es {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x = lo, in the low half
+    return *(const uint32_t *)&v;
+}
+__device__ __forceinline__ float2 unpack_bf16(uint32_t u)
+{
+    __nv_bfloat162 v;
+    *(uint32_t *)&v = u;
+    return __bfloat1622float2(v);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Features of the 4 x 4 block of scale-0 pixels from (X, Y); with a band, `need` tells whether a pixel of the block
+// needs a c-value.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void block_features(const uint16_t *word, int w, int h, int X, int Y, const Band *bd, float &f0,
+                                               float &f1, bool &need)
+{
+    unsigned sum = 0, n = 0, m = 0;
+    bool nd = false;
+    // 8-byte loads need the row start (word + y w + X) 8-byte aligned: X and w multiples of 4, word 8-byte aligned
+    const bool vec = X >= 0 && X + 4 <= w && (X & 3) == 0 && (w & 3) == 0 && (((uintptr_t)word) & 7) == 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int y = Y + r;
+        if (y < 0 || y >= h) continue;
+        unsigned q[4];
+        int cnt = 0;
+        if (vec) {
+            const uint2 v = __ldg((const uint2 *)(word + (size_t)y * w + X));
+            q[0] = v.x & 0xFFFFu;
+            q[1] = v.x >> 16;
+            q[2] = v.y & 0xFFFFu;
+            q[3] = v.y >> 16;
+            cnt = 4;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int x = X + k;
+                if (x >= 0 && x < w) q[cnt++] = word[(size_t)y * w + x];
+            }
+        }
+        for (int k = 0; k < cnt; k++) {
+            sum += q[k] & 0x7FFFu;
+            m += (q[k] >> 15) & 1u;
+            if (bd) {
+                const uint16_t c = code_of(q[k], *bd);
+                nd |= c != kNone && needs_cvalue(c, *bd);
+            }
+        }
+        n += cnt;
+    }
+    f0 = n ? (float)(((double)sum / (double)n - 512.0) / 256.0) : 0.0f;
+    f1 = (float)((double)m / 16.0);
+    need = nd;
+}
+
+__global__ void __launch_bounds__(256) net_features_kernel(const uint16_t *word, int w, int h, const int *xy, int n, int fw,
+                                                           int fh, float *out)
+{
+    const size_t per = (size_t)fw * fh, total = per * n;
+    for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < total; i += (size_t)gridDim.x * 256) {
+        const int c = (int)(i / per), r = (int)(i - (size_t)c * per), v = r / fw, u = r - v * fw;
+        float f0, f1;
+        bool need;
+        block_features(word, w, h, xy[2 * c] + 4 * u, xy[2 * c + 1] + 4 * v, nullptr, f0, f1, need);
+        out[(size_t)c * 2 * per + r] = f0;
+        out[(size_t)c * 2 * per + per + r] = f1;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Training: valid 3 x 3 convolutions on NCHW float crops, weights rounded to bfloat16.
+// ---------------------------------------------------------------------------------------------------------------
+template <int CI, int CO>
+__global__ void __launch_bounds__(256) conv_fwd_kernel(const float *in, int n, int h, int w, const float *P, int woff, int boff,
+                                                       bool relu, float *out)
+{
+    __shared__ float W[CO * CI * 9], B[CO];
+    for (int i = threadIdx.x; i < CO * CI * 9; i += 256) W[i] = bf16r(P[woff + i]);
+    for (int i = threadIdx.x; i < CO; i += 256) B[i] = bf16r(P[boff + i]);
+    __syncthreads();
+    const int ho = h - 2, wo = w - 2;
+    const size_t plane = (size_t)ho * wo, total = plane * n;
+    for (size_t idx = (size_t)blockIdx.x * 256 + threadIdx.x; idx < total; idx += (size_t)gridDim.x * 256) {
+        const int nn = (int)(idx / plane), r = (int)(idx - (size_t)nn * plane), y = r / wo, x = r - y * wo;
+        float acc[CO];
+#pragma unroll
+        for (int co = 0; co < CO; co++) acc[co] = B[co];
+        for (int ci = 0; ci < CI; ci++) {
+            const float *src = in + ((size_t)(nn * CI + ci) * h + y) * w + x;
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                const float v = src[(k / 3) * w + (k % 3)];
+#pragma unroll
+                for (int co = 0; co < CO; co++) acc[co] = __fmaf_rn(v, W[(co * CI + ci) * 9 + k], acc[co]);
+            }
+        }
+#pragma unroll
+        for (int co = 0; co < CO; co++)
+            out[((size_t)(nn * CO + co) * ho + y) * wo + x] = relu ? fmaxf(acc[co], 0.0f) : acc[co];
+    }
+}
+
+// gin = (full correlation of gout with the flipped kernel) x (in > 0): the gradient of the layer's input, through the
+// ReLU that produced it.
+template <int CI, int CO>
+__global__ void __launch_bounds__(256) conv_bwd_data_kernel(const float *gout, const float *in, int n, int h, int w,
+                                                            const float *P, int woff, float *gin)
+{
+    __shared__ float W[CO * CI * 9];
+    for (int i = threadIdx.x; i < CO * CI * 9; i += 256) W[i] = bf16r(P[woff + i]);
+    __syncthreads();
+    const int ho = h - 2, wo = w - 2;
+    const size_t plane = (size_t)h * w, total = plane * n;
+    for (size_t idx = (size_t)blockIdx.x * 256 + threadIdx.x; idx < total; idx += (size_t)gridDim.x * 256) {
+        const int nn = (int)(idx / plane), r = (int)(idx - (size_t)nn * plane), y = r / w, x = r - y * w;
+        float acc[CI];
+#pragma unroll
+        for (int ci = 0; ci < CI; ci++) acc[ci] = 0.0f;
+        for (int co = 0; co < CO; co++) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                const int oy = y - k / 3, ox = x - k % 3;
+                if (oy < 0 || oy >= ho || ox < 0 || ox >= wo) continue;
+                const float g = gout[((size_t)(nn * CO + co) * ho + oy) * wo + ox];
+#pragma unroll
+                for (int ci = 0; ci < CI; ci++) acc[ci] = __fmaf_rn(g, W[(co * CI + ci) * 9 + k], acc[ci]);
+            }
+        }
+#pragma unroll
+        for (int ci = 0; ci < CI; ci++) {
+            const size_t at = ((size_t)(nn * CI + ci) * h + y) * w + x;
+            gin[at] = in[at] > 0.0f ? acc[ci] : 0.0f;
+        }
+    }
+}
+
+// One block per (co, ci): the 9 weight gradients (and the bias gradient when ci == 0), summed in a fixed order.
+template <int CI, int CO>
+__global__ void __launch_bounds__(256) conv_bwd_weight_kernel(const float *gout, const float *in, int n, int h, int w,
+                                                              float *G, int woff, int boff)
+{
+    __shared__ float part[8][10];
+    const int co = blockIdx.x / CI, ci = blockIdx.x % CI;
+    const int ho = h - 2, wo = w - 2;
+    const size_t plane = (size_t)ho * wo, total = plane * n;
+    float acc[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) acc[k] = 0.0f;
+    for (size_t idx = threadIdx.x; idx < total; idx += 256) {
+        const int nn = (int)(idx / plane), r = (int)(idx - (size_t)nn * plane), y = r / wo, x = r - y * wo;
+        const float g = gout[((size_t)(nn * CO + co) * ho + y) * wo + x];
+        const float *src = in + ((size_t)(nn * CI + ci) * h + y) * w + x;
+#pragma unroll
+        for (int k = 0; k < 9; k++) acc[k] = __fmaf_rn(g, src[(k / 3) * w + (k % 3)], acc[k]);
+        acc[9] += g;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+        float v = acc[k];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        if (lane == 0) part[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 10) {
+        float s = 0.0f;
+        for (int k = 0; k < 8; k++) s += part[k][threadIdx.x];
+        if (threadIdx.x < 9) G[woff + (co * CI + ci) * 9 + threadIdx.x] = s;
+        else if (ci == 0) G[boff + co] = s;
+    }
+}
+
+// One block per crop: the mean of each 16 x 16 block of z against its label; gz = d loss / d z with
+// loss = mean over all tiles of (mean - label)^2.
+__global__ void __launch_bounds__(256) net_loss_kernel(const float *z, const float *labels, int n, int ta, int tb, float *gz,
+                                                       float *loss_parts)
+{
+    const int c = blockIdx.x, W = 16 * tb, H = 16 * ta, tiles = ta * tb;
+    const float scale = 2.0f / (float)(n * tiles) / 256.0f;
+    const int row = threadIdx.x & 15;
+    for (int t0 = 0; t0 < tiles; t0 += 16) {  // the same trip count for every thread: the shuffles see full warps
+        const int t = t0 + (threadIdx.x >> 4), by = t / tb, bx = t % tb;
+        const bool on = t < tiles;
+        float s = 0.0f;
+        if (on) {
+            const float *src = z + (size_t)c * H * W + (size_t)(16 * by + row) * W + 16 * bx;
+#pragma unroll
+            for (int k = 0; k < 16; k++) s += src[k];
+        }
+#pragma unroll
+        for (int o = 8; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+        if (!on) continue;
+        const float d = s / 256.0f - labels[(size_t)c * tiles + t];
+        if (row == 0) loss_parts[(size_t)c * tiles + t] = d * d;
+        float *dst = gz + (size_t)c * H * W + (size_t)(16 * by + row) * W + 16 * bx;
+#pragma unroll
+        for (int k = 0; k < 16; k++) dst[k] = d * scale;
+    }
+}
+
+__global__ void net_adam_kernel(float *P, float *R, const float *G, float *M, float *V, int count, float lr, float b1, float b2,
+                                float eps, int t)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float g = G[i];
+    const float m = b1 * M[i] + (1.0f - b1) * g, v = b2 * V[i] + (1.0f - b2) * g * g;
+    M[i] = m;
+    V[i] = v;
+    const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
+    const float p = P[i] - lr * (m / c1) / (sqrtf(v / c2) + eps);
+    P[i] = p;
+    R[i] = bf16r(p);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Inference: one block of 128 threads per scale-0 tile, all four layers in shared memory.
+// ---------------------------------------------------------------------------------------------------------------
+constexpr int kPT = 128;
+struct PredSmem {
+    float f[2][kFeatTile][kFeatTile];             // features
+    float w0[304], w3[145];                       // layers 0 and 3, weights then biases (bfloat16 values)
+    float b12[2][16];
+    __align__(16) uint32_t a1[22 * 22 * 8];       // layer-0 output, [pixel][16 channels] bfloat16; later layer 2's
+    __align__(16) uint32_t a2[20 * 20 * 8];       // layer-1 output
+    uint32_t frags[kNetFrags];                    // B fragments of layers 1 and 2, [layer][tap][n tile][reg][lane]
+    float part[kPT / 32];
+};
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+// One 16 -> 16 layer: input plane `in` (iw x iw pixels of 16 bfloat16 channels, 32 bytes each), output plane `out`
+// (ow x ow, ow = iw - 2), bias, ReLU, bfloat16. Warp w takes m tiles w, w + 4, ...: 16 output pixels each, numbered
+// row by row; rows past the last pixel read a valid pixel and are not stored. frags: this layer's B fragments.
+__device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *out, int ow, const uint32_t *frags,
+                                          const float *bias)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int npx = ow * ow, tiles = (npx + 15) / 16;
+    const int g = lane >> 2, t = lane & 3;
+    const int mrow = ((lane >> 3) & 1) * 8 + (lane & 7), khalf = lane >> 4;  // this lane's ldmatrix row and k half
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(in);
+    for (int mt = warp; mt < tiles; mt += kPT / 32) {
+        const int p = min(16 * mt + mrow, npx - 1);
+        const int oy = p / ow, ox = p - oy * ow;
+        float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const int q = (oy + k / 3) * iw + ox + k % 3;
+            uint32_t a0, a1, a2, a3;
+            ldmatrix_x4(base + q * 32 + khalf * 16, a0, a1, a2, a3);
+            const uint32_t *fk = frags + k * 4 * 32 + lane;  // this tap's fragments: (n tile, register) x lane
+            mma_bf16(c[0], a0, a1, a2, a3, fk[0], fk[32]);
+            mma_bf16(c[1], a0, a1, a2, a3, fk[64], fk[96]);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int ch = 8 * j + 2 * t;
+#pragma unroll
+            for (int hrow = 0; hrow < 2; hrow++) {
+                const int pr = 16 * mt + g + 8 * hrow;
+                if (pr >= npx) continue;
+                const float v0 = fmaxf(c[j][2 * hrow] + bias[ch], 0.0f), v1 = fmaxf(c[j][2 * hrow + 1] + bias[ch + 1], 0.0f);
+                out[pr * 8 + ch / 2] = pack_bf16(v0, v1);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ PredBatch b)
+{
+    __shared__ PredSmem sm;
+    const int tid = threadIdx.x;
+    int j = 0;
+    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
+    const PredJob &J = b.job[j];
+    const int tile = blockIdx.x - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
+    const int X0 = 64 * tx - 16, Y0 = 64 * ty - 16;
+    // features of the 24 x 24 window, and whether a pixel of the tile itself needs a c-value
+    bool need = false;
+    for (int i = tid; i < kFeatTile * kFeatTile; i += kPT) {
+        const int v = i / kFeatTile, u = i - v * kFeatTile;
+        float f0, f1;
+        bool nd;
+        const bool own = u >= 4 && u < 20 && v >= 4 && v < 20;
+        block_features(J.word, J.w, J.h, X0 + 4 * u, Y0 + 4 * v, own ? &b.band : nullptr, f0, f1, nd);
+        sm.f[0][v][u] = f0;
+        sm.f[1][v][u] = f1;
+        need |= nd;
+    }
+    for (int i = tid; i < 304; i += kPT) sm.w0[i] = b.params[net_w(0) + i];
+    for (int i = tid; i < 145; i += kPT) sm.w3[i] = b.params[net_w(3) + i];
+    if (tid < 32) sm.b12[tid >> 4][tid & 15] = b.params[(tid < 16 ? net_b(1) : net_b(2)) + (tid & 15)];
+    for (int i = tid; i < kNetFrags; i += kPT) sm.frags[i] = b.frags[i];
+    if (!__syncthreads_or(need)) {
+        if (tid == 0) b.pred[blockIdx.x] = -INFINITY;
+        return;
+    }
+    // layer 0: 2 -> 16, 22 x 22 outputs
+    for (int p = tid; p < 22 * 22; p += kPT) {
+        const int y = p / 22, x = p - y * 22;
+        float acc[16];
+#pragma unroll
+        for (int co = 0; co < 16; co++) acc[co] = sm.w0[288 + co];
+#pragma unroll 1
+        for (int ck = 0; ck < 18; ck++) {  // input channel ci = ck / 9, tap k = ck % 9
+            const int ci = ck / 9, k = ck - 9 * ci;
+            const float v = sm.f[ci][y + k / 3][x + k % 3];
+#pragma unroll
+            for (int co = 0; co < 16; co++) acc[co] = __fmaf_rn(v, sm.w0[(co * 2 + ci) * 9 + k], acc[co]);
+        }
+        uint4 *dst = (uint4 *)(sm.a1 + p * 8);
+        dst[0] = make_uint4(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)), pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)),
+                            pack_bf16(fmaxf(acc[4], 0.f), fmaxf(acc[5], 0.f)), pack_bf16(fmaxf(acc[6], 0.f), fmaxf(acc[7], 0.f)));
+        dst[1] = make_uint4(pack_bf16(fmaxf(acc[8], 0.f), fmaxf(acc[9], 0.f)), pack_bf16(fmaxf(acc[10], 0.f), fmaxf(acc[11], 0.f)),
+                            pack_bf16(fmaxf(acc[12], 0.f), fmaxf(acc[13], 0.f)), pack_bf16(fmaxf(acc[14], 0.f), fmaxf(acc[15], 0.f)));
+    }
+    __syncthreads();
+    mma_layer(sm.a1, 22, sm.a2, 20, sm.frags, sm.b12[0]);                   // layer 1: 20 x 20
+    __syncthreads();
+    mma_layer(sm.a2, 20, sm.a1, 18, sm.frags + 9 * 2 * 2 * 32, sm.b12[1]);  // layer 2: 18 x 18, into a1
+    __syncthreads();
+    // layer 3: 16 -> 1 on 16 x 16, then the tile mean (a fixed order of additions)
+    float s = 0.0f;
+    for (int p = tid; p < 256; p += kPT) {
+        const int y = p >> 4, x = p & 15;
+        float acc = sm.w3[144];
+#pragma unroll 1
+        for (int k = 0; k < 9; k++) {
+            const uint32_t *src = sm.a1 + ((y + k / 3) * 18 + x + k % 3) * 8;
+#pragma unroll
+            for (int c2 = 0; c2 < 8; c2++) {
+                const float2 v = unpack_bf16(src[c2]);
+                acc = __fmaf_rn(v.x, sm.w3[(2 * c2) * 9 + k], acc);
+                acc = __fmaf_rn(v.y, sm.w3[(2 * c2 + 1) * 9 + k], acc);
+            }
+        }
+        s += acc;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if ((tid & 31) == 0) sm.part[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) b.pred[blockIdx.x] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Proposal and audit of a frame step.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x)
+{
+    // SplitMix64's finaliser (Steele, Lea and Flood 2014)
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__global__ void __launch_bounds__(256) propose_kernel(const __grid_constant__ ProposeBatch b)
+{
+    const unsigned long long frame = *b.frame;
+    for (int gt = blockIdx.x * 256 + threadIdx.x; gt < b.total_tiles; gt += gridDim.x * 256) {
+        int j = 0;
+        while (j + 1 < b.njobs && gt >= b.job[j + 1].first_tile) j++;
+        const ProposeJob &J = b.job[j];
+        const int tile = gt - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
+        uint8_t kind = kTileRun;
+        if (J.scale < 2) {
+            const int s = J.scale;
+            float best = -INFINITY;
+            for (int y = ty << s; y < min((ty + 1) << s, J.pred_tiles_y); y++)
+                for (int x = tx << s; x < min((tx + 1) << s, J.pred_tiles_x); x++)
+                    best = fmaxf(best, b.pred[J.pred_first + y * J.pred_tiles_x + x]);
+            if (best == -INFINITY) {
+                kind = kTileEmpty;  // scale 0: nothing to compute; scale 1: left to the fallback, unaudited
+            } else if (best < b.threshold) {
+                const unsigned long long hsh = mix64(frame * 0x100000001B3ull ^ ((unsigned long long)J.picture << 40) ^
+                                                     ((unsigned long long)s << 36) ^ (unsigned long long)tile);
+                kind = (unsigned)(hsh % 1000ull) < b.audit_permille[s] ? kTileAudit : kTileSkip;
+            }
+            if (kind == kTileAudit) atomicAdd(&b.n_audit[j], 1u);
+            if (kind == kTileSkip) atomicAdd(&b.n_skip[j], 1u);
+        }
+        b.kind[gt] = kind;
+        if (kind == kTileRun || kind == kTileAudit) b.list_a[atomicAdd(b.count_a, 1u)] = (unsigned)gt;
+        else if (kind == kTileSkip || (kind == kTileEmpty && J.scale == 1)) b.list_b[atomicAdd(b.count_b, 1u)] = (unsigned)gt;
+    }
+}
+
+// One block per picture: the audited tiles' c-value mass, scaled up to the skipped tiles, as a change of the score.
+__global__ void __launch_bounds__(256) audit_kernel(const __grid_constant__ AuditBatch b)
+{
+    __shared__ unsigned long long part[8];
+    __shared__ unsigned part_run[8];
+    const AuditJob &J = b.job[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double weight[2] = {16.0, 8.0};
+    double est = 0.0;
+    ProposalStats st{};
+    for (int s = 0; s < 2; s++) {
+        unsigned long long mass = 0;
+        unsigned run = 0;
+        for (int t = threadIdx.x; t < J.tiles[s]; t += 256) {
+            const int gt = J.first_tile[s] + t;
+            const uint8_t k = b.kind[gt];
+            if (k == kTileAudit) mass += b.tile_mass[gt];
+            run += k == kTileRun || k == kTileAudit;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            mass += __shfl_xor_sync(kFull, mass, o);
+            run += __shfl_xor_sync(kFull, run, o);
+        }
+        if (lane == 0) {
+            part[warp] = mass;
+            part_run[warp] = run;
+        }
+        __syncthreads();
+        unsigned long long total = 0;
+        unsigned runs = 0;
+        for (int k = 0; k < 8; k++) {
+            total += part[k];
+            runs += part_run[k];
+        }
+        __syncthreads();
+        const unsigned na = b.n_audit[J.job[s]], ns = b.n_skip[J.job[s]];
+        st.run[s] = runs - na;
+        st.audited[s] = na;
+        st.skipped[s] = ns;
+        if (na > 0 && ns > 0) {
+            const double missing = (double)total / 16777216.0 * ((double)ns / (double)na);
+            est += weight[s] * missing / J.k[s] / ((double)J.window * (double)J.window);
+        }
+    }
+    if (threadIdx.x == 0) {
+        const int fb = est > b.tolerance;
+        b.run[blockIdx.x] = fb;
+        st.estimate = (float)est;
+        st.fallback = fb;
+        b.stats[blockIdx.x] = st;
+    }
+}
+
+// B fragments of layers 1 and 2 from the rounded parameters: word [l][k][j][r][lane] holds, for output channel
+// n = 8 j + lane / 4 and input channels c = 2 (lane % 4) + 8 r and c + 1, the two weights of tap k (low half: c).
+__global__ void net_pack_kernel(const float *R, uint32_t *frags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kNetFrags) return;
+    const int lane = i & 31, r = (i >> 5) & 1, j = (i >> 6) & 1, k = (i >> 7) % 9, l = 1 + (i >> 7) / 9;
+    const int n = 8 * j + (lane >> 2), c = 2 * (lane & 3) + 8 * r;
+    const float *W = R + net_w(l);
+    frags[i] = pack_bf16(W[(n * 16 + c) * 9 + k], W[(n * 16 + c + 1) * 9 + k]);
+}
+
+unsigned grid_for(size_t total) { return (unsigned)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16); }
+
+}  // namespace
+
+cudaError_t launch_predict(const PredBatch &b, cudaStream_t s)
+{
+    if (b.total_tiles <= 0) return cudaSuccess;
+    LaunchTimer t("proposal_predict", s);
+    predict_kernel<<<b.total_tiles, kPT, 0, s>>>(b);
+    return after_launch();
+}
+
+cudaError_t launch_net_features(const uint16_t *word, int w, int h, const int *xy, int n, int fw, int fh, float *out,
+                                cudaStream_t s)
+{
+    const size_t total = (size_t)fw * fh * n;
+    if (!total) return cudaSuccess;
+    LaunchTimer t("proposal_features", s);
+    net_features_kernel<<<grid_for(total), 256, 0, s>>>(word, w, h, xy, n, fw, fh, out);
+    return after_launch();
+}
+
+cudaError_t launch_net_forward(int layer, const float *in, int n, int h, int w, const float *params, float *out, cudaStream_t s)
+{
+    const size_t total = (size_t)(h - 2) * (w - 2) * n;
+    if (!total) return cudaSuccess;
+    LaunchTimer t("proposal_train_forward", s);
+    const unsigned g = grid_for(total);
+    switch (layer) {
+    case 0: conv_fwd_kernel<2, 16><<<g, 256, 0, s>>>(in, n, h, w, params, net_w(0), net_b(0), true, out); break;
+    case 1: conv_fwd_kernel<16, 16><<<g, 256, 0, s>>>(in, n, h, w, params, net_w(1), net_b(1), true, out); break;
+    case 2: conv_fwd_kernel<16, 16><<<g, 256, 0, s>>>(in, n, h, w, params, net_w(2), net_b(2), true, out); break;
+    case 3: conv_fwd_kernel<16, 1><<<g, 256, 0, s>>>(in, n, h, w, params, net_w(3), net_b(3), false, out); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return after_launch();
+}
+
+cudaError_t launch_net_backward(int layer, const float *gout, const float *in, int n, int h, int w, const float *params,
+                                float *gin, float *grads, cudaStream_t s)
+{
+    LaunchTimer t("proposal_train_backward", s);
+    const unsigned g = grid_for((size_t)h * w * n);
+    switch (layer) {
+    case 0: conv_bwd_weight_kernel<2, 16><<<16 * 2, 256, 0, s>>>(gout, in, n, h, w, grads, net_w(0), net_b(0)); break;
+    case 1:
+        conv_bwd_weight_kernel<16, 16><<<256, 256, 0, s>>>(gout, in, n, h, w, grads, net_w(1), net_b(1));
+        count_launch();
+        conv_bwd_data_kernel<16, 16><<<g, 256, 0, s>>>(gout, in, n, h, w, params, net_w(1), gin);
+        break;
+    case 2:
+        conv_bwd_weight_kernel<16, 16><<<256, 256, 0, s>>>(gout, in, n, h, w, grads, net_w(2), net_b(2));
+        count_launch();
+        conv_bwd_data_kernel<16, 16><<<g, 256, 0, s>>>(gout, in, n, h, w, params, net_w(2), gin);
+        break;
+    case 3:
+        conv_bwd_weight_kernel<16, 1><<<16, 256, 0, s>>>(gout, in, n, h, w, grads, net_w(3), net_b(3));
+        count_launch();
+        conv_bwd_data_kernel<16, 1><<<g, 256, 0, s>>>(gout, in, n, h, w, params, net_w(3), gin);
+        break;
+    default: return cudaErrorInvalidValue;
+    }
+    return after_launch();
+}
+
+cudaError_t launch_net_loss(const float *z, const float *labels, int n, int ta, int tb, float *gz, float *loss_parts, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    LaunchTimer t("proposal_train_loss", s);
+    net_loss_kernel<<<n, 256, 0, s>>>(z, labels, n, ta, tb, gz, loss_parts);
+    return after_launch();
+}
+
+cudaError_t launch_net_adam(float *params, float *rounded, const float *grads, float *m, float *v, int count, float lr, float b1,
+                            float b2, float eps, int t, cudaStream_t s)
+{
+    LaunchTimer tm("proposal_train_adam", s);
+    net_adam_kernel<<<(count + 255) / 256, 256, 0, s>>>(params, rounded, grads, m, v, count, lr, b1, b2, eps, t);
+    return after_launch();
+}
+
+cudaError_t launch_net_pack(const float *rounded, uint32_t *frags, cudaStream_t s)
+{
+    LaunchTimer t("proposal_pack", s);
+    net_pack_kernel<<<(kNetFrags + 255) / 256, 256, 0, s>>>(rounded, frags);
+    return after_launch();
+}
+
+cudaError_t launch_propose(const ProposeBatch &b, cudaStream_t s)
+{
+    if (b.total_tiles <= 0) return cudaSuccess;
+    LaunchTimer t("proposal_lists", s);
+    propose_kernel<<<(b.total_tiles + 255) / 256, 256, 0, s>>>(b);
+    return after_launch();
+}
+
+cudaError_t launch_audit(const AuditBatch &b, cudaStream_t s)
+{
+    if (b.njobs <= 0) return cudaSuccess;
+    LaunchTimer t("proposal_audit", s);
+    audit_kernel<<<b.njobs, 256, 0, s>>>(b);
+    return after_launch();
+}
+
+}  // namespace es

@@ -24,7 +24,9 @@ SYMBOLS = (
     "es_last_error", "es_version", "es_launch_count", "es_kernel_timing", "es_kernel_times", "es_module_load", "es_module_unload", "es_module_get", "es_module_launch",
     "es_cambi_create", "es_cambi_create_with", "es_cambi_derive_params", "es_cambi_get_params", "es_cambi_launch",
     "es_cambi_finish", "es_cambi_destroy", "es_cambi_scale_stats", "es_cambi_read_scale", "es_cambi_set_cvalue_planes",
-    "es_cambi_score_noalloc",
+    "es_cambi_score_noalloc", "es_cambi_tile_count", "es_cambi_set_tile_mass", "es_cambi_scale_words",
+    "es_proposal_net_create", "es_proposal_net_get", "es_proposal_net_train_step", "es_proposal_features",
+    "es_proposal_predict", "es_proposal_net_destroy",
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
     "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
@@ -136,6 +138,15 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.POINTER(Accum)), ctypes.POINTER(FrameResult)]
         L.es_frame_read_windows.argtypes = [P, I, P, P]
         L.es_frame_destroy.argtypes = [P]
+        L.es_cambi_tile_count.argtypes = [I, I, ctypes.POINTER(I)]
+        L.es_cambi_set_tile_mass.argtypes = [P, P]
+        L.es_cambi_scale_words.argtypes = [P, I, ctypes.POINTER(U64)]
+        L.es_proposal_net_create.argtypes = [P, U64, ctypes.POINTER(P)]
+        L.es_proposal_net_get.argtypes = [P, P]
+        L.es_proposal_net_train_step.argtypes = [P, P, P, I, I, I, ctypes.c_float, ctypes.POINTER(ctypes.c_double), P, P]
+        L.es_proposal_features.argtypes = [U64, I, I, P, I, I, I, P, P]
+        L.es_proposal_predict.argtypes = [P, U64, I, I, P, P]
+        L.es_proposal_net_destroy.argtypes = [P]
         L.es_batch_create.argtypes = [P, I, ctypes.POINTER(BatchSource), ctypes.POINTER(BatchOptions), ctypes.POINTER(P)]
         L.es_batch_queue.argtypes = [P, ctypes.c_long, ctypes.POINTER(FrameView), ctypes.POINTER(I), ctypes.POINTER(I), P]
         L.es_batch_collect.argtypes = [P, ctypes.c_long, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.POINTER(Accum)),
@@ -245,6 +256,15 @@ class Cambi:
         check(lib().es_cambi_read_scale(self.handle, s, image.ctypes.data, mask.ctypes.data))
         return image, mask
 
+    def set_tile_mass(self, ptr: int | None) -> None:
+        """Per-tile exact c-value sums (2^-24 units) of later launches into the device array at ptr."""
+        check(lib().es_cambi_set_tile_mass(self.handle, ctypes.c_void_p(ptr) if ptr else None))
+
+    def scale_words(self, s: int) -> int:
+        out = ctypes.c_uint64()
+        check(lib().es_cambi_scale_words(self.handle, s, ctypes.byref(out)))
+        return out.value
+
     def set_cvalue_planes(self, ptrs: list | None) -> None:
         arr = (ctypes.c_void_p * SCALES)(*(ptrs or [None] * SCALES))
         check(lib().es_cambi_set_cvalue_planes(self.handle, arr if ptrs else None))
@@ -253,6 +273,58 @@ class Cambi:
         if self.handle:
             lib().es_cambi_destroy(self.handle)
             self.handle = ctypes.c_void_p()
+
+
+def cambi_tile_count(w: int, h: int) -> int:
+    out = ctypes.c_int()
+    check(lib().es_cambi_tile_count(w, h, ctypes.byref(out)))
+    return out.value
+
+
+PROPOSAL_PARAMS = 5089
+
+
+class ProposalNet:
+    """The tile-proposal network on the device (es_proposal_net_*)."""
+
+    def __init__(self, params=None, seed: int = 0):
+        import numpy as np
+        self.handle = ctypes.c_void_p()
+        arr = None
+        if params is not None:
+            self._p = np.ascontiguousarray(params, np.float32)
+            assert self._p.size == PROPOSAL_PARAMS
+            arr = self._p.ctypes.data
+        check(lib().es_proposal_net_create(arr, seed, ctypes.byref(self.handle)))
+
+    def params(self):
+        import numpy as np
+        out = np.zeros(PROPOSAL_PARAMS, np.float32)
+        check(lib().es_proposal_net_get(self.handle, out.ctypes.data))
+        return out
+
+    def train_step(self, x: int, labels: int, n: int, h: int, w: int, lr: float, stream: int = 0, want_loss: bool = True,
+                   want_grads: bool = False):
+        """x, labels: device addresses. Returns (loss or None, grads or None)."""
+        import numpy as np
+        loss = ctypes.c_double()
+        grads = np.zeros(PROPOSAL_PARAMS, np.float32) if want_grads else None
+        check(lib().es_proposal_net_train_step(self.handle, ctypes.c_void_p(x), ctypes.c_void_p(labels), n, h, w, lr,
+                                               ctypes.byref(loss) if want_loss else None,
+                                               grads.ctypes.data if want_grads else None, ctypes.c_void_p(stream)))
+        return (loss.value if want_loss else None), grads
+
+    def predict(self, words: int, w: int, h: int, pred: int, stream: int = 0) -> None:
+        check(lib().es_proposal_predict(self.handle, words, w, h, ctypes.c_void_p(pred), ctypes.c_void_p(stream)))
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_proposal_net_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+def proposal_features(words: int, w: int, h: int, xy: int, n: int, fw: int, fh: int, out: int, stream: int = 0) -> None:
+    check(lib().es_proposal_features(words, w, h, ctypes.c_void_p(xy), n, fw, fh, ctypes.c_void_p(out), ctypes.c_void_p(stream)))
 
 
 def cambi_score_noalloc(img: int, pitch: int, w: int, h: int, depth: int, score_dev: int, stream: int = 0) -> None:

@@ -103,6 +103,15 @@ int es_cambi_read_scale(const es_cambi *c, int s, uint16_t *image, uint8_t *mask
  * computed c-value there (the buffer kernels.cu's cambi_cvalues fills). NULL entries switch it off per scale. */
 int es_cambi_set_cvalue_planes(es_cambi *c, float *const dev_planes[5]);
 
+/* Introspection with no counterpart in the reference: the number of 64 x 64 c-value tiles of all five scales of a
+ * w x h picture (scale 0's first, row by row, then scale 1's, ...). */
+int es_cambi_tile_count(int w, int h, int *count);
+/* With dev_mass a device array of es_cambi_tile_count entries, later launches write each tile's exact sum of positive
+ * c-values there, in units of 2^-24 (the labels of the tile-proposal network); NULL switches it off. */
+int es_cambi_set_tile_mass(es_cambi *c, uint64_t *dev_mass);
+/* The device address of scale s's words (value | mask << 15, sw x sh): valid until the instance's next launch. */
+int es_cambi_scale_words(const es_cambi *c, int s, uint64_t *address);
+
 /* No counterpart in the reference. The CAMBI score of one plane, like es_cambi_create + es_cambi_launch +
  * es_cambi_finish, for callers that must not allocate device memory when they score a picture: plugins whose host
  * application owns the device memory budget, and latency-critical paths where cudaMalloc's implicit device
@@ -194,6 +203,33 @@ int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es
  * src/kernels.cu:434); either pointer may be NULL. */
 int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist);
 void es_frame_destroy(es_frame *fr);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Learned tile proposal: no counterpart in the reference, which computes the c-values of every tile. A network of
+ * four valid 3 x 3 convolutions (2 -> 16 -> 16 -> 16 -> 1, ReLU after the first three, bfloat16 weights, FP32
+ * accumulation) reads 4 x 4 block features of CAMBI's scale-0 words -- the mean value as (mean - 512) / 256 and the
+ * share of masked pixels -- and predicts log1p(mean positive c-value) of each 64 x 64 scale-0 tile. Parameters are
+ * ES_PROPOSAL_PARAMS floats: per layer the weights [co][ci][3][3], then the biases.
+ * --------------------------------------------------------------------------------------------------------------- */
+#define ES_PROPOSAL_PARAMS 5089
+typedef struct es_proposal_net es_proposal_net;
+/* params: ES_PROPOSAL_PARAMS host floats, or NULL for He-initialised weights drawn with `seed`. */
+int es_proposal_net_create(const float *params, uint64_t seed, es_proposal_net **out);
+/* Copies the FP32 master parameters to params (host, ES_PROPOSAL_PARAMS floats). */
+int es_proposal_net_get(const es_proposal_net *net, float *params);
+/* One training step on n crops: x (device, n x 2 x h x w floats of features, h and w = 8 + 16 k), labels (device,
+ * n x (h - 8) / 16 x (w - 8) / 16 floats). Computes the loss (mean squared error of the tile means, written to *loss
+ * when not NULL) and the gradients (copied to the host array grads when not NULL), then takes an Adam step
+ * (b1 0.9, b2 0.999, eps 1e-8) when lr > 0. Waits for the stream when loss or grads is asked for. */
+int es_proposal_net_train_step(es_proposal_net *net, const float *x, const float *labels, int n, int h, int w, float lr,
+                               double *loss, float *grads, void *stream);
+/* Features of n crops of a picture's scale-0 words (device, w x h): crop i starts at pixel (xy[2i], xy[2i+1]) (device
+ * ints, may be negative) and has fw x fh feature pixels; out (device) receives n x 2 x fh x fw floats. */
+int es_proposal_features(uint64_t words, int w, int h, const int *xy, int n, int fw, int fh, float *out, void *stream);
+/* The prediction of every scale-0 tile of a picture's scale-0 words (device) by the fused inference kernel: pred
+ * (device, ceil(h / 64) x ceil(w / 64) floats), -inf for tiles where no pixel needs a c-value. */
+int es_proposal_predict(es_proposal_net *net, uint64_t words, int w, int h, float *pred, void *stream);
+void es_proposal_net_destroy(es_proposal_net *net);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Batched frame steps: no counterpart in the reference, which scores one source per process with one launch per
