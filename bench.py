@@ -345,6 +345,21 @@ def main() -> None:
         def close(self):
             self.b.close()
 
+    class LearnedForm(BatchedForm):
+        name = ("batched + learned proposal (es_batch with es_batch_set_proposal: c-values of scales 0-1 on the network's "
+                "proposed tiles plus a 5%/20% audit, fallback to every tile above an estimated 0.025 change of CAMBI)")
+
+        def __init__(self):
+            super().__init__()
+            import eval_proposal
+            self.net, meta = eval_proposal.load_net(es_b200)
+            self.threshold = meta["threshold"]
+            self.b.set_proposal(self.net, threshold=self.threshold)
+
+        def close(self):
+            super().close()
+            self.net.close()
+
     def time_form(form, f0: int) -> tuple[float, int, dict | None, int]:
         """Warm-up, then args.steps timed steps of `form` over the device pool; returns (ms, launches, clocks, next f).
         The warm-up covers the first 14 frames, so the batched form replays graphs in the timed region."""
@@ -392,12 +407,20 @@ def main() -> None:
                         "gpu_launches": int(launches_b)}
     head = "batched"
     ms, launches = ms_b, launches_b
+    if os.path.exists(os.path.join(ROOT, "encode-score_b200", "proposal_net.npy")):
+        learned = LearnedForm()
+        ms_l, launches_l, clk, _ = time_form(learned, 0)
+        learned.close()
+        forms["learned"] = {"value": pairs / (ms_l / 1000.0), "ms_per_step": ms_l / args.steps, "form": learned.name,
+                            "gpu_launches": int(launches_l), "threshold": learned.threshold}
+        head = "learned"
+        ms, launches = ms_l, launches_l
     value = forms[head]["value"]
 
     # ---- per-kernel leg: one pass over the pool with every kernel alone on the stream, each bracketed by events -
     # (in the timed region kernels of a step overlap, so an event pair there would also time its neighbours; kernel
     # timing also switches graph replay off, so each kernel is launched and timed on its own)
-    kform = BatchedForm() if head == "batched" else PlainForm()
+    kform = {"plain": PlainForm, "batched": BatchedForm, "learned": LearnedForm}[head]()
     kacc = [es_b200.new_accum() for _ in range(n_enc)]
     with torch.cuda.stream(stream):
         kf = 0
@@ -432,7 +455,7 @@ def main() -> None:
         h2d = sum(t.numel() * t.element_size() for pic in host_pool[0] for t in pic)
         windows = (w // 16) * (h // 16)
         d2h = 8 * (3 * n_enc + 3 * (n_enc + 1)) + 136 * n_enc + 2 * 6 * windows * n_enc + 48 * (1 + n_enc)
-        fr2 = BatchedForm() if head == "batched" else PlainForm()
+        fr2 = {"plain": PlainForm, "batched": BatchedForm, "learned": LearnedForm}[head]()
         acc2 = [es_b200.new_accum() for _ in range(n_enc)]
         copy_stream = torch.cuda.Stream()
         copied = [torch.cuda.Event() for _ in range(2)]
@@ -481,7 +504,7 @@ def main() -> None:
     peaks = read_peaks()
     if top:
         per_launch_ms = times[top][0] / times[top][1]
-        alg = algorithmic_bytes(top, wl, pics=(1 + n_enc) if head == "batched" else 1)
+        alg = algorithmic_bytes(top, wl, pics=(1 + n_enc) if head != "plain" else 1)
         achieved = alg / (per_launch_ms / 1000.0) / 1e9 if alg else None
         roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": read_traffic(top, f"{args.workload}:{head}"),

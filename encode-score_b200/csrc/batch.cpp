@@ -20,6 +20,9 @@
 
 using namespace es;
 
+const float *proposal_net_rounded(es_proposal_net *net, cudaStream_t s);
+const uint32_t *proposal_net_frags(const es_proposal_net *net);
+
 namespace {
 constexpr int kRing = 14, kEncRing = 7, kRadius = 6, kStats = 8, kPersist = 5, kBinArrays = 6;
 constexpr int kMaxBatchPictures = kMaxJobs / kScales;  // c-value jobs of one launch
@@ -74,6 +77,22 @@ struct es_batch {
     long queued[2] = {-1, -1};
     long next = 0, last_collected = -1;
     uint64_t graph_launches = 0;
+
+    // learned tile proposal (off while net is null)
+    es_proposal_net *net = nullptr;
+    es_proposal_options popt{};
+    const float *net_params = nullptr;
+    const uint32_t *net_frags = nullptr;
+    int total_tiles = 0, total_tiles0 = 0;   // c-value tiles of every scale / of scale 0, all pictures
+    DeviceBuffer<float> pred;                // per scale-0 tile
+    DeviceBuffer<uint8_t> kind;              // per tile
+    DeviceBuffer<unsigned> lists;            // list_a, then list_b (total_tiles each)
+    DeviceBuffer<unsigned> counters;         // count_a, count_b, next_a, next_b, n_audit[kMaxJobs], n_skip[kMaxJobs]
+    DeviceBuffer<unsigned long long> tile_mass, frame;
+    DeviceBuffer<int> run_flags;
+    DeviceBuffer<ProposalStats> stats;
+    PinnedBuffer<ProposalStats> h_stats[2];
+    PinnedBuffer<unsigned long long> h_frame[2];
 
     ~es_batch()
     {
@@ -185,6 +204,97 @@ uint16_t *luma_of(const es_batch &b, int picture, long f)
     return pic.encode < 0 ? S.src_plane(f) : S.enc_plane(pic.encode, f);
 }
 
+// The c-values of a step with the learned proposal: predictions of every scale-0 tile, the tile lists, the proposed
+// and audited tiles, the audit, then the skipped tiles of the pictures whose audit asks for the fallback. `run` lists
+// the pictures whose CAMBI runs; cb is the step's c-value job table (scales 0-4 of each, in that order).
+void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cudaStream_t s)
+{
+    const int np = (int)run.size();
+    unsigned *count_a = b.counters.ptr, *count_b = count_a + 1, *next_a = count_a + 2, *next_b = count_a + 3;
+    unsigned *n_audit = count_a + 4, *n_skip = n_audit + kMaxJobs;
+    cuda_check(cudaMemsetAsync(b.counters.ptr, 0, b.counters.bytes(), s), "clearing proposal counters");
+    PredBatch pb{};
+    int t0 = 0;
+    for (int r = 0; r < np; r++) {
+        const Picture &pic = *b.pictures[run[r]];
+        PredJob &j = pb.job[pb.njobs++];
+        j.word = pic.words[0].ptr;
+        j.w = pic.w;
+        j.h = pic.h;
+        j.tiles_x = (pic.w + kCvTX - 1) / kCvTX;
+        j.tiles_y = (pic.h + kCvTY - 1) / kCvTY;
+        j.first_tile = t0;
+        t0 += j.tiles_x * j.tiles_y;
+    }
+    pb.total_tiles = t0;
+    pb.band = cb.band;
+    pb.params = b.net_params;
+    pb.frags = b.net_frags;
+    pb.pred = b.pred.ptr;
+    cuda_check(launch_predict(pb, s), "tile predictions");
+    ProposeBatch qb{};
+    AuditBatch ab{};
+    for (int r = 0; r < np; r++) {
+        const Picture &pic = *b.pictures[run[r]];
+        AuditJob &aj = ab.job[ab.njobs++];
+        aj.window = pic.p.window;
+        for (int sc = 0; sc < kScales; sc++) {
+            const int ji = r * kScales + sc;
+            CvJob &cj = cb.job[ji];
+            cj.run_index = r;
+            ProposeJob &pj = qb.job[qb.njobs++];
+            pj.first_tile = cj.first_tile;
+            pj.tiles_x = cj.tiles_x;
+            pj.tiles_y = (cj.h + kCvTY - 1) / kCvTY;
+            pj.scale = sc;
+            pj.picture = run[r];
+            pj.pred_first = pb.job[r].first_tile;
+            pj.pred_tiles_x = pb.job[r].tiles_x;
+            pj.pred_tiles_y = pb.job[r].tiles_y;
+            if (sc < 2) {
+                aj.job[sc] = ji;
+                aj.first_tile[sc] = cj.first_tile;
+                aj.tiles[sc] = pj.tiles_x * pj.tiles_y;
+                aj.k[sc] = (double)topk_count((unsigned long long)pic.sw[sc] * pic.sh[sc], pic.p.topk);
+            }
+        }
+    }
+    qb.total_tiles = cb.total_tiles;
+    qb.pred = b.pred.ptr;
+    qb.threshold = b.popt.threshold;
+    qb.audit_permille[0] = (unsigned)b.popt.audit_permille[0];
+    qb.audit_permille[1] = (unsigned)b.popt.audit_permille[1];
+    qb.frame = b.frame.ptr;
+    qb.list_a = b.lists.ptr;
+    qb.list_b = b.lists.ptr + b.total_tiles;
+    qb.count_a = count_a;
+    qb.count_b = count_b;
+    qb.kind = b.kind.ptr;
+    qb.n_audit = n_audit;
+    qb.n_skip = n_skip;
+    cuda_check(launch_propose(qb, s), "tile proposal");
+    CvBatch ca = cb;
+    ca.tiles = qb.list_a;
+    ca.tile_count = count_a;
+    ca.tile_next = next_a;
+    ca.tile_mass = b.tile_mass.ptr;
+    cuda_check(launch_cvalues(ca, s), "proposed c-values");
+    ab.tile_mass = b.tile_mass.ptr;
+    ab.kind = b.kind.ptr;
+    ab.n_audit = n_audit;
+    ab.n_skip = n_skip;
+    ab.tolerance = b.popt.tolerance;
+    ab.run = b.run_flags.ptr;
+    ab.stats = b.stats.ptr;
+    cuda_check(launch_audit(ab, s), "tile audit");
+    CvBatch cf = cb;
+    cf.tiles = qb.list_b;
+    cf.tile_count = count_b;
+    cf.tile_next = next_b;
+    cf.run = b.run_flags.ptr;
+    cuda_check(launch_cvalues(cf, s), "fallback c-values");
+}
+
 // The CAMBI chain of step f for the pictures whose CAMBI runs, on stream s.
 void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
 {
@@ -261,7 +371,11 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
     }
     cb.lut = b.lut.ptr;
     cb.slots = b.slots.ptr;
-    cuda_check(launch_cvalues(cb, s), "batch c-values");
+    if (!b.net) {
+        cuda_check(launch_cvalues(cb, s), "batch c-values");
+    } else {
+        record_proposal(b, run, cb, s);
+    }
     static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
     for (int round = 0; round < 3; round++)
         cuda_check(launch_select_round(b.slots.ptr, nslots, shifts[round], widths[round], s), "batch top-k");
@@ -277,6 +391,8 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
     cuda_check(launch_score(sb, s), "batch score");
     cuda_check(cudaMemcpyAsync(b.h_scores[f % 2].ptr, b.scores.ptr, b.scores.bytes(), cudaMemcpyDeviceToHost, s),
                "reading scores");
+    if (b.net)
+        cuda_check(cudaMemcpyAsync(b.h_stats[f % 2].ptr, b.stats.ptr, b.stats.bytes(), cudaMemcpyDeviceToHost, s), "reading proposal stats");
 }
 
 // The texture chain of step f (PSNR / color, window figures, lasting texture, reduction) for every source.
@@ -508,6 +624,10 @@ int es_batch_queue(es_batch *b, long f, const es_frame_view *views, const int *c
         cuda_check(cudaStreamWaitEvent(b->main.s, b->start.e, 0), "event");
         cuda_check(cudaMemcpyAsync(b->views.ptr, b->h_views[at].ptr, sizeof(UnpackView) * P, cudaMemcpyHostToDevice, b->main.s),
                    "input addresses");
+        if (b->net) {
+            b->h_frame[at].ptr[0] = (unsigned long long)f;
+            cuda_check(cudaMemcpyAsync(b->frame.ptr, b->h_frame[at].ptr, 8, cudaMemcpyHostToDevice, b->main.s), "frame number");
+        }
         queue_step(*b, f, skip);
         cuda_check(cudaEventRecord(b->done[at].e, b->main.s), "event");
         cuda_check(cudaStreamWaitEvent(caller, b->done[at].e, 0), "event");
@@ -579,6 +699,87 @@ int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5])
         if (b->last_collected < 0) throw Error(ES_ERR_STATE, "es_batch_scale_pooled: no frame collected");
         const double *sc = b->h_scores[b->last_collected % 2].ptr + (size_t)picture * (1 + kScales);
         for (int s = 0; s < kScales; s++) pooled[s] = sc[1 + s];
+    });
+}
+
+int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_options *options)
+{
+    return guarded([&] {
+        require(b != nullptr, "es_batch_set_proposal: NULL batch");
+        if (b->queued[0] > b->last_collected || b->queued[1] > b->last_collected)
+            throw Error(ES_ERR_STATE, "es_batch_set_proposal: collect every queued step first");
+        es_proposal_options o{};
+        o.threshold = 0.05f;
+        o.audit_permille[0] = 50;
+        o.audit_permille[1] = 200;
+        o.tolerance = 0.025;
+        if (options) o = *options;
+        require(o.audit_permille[0] >= 0 && o.audit_permille[0] <= 1000 && o.audit_permille[1] >= 0 && o.audit_permille[1] <= 1000,
+                "es_batch_set_proposal: audit rates are per mille, 0 to 1000");
+        require(o.tolerance >= 0, "es_batch_set_proposal: tolerance must be >= 0");
+        cuda_check(cudaStreamSynchronize(b->main.s), "es_batch_set_proposal");
+        for (auto &g : b->graphs) cudaGraphExecDestroy(g.second);  // captured steps belong to the old setting
+        b->graphs.clear();
+        b->net = net;
+        b->popt = o;
+        if (!net) return;
+        b->net_params = proposal_net_rounded(net, b->main.s);
+        b->net_frags = proposal_net_frags(net);
+        if (!b->pred.ptr) {
+            int tiles = 0, tiles0 = 0;
+            for (auto &pp : b->pictures) {
+                const Picture &pic = *pp;
+                for (int sc = 0; sc < kScales; sc++) {
+                    const int t = ((pic.sw[sc] + kCvTX - 1) / kCvTX) * ((pic.sh[sc] + kCvTY - 1) / kCvTY);
+                    tiles += t;
+                    if (sc == 0) tiles0 += t;
+                }
+            }
+            b->total_tiles = tiles;
+            b->total_tiles0 = tiles0;
+            const int P = (int)b->pictures.size();
+            b->pred.reset(tiles0);
+            b->kind.reset(tiles);
+            b->lists.reset(2 * (size_t)tiles);
+            b->counters.reset(4 + 2 * kMaxJobs);
+            b->tile_mass.reset(tiles);
+            b->frame.reset(1);
+            b->run_flags.reset(P);
+            b->stats.reset(P);
+            for (int i = 0; i < 2; i++) {
+                b->h_stats[i].reset(P);
+                std::memset(b->h_stats[i].ptr, 0, sizeof(ProposalStats) * P);
+                b->h_frame[i].reset(1);
+            }
+        }
+        cuda_check(cudaStreamSynchronize(b->main.s), "es_batch_set_proposal");
+    });
+}
+
+int es_batch_proposal_stats(es_batch *b, int picture, es_proposal_stats *out)
+{
+    return guarded([&] {
+        require(b != nullptr && out != nullptr, "es_batch_proposal_stats: NULL argument");
+        require(picture >= 0 && picture < (int)b->pictures.size(), "es_batch_proposal_stats: picture out of range");
+        require(b->net != nullptr, "es_batch_proposal_stats: the proposal is off");
+        if (b->last_collected < 0) throw Error(ES_ERR_STATE, "es_batch_proposal_stats: no frame collected");
+        // the stats array is in the order of the pictures whose CAMBI ran
+        const int at = (int)(b->last_collected % 2);
+        int r = 0;
+        for (int i = 0; i < picture; i++) {
+            const Picture &pic = *b->pictures[i];
+            if (pic.encode >= 0 || !((b->skipped[at] >> pic.source) & 1u)) r++;
+        }
+        const Picture &me = *b->pictures[picture];
+        if (me.encode < 0 && ((b->skipped[at] >> me.source) & 1u)) throw Error(ES_ERR_STATE, "es_batch_proposal_stats: that CAMBI was skipped");
+        const ProposalStats &st = b->h_stats[at].ptr[r];
+        out->estimate = st.estimate;
+        out->fallback = st.fallback;
+        for (int k = 0; k < 2; k++) {
+            out->run[k] = st.run[k];
+            out->audited[k] = st.audited[k];
+            out->skipped[k] = st.skipped[k];
+        }
     });
 }
 

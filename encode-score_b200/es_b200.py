@@ -30,7 +30,7 @@ SYMBOLS = (
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
     "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
-    "es_batch_graph_launches", "es_batch_destroy",
+    "es_batch_graph_launches", "es_batch_destroy", "es_batch_set_proposal", "es_batch_proposal_stats",
 )
 
 
@@ -88,6 +88,15 @@ _lib = None
 
 class BatchSource(ctypes.Structure):
     _fields_ = [("w", ctypes.c_int), ("h", ctypes.c_int), ("pd", ctypes.c_int), ("n_encodes", ctypes.c_int)]
+
+
+class ProposalOptions(ctypes.Structure):
+    _fields_ = [("threshold", ctypes.c_float), ("audit_permille", ctypes.c_int * 2), ("tolerance", ctypes.c_double)]
+
+
+class ProposalStats(ctypes.Structure):
+    _fields_ = [("estimate", ctypes.c_float), ("fallback", ctypes.c_int), ("run", ctypes.c_uint32 * 2), ("audited", ctypes.c_uint32 * 2),
+                ("skipped", ctypes.c_uint32 * 2)]
 
 
 class BatchOptions(ctypes.Structure):
@@ -156,6 +165,8 @@ def lib() -> ctypes.CDLL:
         L.es_batch_graph_launches.argtypes = [P]
         L.es_batch_graph_launches.restype = U64
         L.es_batch_destroy.argtypes = [P]
+        L.es_batch_set_proposal.argtypes = [P, P, ctypes.POINTER(ProposalOptions)]
+        L.es_batch_proposal_stats.argtypes = [P, I, ctypes.POINTER(ProposalStats)]
         _lib = L
     return _lib
 
@@ -431,6 +442,17 @@ class Batch:
         out = (ctypes.c_double * SCALES)()
         check(lib().es_batch_scale_pooled(self.handle, picture, out))
         return list(out)
+
+    def set_proposal(self, net, threshold: float = 0.05, audit=(50, 200), tolerance: float = 0.025) -> None:
+        """Switches the learned tile proposal on (net: ProposalNet) or off (net None)."""
+        opt = ProposalOptions(threshold, (ctypes.c_int * 2)(*audit), tolerance)
+        check(lib().es_batch_set_proposal(self.handle, net.handle if net is not None else None, ctypes.byref(opt)))
+
+    def proposal_stats(self, picture: int) -> dict:
+        st = ProposalStats()
+        check(lib().es_batch_proposal_stats(self.handle, picture, ctypes.byref(st)))
+        return {"estimate": st.estimate, "fallback": st.fallback, "run": list(st.run), "audited": list(st.audited),
+                "skipped": list(st.skipped)}
 
     def graph_launches(self) -> int:
         return int(lib().es_batch_graph_launches(self.handle))

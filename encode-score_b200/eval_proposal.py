@@ -1,0 +1,135 @@
+#!/usr/bin/env python3
+"""Evaluates the learned tile proposal: fresh seeded 3840x2160 10-bit frame pairs (es_synth_gpu, seeds disjoint from
+training) are scored by the exact batched step and by the batched step with the proposal, on the same inputs.
+
+Reports per picture |delta CAMBI| (proposal - exact) as a distribution, the share of pictures within 0.05, the
+fallback rate, the share of non-empty tiles of scales 0-1 that ran, and each form's frame-pairs/s (CUDA events
+around queue + collect of the timed steps; frame generation untimed). With --untrained, the same run with a
+He-initialised network at the same threshold (the ablation: what the training buys).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+W, H = 3840, 2160
+
+
+def load_net(es_b200, path=None):
+    import numpy as np
+
+    path = path or os.path.join(HERE, "proposal_net.npy")
+    params = np.load(path)
+    with open(os.path.splitext(path)[0] + ".json") as f:
+        meta = json.load(f)
+    return es_b200.ProposalNet(params), meta
+
+
+def planar(torch, es_b200, y):
+    """A planar 16-bit frame view of luma y (int16 codes) with chroma = luma / 2 averaged 2 x 2."""
+    c = (y.float().view(H // 2, 2, W // 2, 2).mean(dim=(1, 3)) / 2).round().to(torch.int16).contiguous()
+    u, v = c, c.clone()
+    view = es_b200.FrameView(y.data_ptr(), u.data_ptr(), v.data_ptr(), W * 2, W, 0, 2, 0, 10)
+    return view, (y, u, v)
+
+
+def run(torch, es_b200, module, frames: int, seed: int, net, threshold: float, audit=(50, 200), tolerance: float = 0.025):
+    """Scores `frames` frame pairs with the exact and the proposal form; returns per-picture rows and timings."""
+    import es_synth_gpu
+
+    exact = es_b200.Batch(module, [(W, H, 10, 1)])
+    prop = es_b200.Batch(module, [(W, H, 10, 1)])
+    prop.set_proposal(net, threshold=threshold, audit=audit, tolerance=tolerance)
+    stream = torch.cuda.current_stream().cuda_stream
+    rows = []
+    t_exact = t_prop = 0.0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for f in range(frames):
+        src, enc, prm = es_synth_gpu.frame_pair(torch, f, seed=seed)
+        vs, keep_s = planar(torch, es_b200, src.contiguous())
+        ve, keep_e = planar(torch, es_b200, enc.contiguous())
+        torch.cuda.synchronize()
+        ev[0].record()
+        exact.queue(f, [vs, ve], stream)
+        re = exact.collect(f)[0]
+        ev[1].record()
+        prop.queue(f, [vs, ve], stream)
+        rp = prop.collect(f)[0]
+        ev[2].record()
+        torch.cuda.synchronize()
+        if f >= 15:  # both forms replay graphs from frame 14 on
+            t_exact += ev[0].elapsed_time(ev[1])
+            t_prop += ev[1].elapsed_time(ev[2])
+        for pic, (a, b) in enumerate(((re.cambi_source, rp.cambi_source), (re.cambi, rp.cambi))):
+            st = prop.proposal_stats(pic)
+            rows.append({"frame": f, "picture": pic, "exact": a, "proposal": b, "delta": b - a, "fallback": st["fallback"],
+                         "estimate": st["estimate"], "run": st["run"], "audited": st["audited"], "skipped": st["skipped"]})
+    exact.close()
+    prop.close()
+    timed = max(frames - 15, 1)
+    return rows, {"exact_ms_per_pair": t_exact / timed, "proposal_ms_per_pair": t_prop / timed}
+
+
+def summarize(rows, timing):
+    import numpy as np
+
+    d = np.abs(np.array([r["delta"] for r in rows]))
+    ran = sum(r["run"][0] + r["run"][1] + r["audited"][0] + r["audited"][1] for r in rows if not r["fallback"])
+    ran += sum(r["run"][0] + r["run"][1] + r["audited"][0] + r["audited"][1] + r["skipped"][0] + r["skipped"][1]
+               for r in rows if r["fallback"])
+    total = sum(r["run"][0] + r["run"][1] + r["audited"][0] + r["audited"][1] + r["skipped"][0] + r["skipped"][1] for r in rows)
+    return {
+        "pictures": len(rows),
+        "abs_delta_cambi": {"max": float(d.max()), "p50": float(np.percentile(d, 50)), "p99": float(np.percentile(d, 99)),
+                            "mean": float(d.mean())},
+        "share_within_0.05": float(np.mean(d <= 0.05)),
+        "fallback_rate": float(np.mean([r["fallback"] for r in rows])),
+        "tiles_run_share": ran / max(total, 1),
+        "exact_frame_pairs_per_s": 1000.0 / timing["exact_ms_per_pair"] if timing["exact_ms_per_pair"] else None,
+        "proposal_frame_pairs_per_s": 1000.0 / timing["proposal_ms_per_pair"] if timing["proposal_ms_per_pair"] else None,
+        **timing,
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--frames", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=90_000_000)
+    ap.add_argument("--net", default=None)
+    ap.add_argument("--untrained", action="store_true", help="also run a He-initialised network at the same threshold")
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+
+    import torch
+
+    import es_b200
+
+    torch.cuda.set_device(0)
+    module = es_b200.Module()
+    net, meta = load_net(es_b200, args.net)
+    t0 = time.time()
+    rows, timing = run(torch, es_b200, module, args.frames, args.seed, net, meta["threshold"])
+    out = {"threshold": meta["threshold"], "trained": summarize(rows, timing), "seconds": time.time() - t0}
+    if args.untrained:
+        raw = es_b200.ProposalNet(seed=12345)
+        rows_u, timing_u = run(torch, es_b200, module, args.frames, args.seed, raw, meta["threshold"])
+        out["untrained"] = summarize(rows_u, timing_u)
+        raw.close()
+    net.close()
+    module.close()
+    text = json.dumps(out, indent=1)
+    print(text)
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(text)
+
+
+if __name__ == "__main__":
+    main()

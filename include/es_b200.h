@@ -264,6 +264,28 @@ int es_batch_collect(es_batch *b, long f, const double *cached_source_cambi, es_
 int es_batch_read_windows(es_batch *b, int source, int encode, float *stats, float *persist);
 /* Introspection for tests: the pooled value of each scale of picture `picture` in the last collected step. */
 int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5]);
+/* The learned tile proposal (no counterpart in the reference): with a network, later steps compute c-values of
+ * scales 0 and 1 only on tiles whose prediction (or, at scale 1, the prediction of a scale-0 tile it covers) reaches
+ * `threshold`, plus a random audit sample (per mille of the other tiles, per scale); scales 2-4 always run. From the
+ * audited tiles' exact c-value sums the device estimates how much the skipped tiles would add to each picture's score;
+ * above `tolerance` the skipped tiles run too (the fallback), so the score is then exact. Scale-0 tiles with no pixel
+ * that needs a c-value are skipped in every mode (they add nothing). net NULL switches the proposal off. The network
+ * must stay alive while the batch uses it; after training it further, call this again. Every queued step must have
+ * been collected. options NULL = {threshold 0.05, audit 50 and 200 per mille, tolerance 0.025}. */
+typedef struct {
+    float threshold;       /* in the network's label space, log1p(mean c-value of the tile) */
+    int audit_permille[2]; /* scales 0 and 1 */
+    double tolerance;      /* estimated change of the score above which the fallback runs */
+} es_proposal_options;
+int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_options *options);
+typedef struct {
+    float estimate;        /* the audit's estimate of the skipped tiles' share of the score */
+    int fallback;          /* 1: the skipped tiles ran too */
+    uint32_t run[2];       /* proposed tiles of scales 0 and 1 */
+    uint32_t audited[2], skipped[2];
+} es_proposal_stats;
+/* The proposal's figures for picture `picture` in the last collected step. */
+int es_batch_proposal_stats(es_batch *b, int picture, es_proposal_stats *out);
 /* Diagnostics: how many steps were replayed from CUDA graphs. */
 uint64_t es_batch_graph_launches(const es_batch *b);
 void es_batch_destroy(es_batch *b);
