@@ -30,6 +30,7 @@ SYMBOLS = (
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
     "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
+    "es_windows_create", "es_windows_compute", "es_windows_figures", "es_windows_destroy",
     "es_batch_graph_launches", "es_batch_destroy", "es_batch_set_proposal", "es_batch_proposal_stats",
 )
 
@@ -156,6 +157,10 @@ def lib() -> ctypes.CDLL:
         L.es_proposal_features.argtypes = [U64, I, I, P, I, I, I, P, P]
         L.es_proposal_predict.argtypes = [P, U64, I, I, P, P]
         L.es_proposal_net_destroy.argtypes = [P]
+        L.es_windows_create.argtypes = [I, I, ctypes.POINTER(P)]
+        L.es_windows_compute.argtypes = [P, U64, U64, I, P]
+        L.es_windows_figures.argtypes = [P, I, I, P, P]
+        L.es_windows_destroy.argtypes = [P]
         L.es_batch_create.argtypes = [P, I, ctypes.POINTER(BatchSource), ctypes.POINTER(BatchOptions), ctypes.POINTER(P)]
         L.es_batch_queue.argtypes = [P, ctypes.c_long, ctypes.POINTER(FrameView), ctypes.POINTER(I), ctypes.POINTER(I), P]
         L.es_batch_collect.argtypes = [P, ctypes.c_long, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.POINTER(Accum)),
@@ -283,6 +288,28 @@ class Cambi:
     def close(self) -> None:
         if self.handle:
             lib().es_cambi_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+class Windows:
+    """Texture window energies in three arithmetics (es_windows_*): mode 0 integer, 1 compensated FP32, 2 FP32."""
+
+    INTEGER, COMPENSATED, FP32 = 0, 1, 2
+
+    def __init__(self, w: int, h: int):
+        self.handle = ctypes.c_void_p()
+        self.w, self.h = w, h
+        check(lib().es_windows_create(w, h, ctypes.byref(self.handle)))
+
+    def compute(self, src: int, enc: int, up: int, stream: int = 0) -> None:
+        check(lib().es_windows_compute(self.handle, src, enc, up, ctypes.c_void_p(stream)))
+
+    def figures(self, window: int, mode: int, out: int, stream: int = 0) -> None:
+        check(lib().es_windows_figures(self.handle, window, mode, ctypes.c_void_p(out), ctypes.c_void_p(stream)))
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_windows_destroy(self.handle)
             self.handle = ctypes.c_void_p()
 
 

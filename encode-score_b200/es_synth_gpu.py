@@ -80,3 +80,30 @@ def frame_pair(torch, index: int, w: int = 3840, h: int = 2160, seed: int = 5000
     enc = torch.clamp(enc, 64, 940)
     params = {"lo": lo, "hi": hi, "grain": sigma, "blur": blur, "degrain": degrain, "step": step, "left_half": left}
     return src.to(torch.int16), enc.to(torch.int16), params
+
+
+def c4_pair(torch, index: int, w: int = 3840, h: int = 2160, seed: int = 4000):
+    """The precision workload: a bright 10-bit gradient (codes 600-940, 3 seeded linear or radial gradients) with heavy
+    Gaussian grain (sigma 20 codes), clipped to 0-1023; the encode blurs it (sigma 1.0). int16 CUDA tensors."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed + index)
+
+    def u(lo=0.0, hi=1.0):
+        return lo + (hi - lo) * float(torch.rand(1, generator=g, device="cuda").item())
+
+    yy = torch.linspace(0, 1, h, device="cuda").view(h, 1).expand(h, w)
+    xx = torch.linspace(0, 1, w, device="cuda").view(1, w).expand(h, w)
+    field = torch.zeros(h, w, device="cuda")
+    for _ in range(3):
+        if u() < 0.5:
+            a = u(0, 2 * math.pi)
+            field += math.cos(a) * xx + math.sin(a) * yy
+        else:
+            cx, cy = u(), u()
+            field += torch.sqrt((xx - cx) ** 2 + (yy - cy) ** 2)
+    field -= field.min()
+    field /= field.max().clamp_min(1e-6)
+    noise = torch.randn(h, w, generator=g, device="cuda")
+    src = torch.clamp(torch.round(600 + 340 * field + 20 * noise), 0, 1023)
+    enc = torch.clamp(torch.round(_gauss_blur(torch, src, 1.0)), 0, 1023)
+    return src.to(torch.int16), enc.to(torch.int16)

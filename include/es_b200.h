@@ -205,6 +205,22 @@ int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist
 void es_frame_destroy(es_frame *fr);
 
 /* ---------------------------------------------------------------------------------------------------------------
+ * Texture window energies on larger windows, in three arithmetics (the precision study; no counterpart in the
+ * reference, which sums FP32 box means over fixed 16 x 16 windows, src/kernels.cu:331-428). The 3 x 3 and 9 x 9 box
+ * sums (edge pixels repeated) come from summed-area tables of each luma plane kept as int64, as FP32 with two-sum
+ * compensation, and as plain FP32; pixel terms and their per-16 x 16-block sums follow in the same arithmetic (exact
+ * int64 numerators; Neumaier-compensated FP32; plain FP32). A window of side 16 k sums k x k blocks and gives the
+ * 8 figures of src/kernels.cu:340-341 (windows x 8 doubles, window (x, y) at index y * (w / window) + x).
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct es_windows es_windows;
+int es_windows_create(int w, int h, es_windows **out);
+/* src / enc: device luma planes (w x h uint16 at the pipeline depth); up = 10 - depth (0 or 2). */
+int es_windows_compute(es_windows *p, uint64_t src, uint64_t enc, int up, void *stream);
+/* mode 0: integer tables (exact, rounded once to double); 1: compensated FP32; 2: plain FP32. out: device doubles. */
+int es_windows_figures(es_windows *p, int window, int mode, double *out, void *stream);
+void es_windows_destroy(es_windows *p);
+
+/* ---------------------------------------------------------------------------------------------------------------
  * Learned tile proposal: no counterpart in the reference, which computes the c-values of every tile. A network of
  * four valid 3 x 3 convolutions (2 -> 16 -> 16 -> 16 -> 1, ReLU after the first three, bfloat16 weights, FP32
  * accumulation) reads 4 x 4 block features of CAMBI's scale-0 words -- the mean value as (mean - 512) / 256 and the
