@@ -51,6 +51,7 @@ struct Source {
 struct Picture {
     int source = 0, encode = -1;  // encode -1: the source's own picture
     int w = 0, h = 0, depth = 10;
+    int tile_rows[kScales] = {64, 64, 64, 64, 64};  // c-value tile rows per scale
     es_cambi_params p{};
     int sw[kScales], sh[kScales];
     DeviceBuffer<uint16_t> words[kScales];
@@ -245,7 +246,7 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
             ProposeJob &pj = qb.job[qb.njobs++];
             pj.first_tile = cj.first_tile;
             pj.tiles_x = cj.tiles_x;
-            pj.tiles_y = (cj.h + kCvTY - 1) / kCvTY;
+            pj.tiles_y = (cj.h + cj.tile_rows - 1) / cj.tile_rows;
             pj.scale = sc;
             pj.picture = run[r];
             pj.pred_first = pb.job[r].first_tile;
@@ -356,7 +357,8 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
             j.first_tile = tiles;
             j.slot = i * kScales + sc;
             j.plane = nullptr;
-            tiles += j.tiles_x * ((j.h + kCvTY - 1) / kCvTY);
+            j.tile_rows = (b.net && sc < 2) ? 64 : pic.tile_rows[sc];  // the proposal maps 64-row tiles of scales 0, 1
+            tiles += j.tiles_x * ((j.h + j.tile_rows - 1) / j.tile_rows);
         }
     }
     cb.total_tiles = tiles;
@@ -586,6 +588,11 @@ int es_batch_create(const es_module *m, int n_sources, const es_batch_source *so
                 pic->h = sources[i].h;
                 pic->depth = sources[i].pd;
                 pic->p = p;
+                for (int sc = 0; sc < kScales; sc++) {
+                    const int r = sources[i].cv_tile_rows[sc];
+                    require(r == 0 || r == 16 || r == 32 || r == 64, "es_batch_create: c-value tile rows must be 0, 16, 32 or 64");
+                    pic->tile_rows[sc] = r ? r : 64;
+                }
                 b->pictures.push_back(std::move(pic));
             }
             b->sources.push_back(std::move(S));
@@ -730,7 +737,8 @@ int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_o
             for (auto &pp : b->pictures) {
                 const Picture &pic = *pp;
                 for (int sc = 0; sc < kScales; sc++) {
-                    const int t = ((pic.sw[sc] + kCvTX - 1) / kCvTX) * ((pic.sh[sc] + kCvTY - 1) / kCvTY);
+                    const int tr = sc < 2 ? 64 : pic.tile_rows[sc];
+                    const int t = ((pic.sw[sc] + kCvTX - 1) / kCvTX) * ((pic.sh[sc] + tr - 1) / tr);
                     tiles += t;
                     if (sc == 0) tiles0 += t;
                 }

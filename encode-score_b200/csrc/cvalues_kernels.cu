@@ -70,7 +70,7 @@ __device__ __forceinline__ void pair_match(uint32_t quad, uint32_t ta4, uint32_t
     ma = hit ^ mb;
 }
 
-__global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_constant__ CvBatch b)
+__global__ void __launch_bounds__(kCvThreads, 3) cvalues_kernel(const __grid_constant__ CvBatch b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t occ[32], srv[32], rel[32], needbits[32];
@@ -101,9 +101,10 @@ __global__ void __launch_bounds__(kCvThreads) cvalues_kernel(const __grid_consta
     const CvJob &J = b.job[j];
     if (b.run && !b.run[J.run_index]) return;
     const int tile = gt - J.first_tile;
-    const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * kCvTY;
+    const int th = J.tile_rows ? J.tile_rows : kCvTY;  // shorter tiles use the same buffers, like a picture's last row
+    const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * th;
     const int w = J.w, h = J.h, P = J.pad;
-    const int rows = min(kCvTY, h - y0), cols = min(kCvTX, w - x0);
+    const int rows = min(th, h - y0), cols = min(kCvTX, w - x0);
     const bool vec = (w & 7) == 0 && (((uintptr_t)J.word) & 15) == 0;  // rows of 16-byte vectors
 
     // 1. does any pixel of the tile need a c-value?

@@ -99,6 +99,7 @@ struct CvJob {
     int slot;       // index into the CvSlot array
     float *plane;   // optional: every computed c-value at its pixel
     int run_index;  // the entry of CvBatch::run that gates this job (with a run table)
+    int tile_rows;  // rows of this job's tiles: 64 (0 means 64), 32 or 16; tiles are numbered row by row
 };
 struct CvBatch {
     CvJob job[kMaxJobs];

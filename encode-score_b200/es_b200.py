@@ -88,7 +88,8 @@ _lib = None
 
 
 class BatchSource(ctypes.Structure):
-    _fields_ = [("w", ctypes.c_int), ("h", ctypes.c_int), ("pd", ctypes.c_int), ("n_encodes", ctypes.c_int)]
+    _fields_ = [("w", ctypes.c_int), ("h", ctypes.c_int), ("pd", ctypes.c_int), ("n_encodes", ctypes.c_int),
+                ("cv_tile_rows", ctypes.c_int * 5)]
 
 
 class ProposalOptions(ctypes.Structure):
@@ -427,16 +428,52 @@ class Frame:
             self.handle = ctypes.c_void_p()
 
 
+def device_step(torch, step) -> tuple:
+    """A synthetic frame step (es_synth.Step) copied to the device as planar 16-bit frames: (tensors to keep alive,
+    [source view, encode views ...])."""
+    import numpy as np
+    keep, views = [], []
+    for pic in [step.source] + list(step.encodes):
+        t = [torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).cuda() for a in (pic.y, pic.u, pic.v)]
+        keep.append(t)
+        views.append(FrameView(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), t[0].stride(0) * 2, t[1].stride(0) * 2, 0, 2, 0,
+                               pic.depth))
+    return keep, views
+
+
+AUTOTUNE_PATH = os.path.join(HERE, "autotune.json")
+
+
+def autotune_table(path: str = AUTOTUNE_PATH) -> dict:
+    """{(w, h): c-value tile rows per scale} from the autotuner's table (empty when there is none)."""
+    import json
+    try:
+        with open(path) as f:
+            t = json.load(f)
+    except (OSError, ValueError):
+        return {}
+    out = {}
+    for key, entry in t.get("classes", {}).items():
+        w, h = (int(v) for v in key.split("x"))
+        out[(w, h)] = list(entry["cv_tile_rows"])
+    return out
+
+
 class Batch:
     """Batched frame steps of several sources (es_batch_*): one launch per stage for all pictures, CUDA graphs from
-    frame 14 on. ``sources`` is a list of (w, h, pd, n_encodes); pictures and encodes are numbered source by source."""
+    frame 14 on. ``sources`` is a list of (w, h, pd, n_encodes); pictures and encodes are numbered source by source.
+    ``tuning``: None for the autotuned c-value tile rows of autotune.json (by picture size; 64 where absent), False
+    for 64 everywhere, or a dict {(w, h): [rows per scale]}."""
 
-    def __init__(self, module: Module, sources: list, use_graphs: bool = True):
+    def __init__(self, module: Module, sources: list, use_graphs: bool = True, tuning=None):
         self.handle = ctypes.c_void_p()
         self.sources = [tuple(s) for s in sources]
         self.n_pictures = sum(1 + s[3] for s in self.sources)
         self.n_encodes = sum(s[3] for s in self.sources)
-        arr = (BatchSource * len(self.sources))(*[BatchSource(*s) for s in self.sources])
+        table = autotune_table() if tuning is None else (tuning or {})
+        self.tile_rows = [list(table.get((s[0], s[1]), [64] * 5)) for s in self.sources]
+        arr = (BatchSource * len(self.sources))(*[BatchSource(*s, (ctypes.c_int * 5)(*r))
+                                                  for s, r in zip(self.sources, self.tile_rows)])
         opt = BatchOptions(int(use_graphs))
         check(lib().es_batch_create(module.handle, len(self.sources), arr, ctypes.byref(opt), ctypes.byref(self.handle)))
 

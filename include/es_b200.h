@@ -259,6 +259,8 @@ typedef struct {
     int w, h;      /* common picture area of the source and its encodes (even) */
     int pd;        /* pipeline depth, 8 or 10 */
     int n_encodes; /* 1 to 16 */
+    int cv_tile_rows[5]; /* rows of the c-value tiles per scale: 64, 32 or 16 (0 = 64); an autotuner's choice. With
+                          * the learned proposal on, scales 0 and 1 use 64. */
 } es_batch_source;
 typedef struct {
     int use_graphs; /* replay steps from CUDA graphs once the rings are full (frame 14 on) */
