@@ -256,13 +256,117 @@ def reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_c3(args, rank: int, world: int, local: int) -> None:
+    """The uneven batch: 16 source / encode pairs per frame step (6 x 1280x720 8-bit, 6 x 1920x800 10-bit cropped from
+    1920x1080 frames with black bars, 4 x 3840x1600 10-bit; es_synth.c3_step), scored as 16 plain es_frame instances
+    and as one es_batch (one launch per stage for all 32 pictures, graphs from frame 14, autotuned tiles). Device-
+    resident inputs, pool of 2 distinct steps (1.1 GB, larger than L2); time on the device with CUDA events."""
+    import numpy as np
+    import torch
+
+    import es_b200
+    import es_synth
+
+    torch.cuda.set_device(local)
+    srcs = es_synth.C3_SOURCES
+    pool = []
+    for f in range(2):
+        step = []
+        for i, (w, h, d) in enumerate(srcs):
+            st = es_synth.c3_step(f, i, w, h, d)
+            fw, fh = es_synth.C3_BARS.get((w, h), (w, h))
+            y0 = ((fh - h) // 2) & ~1
+            pics = []
+            for pic in [st.source] + st.encodes:
+                Y = np.zeros((fh, fw), np.uint16)
+                Y[y0:y0 + h] = pic.y
+                U = np.full((fh // 2, fw // 2), 0, np.uint16)
+                V = U.copy()
+                U[y0 // 2:y0 // 2 + h // 2], V[y0 // 2:y0 // 2 + h // 2] = pic.u, pic.v
+                t = [torch.from_numpy(a.view(np.int16)).cuda() for a in (Y, U, V)]
+                pics.append((t, es_b200.FrameView(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), fw * 2, fw, 0, 2, 0, d), y0))
+            step.append(pics)
+        pool.append(step)
+    torch.cuda.synchronize()
+    module = es_b200.Module()
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    pairs = len(srcs) * args.steps
+
+    def timed(queue, collect):
+        f = 0
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 28)):
+                queue(f)
+                collect(f)
+                f += 1
+            torch.cuda.synchronize()
+            l0 = es_b200.launch_count()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for k in range(args.steps):
+                queue(f)
+                if k:
+                    collect(f - 1)
+                f += 1
+            collect(f - 1)
+            b.record(stream)
+            b.synchronize()
+        return a.elapsed_time(b), es_b200.launch_count() - l0
+
+    frames = [es_b200.Frame(module, w, h, d, 1) for (w, h, d) in srcs]
+    accs = [[es_b200.new_accum()] for _ in srcs]
+
+    def q_plain(f):
+        step = pool[f % 2]
+        for i, fr in enumerate(frames):
+            (ts, vs, ys), (te, ve, ye) = step[i]
+            fr.queue(f, vs, [ve], sh, sx=0, sy=ys, ex=[0], ey=[ye])
+
+    def c_plain(f):
+        for i, fr in enumerate(frames):
+            fr.collect(f, accs[i], accs[i])
+
+    ms_plain, l_plain = timed(q_plain, c_plain)
+    for fr in frames:
+        fr.close()
+    batch = es_b200.Batch(module, [(w, h, d, 1) for (w, h, d) in srcs])
+    acc = [es_b200.new_accum() for _ in srcs]
+
+    def q_batch(f):
+        step = pool[f % 2]
+        views = [p[1] for pics in step for p in pics]
+        crops = [(0, p[2]) for pics in step for p in pics]
+        batch.queue(f, views, sh, crops=crops)
+
+    def c_batch(f):
+        batch.collect(f, acc, acc)
+
+    ms_b, l_b = timed(q_batch, c_batch)
+    graphs = batch.graph_launches()
+    batch.close()
+    module.close()
+    if rank == 0:
+        line = {"metric": "frame-pairs/s, 16 uneven source/encode pairs per frame step", "value": pairs / (ms_b / 1000.0),
+                "unit": "frame-pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/int64",
+                "data": "synthetic (seeded es_synth c3 frames)",
+                "config": {"workload": "6 x 1280x720 8-bit, 6 x 1920x800 10-bit (cropped from 1920x1080 with bars), 4 x 3840x1600 10-bit",
+                           "frame_pairs_per_step": len(srcs), "l2": "2 distinct steps of 1.1 GB input cycled",
+                           "form": "batched (es_batch, graphs, autotuned c-value tiles)"},
+                "forms": {"plain": {"value": pairs / (ms_plain / 1000.0), "ms_per_step": ms_plain / args.steps, "gpu_launches": int(l_plain)},
+                          "batched": {"value": pairs / (ms_b / 1000.0), "ms_per_step": ms_b / args.steps, "gpu_launches": int(l_b),
+                                      "graph_steps": int(graphs)}}}
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3"], default="c2")
     ap.add_argument("--pool", type=int, default=6, help="distinct frame steps cycled through")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -273,6 +377,9 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.workload == "c3":
+        run_c3(args, rank, world, local)
         return
 
     import numpy as np
@@ -362,12 +469,13 @@ def main() -> None:
 
     def time_form(form, f0: int) -> tuple[float, int, dict | None, int]:
         """Warm-up, then args.steps timed steps of `form` over the device pool; returns (ms, launches, clocks, next f).
-        The warm-up covers the first 14 frames, so the batched form replays graphs in the timed region."""
+        The warm-up runs frames 0-27, so the batched forms have captured the graph of each of the 14 ring phases and only
+        replay graphs in the timed region."""
         acc = [es_b200.new_accum() for _ in range(n_enc)]
         f = f0
         with torch.cuda.stream(stream):
             sh = stream.cuda_stream
-            for _ in range(max(args.warmup, 15)):
+            for _ in range(max(args.warmup, 28)):
                 p = dev_pool[f % len(dev_pool)]
                 form.queue(f, [x[1] for x in p], sh)
                 form.collect(f, acc)
@@ -477,7 +585,7 @@ def main() -> None:
                 fr2.collect(g - 1, acc2)
 
         with torch.cuda.stream(stream):
-            warm = max(args.warmup, 15)
+            warm = max(args.warmup, 28)
             for g in range(warm):
                 e2e_step(g, g > 0)
             fr2.collect(warm - 1, acc2)

@@ -259,8 +259,10 @@ constexpr int kNetParams = 5089;
 __host__ __device__ constexpr int net_w(int l) { return l == 0 ? 0 : l == 1 ? 304 : l == 2 ? 2624 : 4944; }   // weights of layer l
 __host__ __device__ constexpr int net_b(int l) { return l == 0 ? 288 : l == 1 ? 2608 : l == 2 ? 4928 : 5088; }  // its biases
 constexpr int kFeatTile = 24;  // feature pixels per side around one tile (16 + 2 x 4 halo)
-// mma B fragments of the two 16 -> 16 layers: [layer 1, 2][tap][n tile][register][lane]
-constexpr int kNetFrags = 2 * 9 * 2 * 2 * 32;
+// mma B fragments: layers 1 and 2 (16 -> 16) [layer][tap][n tile][register][lane], then layer 3 (16 -> 1, its one
+// output channel in column 0 of an 8-wide n tile) [tap][register][lane]
+constexpr int kNetFrags12 = 2 * 9 * 2 * 2 * 32;
+constexpr int kNetFrags = kNetFrags12 + 9 * 2 * 32;
 
 struct PredJob {
     const uint16_t *word;  // scale-0 words of a picture

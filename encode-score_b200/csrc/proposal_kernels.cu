@@ -28,19 +28,13 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x = lo, in the low half
     return *(const uint32_t *)&v;
 }
-__device__ __forceinline__ float2 unpack_bf16(uint32_t u)
-{
-    __nv_bfloat162 v;
-    *(uint32_t *)&v = u;
-    return __bfloat1622float2(v);
-}
 
 // ---------------------------------------------------------------------------------------------------------------
 // Features of the 4 x 4 block of scale-0 pixels from (X, Y); with a band, `need` tells whether a pixel of the block
 // needs a c-value.
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ void block_features(const uint16_t *word, int w, int h, int X, int Y, const Band *bd, float &f0,
-                                               float &f1, bool &need)
+__device__ __forceinline__ void block_features(const uint16_t *word, int w, int h, int X, int Y, const Band *bd,
+                                               const uint32_t *needbits, float &f0, float &f1, bool &need)
 {
     unsigned sum = 0, n = 0, m = 0;
     bool nd = false;
@@ -69,9 +63,9 @@ __device__ __forceinline__ void block_features(const uint16_t *word, int w, int 
         for (int k = 0; k < cnt; k++) {
             sum += q[k] & 0x7FFFu;
             m += (q[k] >> 15) & 1u;
-            if (bd) {
+            if (bd) {  // needbits: bit c set when code c needs a c-value
                 const uint16_t c = code_of(q[k], *bd);
-                nd |= c != kNone && needs_cvalue(c, *bd);
+                nd |= c != kNone && ((needbits[c >> 5] >> (c & 31)) & 1u);
             }
         }
         n += cnt;
@@ -89,7 +83,7 @@ __global__ void __launch_bounds__(256) net_features_kernel(const uint16_t *word,
         const int c = (int)(i / per), r = (int)(i - (size_t)c * per), v = r / fw, u = r - v * fw;
         float f0, f1;
         bool need;
-        block_features(word, w, h, xy[2 * c] + 4 * u, xy[2 * c + 1] + 4 * v, nullptr, f0, f1, need);
+        block_features(word, w, h, xy[2 * c] + 4 * u, xy[2 * c + 1] + 4 * v, nullptr, nullptr, f0, f1, need);
         out[(size_t)c * 2 * per + r] = f0;
         out[(size_t)c * 2 * per + per + r] = f1;
     }
@@ -252,7 +246,8 @@ struct PredSmem {
     float b12[2][16];
     __align__(16) uint32_t a1[22 * 22 * 8];       // layer-0 output, [pixel][16 channels] bfloat16; later layer 2's
     __align__(16) uint32_t a2[20 * 20 * 8];       // layer-1 output
-    uint32_t frags[kNetFrags];                    // B fragments of layers 1 and 2, [layer][tap][n tile][reg][lane]
+    uint32_t frags[kNetFrags];                    // B fragments of layers 1, 2 and 3
+    uint32_t needbits[32];                        // codes that need a c-value
     float part[kPT / 32];
 };
 
@@ -308,6 +303,32 @@ __device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *
     }
 }
 
+// Layer 3 (16 -> 1) on the 16 x 16 output from the 18 x 18 plane `in`: one 8-wide n tile whose column 0 holds the
+// output channel. Returns this warp's sum of its output pixels (lanes with lane % 4 == 0 hold column 0 of rows g and
+// g + 8), bias excluded.
+__device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *frags)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int mrow = ((lane >> 3) & 1) * 8 + (lane & 7), khalf = lane >> 4;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(in);
+    float sum = 0.0f;
+    for (int mt = warp; mt < 16; mt += kPT / 32) {  // m tile mt: output row mt, 16 pixels
+        float c[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const int q = (mt + k / 3) * 18 + mrow + k % 3;
+            uint32_t a0, a1, a2, a3;
+            ldmatrix_x4(base + q * 32 + khalf * 16, a0, a1, a2, a3);
+            const uint32_t *fk = frags + k * 2 * 32 + lane;
+            mma_bf16(c, a0, a1, a2, a3, fk[0], fk[32]);
+        }
+        if ((lane & 3) == 0) sum += c[0] + c[2];
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+    return sum;
+}
+
 __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ PredBatch b)
 {
     __shared__ PredSmem sm;
@@ -317,6 +338,16 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
     const PredJob &J = b.job[j];
     const int tile = blockIdx.x - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
     const int X0 = 64 * tx - 16, Y0 = 64 * ty - 16;
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int code = (warp + 4 * k) * 32 + lane;
+            const unsigned m = __ballot_sync(kFull, code < b.band.band_size && needs_cvalue(code, b.band));
+            if (lane == 0) sm.needbits[warp + 4 * k] = m;
+        }
+    }
+    __syncthreads();
     // features of the 24 x 24 window, and whether a pixel of the tile itself needs a c-value
     bool need = false;
     for (int i = tid; i < kFeatTile * kFeatTile; i += kPT) {
@@ -324,7 +355,7 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
         float f0, f1;
         bool nd;
         const bool own = u >= 4 && u < 20 && v >= 4 && v < 20;
-        block_features(J.word, J.w, J.h, X0 + 4 * u, Y0 + 4 * v, own ? &b.band : nullptr, f0, f1, nd);
+        block_features(J.word, J.w, J.h, X0 + 4 * u, Y0 + 4 * v, own ? &b.band : nullptr, sm.needbits, f0, f1, nd);
         sm.f[0][v][u] = f0;
         sm.f[1][v][u] = f1;
         need |= nd;
@@ -337,52 +368,40 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
         if (tid == 0) b.pred[blockIdx.x] = -INFINITY;
         return;
     }
-    // layer 0: 2 -> 16, 22 x 22 outputs
-    for (int p = tid; p < 22 * 22; p += kPT) {
-        const int y = p / 22, x = p - y * 22;
-        float acc[16];
+    // layer 0: 2 -> 16, 22 x 22 outputs; warp g computes channels 4 g .. 4 g + 3 with their weights in registers
+    {
+        const int lane = tid & 31, cg = tid >> 5;
+        float wr[4][18], br[4];
 #pragma unroll
-        for (int co = 0; co < 16; co++) acc[co] = sm.w0[288 + co];
-#pragma unroll 1
-        for (int ck = 0; ck < 18; ck++) {  // input channel ci = ck / 9, tap k = ck % 9
-            const int ci = ck / 9, k = ck - 9 * ci;
-            const float v = sm.f[ci][y + k / 3][x + k % 3];
+        for (int c = 0; c < 4; c++) {
+            br[c] = sm.w0[288 + 4 * cg + c];
 #pragma unroll
-            for (int co = 0; co < 16; co++) acc[co] = __fmaf_rn(v, sm.w0[(co * 2 + ci) * 9 + k], acc[co]);
+            for (int ck = 0; ck < 18; ck++) wr[c][ck] = sm.w0[(4 * cg + c) * 18 + ck];  // [co][ci][k] = co * 18 + ci * 9 + k
         }
-        uint4 *dst = (uint4 *)(sm.a1 + p * 8);
-        dst[0] = make_uint4(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)), pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)),
-                            pack_bf16(fmaxf(acc[4], 0.f), fmaxf(acc[5], 0.f)), pack_bf16(fmaxf(acc[6], 0.f), fmaxf(acc[7], 0.f)));
-        dst[1] = make_uint4(pack_bf16(fmaxf(acc[8], 0.f), fmaxf(acc[9], 0.f)), pack_bf16(fmaxf(acc[10], 0.f), fmaxf(acc[11], 0.f)),
-                            pack_bf16(fmaxf(acc[12], 0.f), fmaxf(acc[13], 0.f)), pack_bf16(fmaxf(acc[14], 0.f), fmaxf(acc[15], 0.f)));
+        for (int p = lane; p < 22 * 22; p += 32) {
+            const int y = p / 22, x = p - y * 22;
+            float acc[4] = {br[0], br[1], br[2], br[3]};
+#pragma unroll
+            for (int ck = 0; ck < 18; ck++) {
+                const int ci = ck / 9, k = ck % 9;
+                const float v = sm.f[ci][y + k / 3][x + k % 3];
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[c] = __fmaf_rn(v, wr[c][ck], acc[c]);
+            }
+            *(uint2 *)(sm.a1 + p * 8 + 2 * cg) = make_uint2(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)),
+                                                            pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)));
+        }
     }
     __syncthreads();
     mma_layer(sm.a1, 22, sm.a2, 20, sm.frags, sm.b12[0]);                   // layer 1: 20 x 20
     __syncthreads();
     mma_layer(sm.a2, 20, sm.a1, 18, sm.frags + 9 * 2 * 2 * 32, sm.b12[1]);  // layer 2: 18 x 18, into a1
     __syncthreads();
-    // layer 3: 16 -> 1 on 16 x 16, then the tile mean (a fixed order of additions)
-    float s = 0.0f;
-    for (int p = tid; p < 256; p += kPT) {
-        const int y = p >> 4, x = p & 15;
-        float acc = sm.w3[144];
-#pragma unroll 1
-        for (int k = 0; k < 9; k++) {
-            const uint32_t *src = sm.a1 + ((y + k / 3) * 18 + x + k % 3) * 8;
-#pragma unroll
-            for (int c2 = 0; c2 < 8; c2++) {
-                const float2 v = unpack_bf16(src[c2]);
-                acc = __fmaf_rn(v.x, sm.w3[(2 * c2) * 9 + k], acc);
-                acc = __fmaf_rn(v.y, sm.w3[(2 * c2 + 1) * 9 + k], acc);
-            }
-        }
-        s += acc;
-    }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    // layer 3: 16 -> 1 on 16 x 16 (tensor cores), then the tile mean (a fixed order of additions)
+    const float s = mma_head(sm.a1, sm.frags + kNetFrags12);
     if ((tid & 31) == 0) sm.part[tid >> 5] = s;
     __syncthreads();
-    if (tid == 0) b.pred[blockIdx.x] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f;
+    if (tid == 0) b.pred[blockIdx.x] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f + sm.w3[144];
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -488,6 +507,13 @@ __global__ void net_pack_kernel(const float *R, uint32_t *frags)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kNetFrags) return;
+    if (i >= kNetFrags12) {  // layer 3: word [k][r][lane], column n = lane / 4 holds the weights when n == 0, else 0
+        const int q = i - kNetFrags12, lane = q & 31, r = (q >> 5) & 1, k = q >> 6;
+        const int n = lane >> 2, c = 2 * (lane & 3) + 8 * r;
+        const float *W = R + net_w(3);
+        frags[i] = n == 0 ? pack_bf16(W[c * 9 + k], W[(c + 1) * 9 + k]) : 0u;
+        return;
+    }
     const int lane = i & 31, r = (i >> 5) & 1, j = (i >> 6) & 1, k = (i >> 7) % 9, l = 1 + (i >> 7) / 9;
     const int n = 8 * j + (lane >> 2), c = 2 * (lane & 3) + 8 * r;
     const float *W = R + net_w(l);
