@@ -504,7 +504,7 @@ void record_step(es_batch &b, long f, uint32_t skip)
         j.h = S.h;
         j.pd = S.pd;
         j.first_block = first;
-        first += (int)(((size_t)(S.w / 2) * (S.h / 2) + 255) / 256);
+        first += unpack_blocks(S.w, S.h);
     }
     ub.total_blocks = first;
     cuda_check(launch_unpack(ub, s), "batch unpacking");

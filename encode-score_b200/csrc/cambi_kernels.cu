@@ -121,30 +121,47 @@ __global__ void __launch_bounds__(256) prep0_kernel(const __grid_constant__ Prep
 
 // ---------------------------------------------------------------------------------------------------------------
 // Scales 1-4: src/kernels.cu:43-53 (decimate) and 488-500 (mode) on the decimated picture, mask decimated alongside.
+// A block of 256 threads makes a 64 x 16 tile: the decimated words of the tile and a 1-pixel margin (the even rows
+// and columns of the previous scale, 4-byte loads keeping the even half) are staged in shared memory; thread (c, g)
+// then makes column c of rows 4 g .. 4 g + 3 from 6 horizontal modes.
 // ---------------------------------------------------------------------------------------------------------------
+constexpr int kDTW = 64, kDTH = 16;
+
 __global__ void __launch_bounds__(256) decimate_mode_kernel(const __grid_constant__ DecBatch b)
 {
+    __shared__ uint16_t d[kDTH + 2][kDTW + 2];
     int j = 0;
     while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
     const DecJob &J = b.job[j];
-    const int i = (blockIdx.x - J.first_block) * 256 + threadIdx.x;
-    if (i >= J.w * J.h) return;
-    const int x = i % J.w, y = i / J.w, w = J.w, h = J.h;
-    auto val = [&](int xx, int yy) -> uint16_t { return J.src[(size_t)(2 * yy) * J.sw + 2 * xx] & 0x7FFF; };
-    const uint16_t m = J.src[(size_t)(2 * y) * J.sw + 2 * x] & kMaskBit;
-    uint16_t v;
-    if (y == 0 || y == h - 1) {
-        v = val(x, y);
-    } else {
-        uint16_t mm[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const int rr = y - 1 + k;
-            mm[k] = (x == 0 || x == w - 1) ? val(x, rr) : mode3(val(x - 1, rr), val(x, rr), val(x + 1, rr));
+    const int w = J.w, h = J.h, tiles_x = (w + kDTW - 1) / kDTW, t = blockIdx.x - J.first_block;
+    const int x0 = (t % tiles_x) * kDTW, y0 = (t / tiles_x) * kDTH;
+    for (int i = threadIdx.x; i < (kDTH + 2) * (kDTW + 2); i += 256) {
+        const int r = i / (kDTW + 2), c = i - r * (kDTW + 2), X = x0 - 1 + c, Y = y0 - 1 + r;
+        uint16_t v = 0;
+        if (X >= 0 && X < w && Y >= 0 && Y < h) {  // word (2 X, 2 Y) of the previous scale
+            const uint16_t *p = J.src + (size_t)(2 * Y) * J.sw + 2 * X;
+            // the low half of a 4-byte load, unless the word ends an odd-width row (the high half would be past it)
+            v = 2 * X + 1 < J.sw ? (uint16_t)(__ldg((const unsigned *)p) & 0xFFFFu) : *p;
         }
-        v = mode3(mm[0], mm[1], mm[2]);
+        d[r][c] = v;
     }
-    J.dst[i] = (uint16_t)(v | m);
+    __syncthreads();
+    const int c = threadIdx.x & (kDTW - 1), r0 = (threadIdx.x >> 6) * 4, x = x0 + c;
+    if (x >= w) return;
+    auto val = [&](int r, int cc) -> uint16_t { return d[r][cc] & 0x7FFF; };
+    const bool edge_x = x == 0 || x == w - 1;
+    uint16_t hm[6];  // horizontal modes of tile rows r0 - 1 .. r0 + 4 (staged rows r0 .. r0 + 5)
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        hm[k] = edge_x ? val(r0 + k, c + 1) : mode3(val(r0 + k, c), val(r0 + k, c + 1), val(r0 + k, c + 2));
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int y = y0 + r0 + i;
+        if (y >= h) break;
+        const uint16_t word = d[r0 + i + 1][c + 1];
+        const uint16_t v = (y == 0 || y == h - 1) ? (uint16_t)(word & 0x7FFF) : mode3(hm[i], hm[i + 1], hm[i + 2]);
+        J.dst[(size_t)y * w + x] = (uint16_t)(v | (word & kMaskBit));
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -315,8 +332,14 @@ cudaError_t launch_prep0(const Prep0Batch &b, cudaStream_t s)
     return after_launch();
 }
 
-cudaError_t launch_decimate_mode(const DecBatch &b, cudaStream_t s)
+cudaError_t launch_decimate_mode(DecBatch &b, cudaStream_t s)
 {
+    int blocks = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        b.job[j].first_block = blocks;
+        blocks += ((b.job[j].w + kDTW - 1) / kDTW) * ((b.job[j].h + kDTH - 1) / kDTH);
+    }
+    b.total_blocks = blocks;
     if (b.total_blocks <= 0) return cudaSuccess;
     LaunchTimer t("cambi_decimate_mode", s);
     decimate_mode_kernel<<<b.total_blocks, 256, 0, s>>>(b);
@@ -337,7 +360,7 @@ cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width,
     if (nslots <= 0) return cudaSuccess;
     {
         LaunchTimer t("cambi_select_hist", s);
-        select_hist_kernel<<<296, 256, 0, s>>>(slots, nslots, shift, width);
+        select_hist_kernel<<<148 * 8, 256, 0, s>>>(slots, nslots, shift, width);
     }
     cudaError_t e = after_launch();
     if (e != cudaSuccess) return e;
@@ -350,7 +373,7 @@ cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s)
 {
     if (nslots <= 0) return cudaSuccess;
     LaunchTimer t("cambi_sum_above", s);
-    sum_above_kernel<<<296, 256, 0, s>>>(slots, nslots);
+    sum_above_kernel<<<148 * 8, 256, 0, s>>>(slots, nslots);
     return after_launch();
 }
 

@@ -70,14 +70,14 @@ struct DecJob {
     int sw, sh;
     uint16_t *dst;        // this scale's words, w x h
     int w, h;
-    int first_block;      // blocks of 256 pixels
+    int first_block;      // set by the launcher: the job's first 64 x 16 output tile
 };
 constexpr int kDecMaxJobs = kMaxPictures;
 struct DecBatch {
     DecJob job[kDecMaxJobs];
-    int njobs, total_blocks;
+    int njobs, total_blocks;  // total_blocks: set by the launcher
 };
-cudaError_t launch_decimate_mode(const DecBatch &b, cudaStream_t s);
+cudaError_t launch_decimate_mode(DecBatch &b, cudaStream_t s);
 
 // ---- c-values --------------------------------------------------------------------------------------------------------
 // Per picture-scale counters in device memory. The c-values are exact multiples of 2^-24 (they are at least 0.5), so
@@ -154,9 +154,11 @@ struct UnpackJob {
     int x0, y0;
     uint16_t *y16, *u16, *v16;  // w x h, w/2 x h/2
     int w, h, pd;               // common picture area and pipeline depth of this picture's source
-    int first_block;            // blocks of 2 x 2-pixel groups
+    int first_block;            // in blocks of unpack_blocks(w, h)
 };
 constexpr int kUnpackMaxJobs = kMaxPictures;
+// Blocks of 256 threads for one picture of w x h: a thread takes 4 consecutive 2 x 2 groups of a chroma row.
+inline int unpack_blocks(int w, int h) { return (int)(((size_t)((w / 2 + 3) / 4) * (h / 2) + 255) / 256); }
 struct UnpackView {
     FrameViewDev f;
     int x0, y0;

@@ -89,7 +89,7 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     const int at = (int)(f % 2), up = 10 - fr->pd;
     // unpack every picture of the step in one launch
     UnpackBatch ub{};
-    const int blocks = (int)(((size_t)(fr->w / 2) * (fr->h / 2) + 255) / 256);
+    const int blocks = unpack_blocks(fr->w, fr->h);
     int first = 0;
     for (int p = 0; p <= fr->nenc; p++) {
         UnpackJob &j = ub.job[p];

@@ -23,6 +23,9 @@ __device__ __forceinline__ unsigned sample_at(const void *plane, int pitch, int 
     return v >> f.shift;
 }
 
+// Thread i takes 4 consecutive 2 x 2 groups of one chroma row (2 rows x 8 luma columns, 4 samples of U and of V).
+// Planar frames whose rows and crop allow it are moved with 16- / 8-byte loads and stores; every other layout
+// (semi-planar, shifted samples such as P010, odd alignments) one sample at a time.
 __global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ UnpackBatch b)
 {
     int j = 0;
@@ -30,22 +33,58 @@ __global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ Unp
     const UnpackJob &J = b.job[j];
     const FrameViewDev f = b.views ? b.views[j].f : J.f;
     const int x0 = b.views ? b.views[j].x0 : J.x0, y0 = b.views ? b.views[j].y0 : J.y0;
-    const int cw = J.w / 2, ch = J.h / 2;
+    const int cw = J.w / 2, ch = J.h / 2, qw = (cw + 3) / 4;
     const int i = (blockIdx.x - J.first_block) * 256 + threadIdx.x;
-    if (i >= cw * ch) return;
-    const int cx = i % cw, cy = i / cw, up = J.pd - f.depth;
+    if (i >= qw * ch) return;
+    const int cy = i / qw, cx0 = 4 * (i - cy * qw), up = J.pd - f.depth;
+    const bool full = cx0 + 4 <= cw && !f.semi && f.shift == 0 && (x0 & 7) == 0;
+    if (full && f.bytes == 2 && (f.ypitch & 15) == 0 && (f.cpitch & 7) == 0 && (((uintptr_t)f.y & 15) | ((uintptr_t)f.u & 7) | ((uintptr_t)f.v & 7)) == 0 &&
+        (J.w & 7) == 0) {
+        auto sh4 = [&](uint4 q) { return make_uint4(q.x << up, q.y << up, q.z << up, q.w << up); };  // samples < 2^10
 #pragma unroll
-    for (int dy = 0; dy < 2; dy++) {
-        const int y = 2 * cy + dy;
-        const unsigned a = sample_at(f.y, f.ypitch, 2 * cx + x0, y + y0, f);
-        const unsigned c = sample_at(f.y, f.ypitch, 2 * cx + 1 + x0, y + y0, f);
-        *(uint32_t *)(J.y16 + (size_t)y * J.w + 2 * cx) = (a << up) | ((c << up) << 16);
+        for (int dy = 0; dy < 2; dy++) {
+            const uint4 q = __ldg((const uint4 *)((const unsigned char *)f.y + (size_t)(2 * cy + dy + y0) * f.ypitch) + (2 * cx0 + x0) / 8);
+            *(uint4 *)(J.y16 + (size_t)(2 * cy + dy) * J.w + 2 * cx0) = sh4(q);
+        }
+        const size_t co = (size_t)(cy + y0 / 2) * f.cpitch;
+        const uint2 u = __ldg((const uint2 *)((const unsigned char *)f.u + co) + (cx0 + x0 / 2) / 4);
+        const uint2 v = __ldg((const uint2 *)((const unsigned char *)f.v + co) + (cx0 + x0 / 2) / 4);
+        *(uint2 *)(J.u16 + (size_t)cy * cw + cx0) = make_uint2(u.x << up, u.y << up);
+        *(uint2 *)(J.v16 + (size_t)cy * cw + cx0) = make_uint2(v.x << up, v.y << up);
+        return;
     }
-    const int sx = (2 * cx + x0) / 2, sy = (2 * cy + y0) / 2;
-    const unsigned u = f.semi ? sample_at(f.u, f.cpitch, 2 * sx, sy, f) : sample_at(f.u, f.cpitch, sx, sy, f);
-    const unsigned v = f.semi ? sample_at(f.u, f.cpitch, 2 * sx + 1, sy, f) : sample_at(f.v, f.cpitch, sx, sy, f);
-    J.u16[(size_t)cy * cw + cx] = (uint16_t)(u << up);
-    J.v16[(size_t)cy * cw + cx] = (uint16_t)(v << up);
+    if (full && f.bytes == 1 && (f.ypitch & 7) == 0 && (f.cpitch & 3) == 0 && (((uintptr_t)f.y & 7) | ((uintptr_t)f.u & 3) | ((uintptr_t)f.v & 3)) == 0 &&
+        (J.w & 7) == 0) {
+        auto widen2 = [&](unsigned q) {  // 4 bytes -> 4 16-bit samples, shifted
+            return make_uint2(__byte_perm(q, 0, 0x4140) << up, __byte_perm(q, 0, 0x4342) << up);
+        };
+#pragma unroll
+        for (int dy = 0; dy < 2; dy++) {
+            const uint2 q = __ldg((const uint2 *)((const unsigned char *)f.y + (size_t)(2 * cy + dy + y0) * f.ypitch) + (2 * cx0 + x0) / 8);
+            const uint2 lo = widen2(q.x), hi = widen2(q.y);
+            *(uint4 *)(J.y16 + (size_t)(2 * cy + dy) * J.w + 2 * cx0) = make_uint4(lo.x, lo.y, hi.x, hi.y);
+        }
+        const size_t co = (size_t)(cy + y0 / 2) * f.cpitch;
+        const unsigned u = __ldg((const unsigned *)((const unsigned char *)f.u + co) + (cx0 + x0 / 2) / 4);
+        const unsigned v = __ldg((const unsigned *)((const unsigned char *)f.v + co) + (cx0 + x0 / 2) / 4);
+        *(uint2 *)(J.u16 + (size_t)cy * cw + cx0) = widen2(u);
+        *(uint2 *)(J.v16 + (size_t)cy * cw + cx0) = widen2(v);
+        return;
+    }
+    for (int cx = cx0; cx < min(cx0 + 4, cw); cx++) {
+#pragma unroll
+        for (int dy = 0; dy < 2; dy++) {
+            const int y = 2 * cy + dy;
+            const unsigned a = sample_at(f.y, f.ypitch, 2 * cx + x0, y + y0, f);
+            const unsigned c = sample_at(f.y, f.ypitch, 2 * cx + 1 + x0, y + y0, f);
+            *(uint32_t *)(J.y16 + (size_t)y * J.w + 2 * cx) = (a << up) | ((c << up) << 16);
+        }
+        const int sx = (2 * cx + x0) / 2, sy = (2 * cy + y0) / 2;
+        const unsigned u = f.semi ? sample_at(f.u, f.cpitch, 2 * sx, sy, f) : sample_at(f.u, f.cpitch, sx, sy, f);
+        const unsigned v = f.semi ? sample_at(f.u, f.cpitch, 2 * sx + 1, sy, f) : sample_at(f.v, f.cpitch, sx, sy, f);
+        J.u16[(size_t)cy * cw + cx] = (uint16_t)(u << up);
+        J.v16[(size_t)cy * cw + cx] = (uint16_t)(v << up);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
