@@ -24,38 +24,50 @@ __device__ __forceinline__ uint16_t mode3(uint16_t a, uint16_t b, uint16_t c)
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Scale 0: src/kernels.cu:524-535 (from8), 14-40 (mask), 488-500 (mode), in one pass over a 64 x 32 tile.
-// The preprocessed values are staged with a 3-4 pixel margin; a warp per row packs the flat pixels into bit words by
-// ballot; each thread then walks 8 rows of one column, counting the 7 flat bits around it with a funnel shift and a
-// popcount, summing 7 rows as it goes, and applying the separable mode filter from running row modes.
+// Scale 0: src/kernels.cu:524-535 (from8), 14-40 (mask), 488-500 (mode), in one pass over a 64 x 64 tile.
+// The plane is staged with its margins (8-byte loads for tiles inside the picture); an 8-bit plane is turned into
+// 10-bit anti-dithered values, a 10-bit one is used as staged. A warp per row packs the flat pixels into bit words by
+// ballot; each thread then walks 16 rows of one column, counting the 7 flat bits around each pixel with a funnel shift
+// and a popcount, summing 7 rows as it goes, and applying the separable mode filter from running row modes.
+// Staged region: columns x0-4 .. x0+71 (index x - (x0-4)), rows y0-3 .. y0+68 (index y - (y0-3)).
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int kP0W = 64, kP0H = 32;                       // output tile
-constexpr int kP0RW = kP0W + 8, kP0RH = kP0H + 8;         // input region x0-3 .. x0+kP0W+4 (72 x 40)
-constexpr int kP0FW = kP0W + 6, kP0FH = kP0H + 6;         // flat pixels x0-3 .. x0+kP0W+2 (70 x 38)
+constexpr int kP0T = 64;                    // output tile side
+constexpr int kP0C = kP0T + 12, kP0R = kP0T + 8;  // staged columns (76) and rows (72)
+constexpr int kP0F = kP0T + 6;              // flat pixels per side: x0-3 .. x0+66, y0-3 .. y0+66
 
-__global__ void __launch_bounds__(256) prep0_kernel(const __grid_constant__ Prep0Batch b)
+__global__ void __launch_bounds__(256, 3) prep0_kernel(const __grid_constant__ Prep0Batch b)
 {
-    __shared__ uint16_t raw[kP0RH][kP0RW];
-    __shared__ uint16_t pre[kP0RH - 1][kP0RW];
-    __shared__ uint32_t flatbits[kP0FH][3];
+    __shared__ __align__(16) uint16_t raw[kP0R][kP0C];
+    __shared__ __align__(16) uint16_t pre8[kP0R - 1][kP0C];
+    __shared__ uint32_t flatbits[kP0F][3];
     int j = 0;
     while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
     const Prep0Job &J = b.job[j];
     const int t = blockIdx.x - J.first_tile, w = J.w, h = J.h, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int x0 = (t % J.tiles_x) * kP0W, y0 = (t / J.tiles_x) * kP0H;
-    for (int i = tid; i < kP0RH * kP0RW; i += 256) {
-        const int r = i / kP0RW, c = i - r * kP0RW, x = x0 - 3 + c, y = y0 - 3 + r;
-        raw[r][c] = (x >= 0 && x < w && y >= 0 && y < h) ? J.img[(size_t)y * J.pitch + x] : (uint16_t)0;
+    const int x0 = (t % J.tiles_x) * kP0T, y0 = (t / J.tiles_x) * kP0T;
+    const int xs = x0 - 4, ys = y0 - 3;
+    const bool inside = xs >= 0 && xs + kP0C <= w && ys >= 0 && ys + kP0R <= h && (J.pitch & 3) == 0 && (((uintptr_t)J.img) & 7) == 0;
+    if (inside) {
+        for (int i = tid; i < kP0R * (kP0C / 4); i += 256) {
+            const int r = i / (kP0C / 4), q = i - r * (kP0C / 4);
+            *(uint2 *)&raw[r][4 * q] = __ldg((const uint2 *)(J.img + (size_t)(ys + r) * J.pitch + xs) + q);
+        }
+    } else {
+        for (int i = tid; i < kP0R * kP0C; i += 256) {
+            const int r = i / kP0C, c = i - r * kP0C, x = xs + c, y = ys + r;
+            raw[r][c] = (x >= 0 && x < w && y >= 0 && y < h) ? J.img[(size_t)y * J.pitch + x] : (uint16_t)0;
+        }
     }
     __syncthreads();
-    // preprocessed values of x0-3 .. x0+kP0W+3, y0-3 .. y0+kP0H+3
+    // preprocessed values of x0-4 .. x0+71, y0-3 .. y0+67: an 8-bit plane at 10 bits, the mean of the 2 x 2 block to
+    // the lower right (pairs on the last row and column); a 10-bit plane as staged (0 outside the picture)
+    const uint16_t(*pre)[kP0C] = raw;
     if (J.depth == 8) {
-        for (int i = tid; i < (kP0RH - 1) * (kP0RW - 1); i += 256) {
-            const int r = i / (kP0RW - 1), c = i - r * (kP0RW - 1), x = x0 - 3 + c, y = y0 - 3 + r;
+        for (int i = tid; i < (kP0R - 1) * (kP0C - 1); i += 256) {
+            const int r = i / (kP0C - 1), c = i - r * (kP0C - 1), x = xs + c, y = ys + r;
             unsigned v = 0;
             if (x >= 0 && x < w && y >= 0 && y < h) {
-                // 10 bits, then the mean of the 2x2 block to the lower right; pairs on the last row and column
                 const unsigned a = (unsigned)raw[r][c] << 2;
                 if (x < w - 1 && y < h - 1)
                     v = (a + ((unsigned)raw[r][c + 1] << 2) + ((unsigned)raw[r + 1][c] << 2) + ((unsigned)raw[r + 1][c + 1] << 2)) >> 2;
@@ -63,56 +75,55 @@ __global__ void __launch_bounds__(256) prep0_kernel(const __grid_constant__ Prep
                 else if (x < w - 1) v = (a + ((unsigned)raw[r][c + 1] << 2)) >> 1;
                 else v = a;
             }
-            pre[r][c] = (uint16_t)v;
+            pre8[r][c] = (uint16_t)v;
         }
-    } else {
-        for (int i = tid; i < (kP0RH - 1) * (kP0RW - 1); i += 256) {
-            const int r = i / (kP0RW - 1), c = i - r * (kP0RW - 1);
-            pre[r][c] = raw[r][c];
-        }
+        __syncthreads();
+        pre = pre8;
     }
-    __syncthreads();
     // flat: equal to the right and lower neighbours (the last column / row count as equal); nothing outside
-    for (int q = warp; q < kP0FH; q += 8) {
-        const int y = y0 - 3 + q;
+    const bool interior = x0 >= 3 && x0 + kP0T + 3 < w && y0 >= 3 && y0 + kP0T + 3 < h;
+    for (int q = warp; q < kP0F; q += 8) {
+        const int y = ys + q;
         uint32_t words[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const int c = lane + 32 * k, x = x0 - 3 + c;
+            const int c = lane + 32 * k, x = x0 - 3 + c;  // staged column c + 1
             bool f = false;
-            if (c < kP0FW && x >= 0 && x < w && y >= 0 && y < h) {
-                const uint16_t v = pre[q][c];
-                f = (x == w - 1 || v == pre[q][c + 1]) && (y == h - 1 || v == pre[q + 1][c]);
+            if (c < kP0F) {
+                const uint16_t v = pre[q][c + 1];
+                if (interior) f = v == pre[q][c + 2] && v == pre[q + 1][c + 1];
+                else if (x >= 0 && x < w && y >= 0 && y < h)
+                    f = (x == w - 1 || v == pre[q][c + 2]) && (y == h - 1 || v == pre[q + 1][c + 1]);
             }
             words[k] = __ballot_sync(0xffffffffu, f);
         }
         if (lane < 3) flatbits[q][lane] = lane == 0 ? words[0] : lane == 1 ? words[1] : words[2];
     }
     __syncthreads();
-    const int c = tid & (kP0W - 1), r0 = (tid >> 6) * 8, x = x0 + c;
+    const int c = tid & (kP0T - 1), g = tid >> 6, x = x0 + c;
     if (x >= w) return;
-    // flat counts of the 7 columns around x in flat rows r0 .. r0 + 13, summed 7 rows at a time
-    int h7[14];
-    const int k = c >> 5, sh = c & 31;
+    // flat counts of the 7 columns around x in flat rows 16 g .. 16 g + 21 (bit c of a row is column x - 3)
+    int h7[22];
+    const int kw = c >> 5, sh = c & 31;
 #pragma unroll
-    for (int q = 0; q < 14; q++) h7[q] = __popc(__funnelshift_r(flatbits[r0 + q][k], flatbits[r0 + q][k + 1], sh) & 0x7Fu);
-    // horizontal mode of pre rows r0 + 2 .. r0 + 12 (pictures rows y0 + r0 - 1 .. y0 + r0 + 9)
-    uint16_t hm[11];
+    for (int q = 0; q < 22; q++) h7[q] = __popc(__funnelshift_r(flatbits[16 * g + q][kw], flatbits[16 * g + q][kw + 1], sh) & 0x7Fu);
+    // horizontal modes of picture rows y0 + 16 g - 1 .. y0 + 16 g + 16 (staged rows 16 g + 2 .. 16 g + 19)
+    uint16_t hm[18];
     const bool edge_x = x == 0 || x == w - 1;
 #pragma unroll
-    for (int q = 0; q < 11; q++) {
-        const uint16_t *row = pre[r0 + 2 + q];
-        hm[q] = edge_x ? row[c + 3] : mode3(row[c + 2], row[c + 3], row[c + 4]);
+    for (int k = 0; k < 18; k++) {
+        const uint16_t *row = pre[16 * g + 2 + k];
+        hm[k] = edge_x ? row[c + 4] : mode3(row[c + 3], row[c + 4], row[c + 5]);
     }
     int cnt = 0;
 #pragma unroll
     for (int q = 0; q < 6; q++) cnt += h7[q];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < 16; i++) {
         cnt += h7[i + 6];
-        const int y = y0 + r0 + i;
+        const int y = y0 + 16 * g + i;
         if (y < h) {
-            const uint16_t v = (y == 0 || y == h - 1) ? pre[r0 + i + 3][c + 3] : mode3(hm[i], hm[i + 1], hm[i + 2]);
+            const uint16_t v = (y == 0 || y == h - 1) ? pre[16 * g + 3 + i][c + 4] : mode3(hm[i], hm[i + 1], hm[i + 2]);
             J.word[(size_t)y * w + x] = (uint16_t)(v | (cnt > J.mask_index ? kMaskBit : 0));
         }
         cnt -= h7[i];
@@ -324,8 +335,16 @@ __global__ void score_kernel(const __grid_constant__ ScoreBatch b)
 
 }  // namespace
 
-cudaError_t launch_prep0(const Prep0Batch &b, cudaStream_t s)
+cudaError_t launch_prep0(Prep0Batch &b, cudaStream_t s)
 {
+    int tiles = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        Prep0Job &J = b.job[j];
+        J.tiles_x = (J.w + kP0T - 1) / kP0T;
+        J.first_tile = tiles;
+        tiles += J.tiles_x * ((J.h + kP0T - 1) / kP0T);
+    }
+    b.total_tiles = tiles;
     if (b.total_tiles <= 0) return cudaSuccess;
     LaunchTimer t("cambi_prep0", s);
     prep0_kernel<<<b.total_tiles, 256, 0, s>>>(b);

@@ -55,14 +55,14 @@ struct Prep0Job {
     const uint16_t *img;  // input plane, `pitch` pixels per row
     int pitch, w, h, depth, mask_index;
     uint16_t *word;       // out: w x h, mode-filtered value | mask << 15
-    int tiles_x, first_tile;
+    int tiles_x, first_tile;  // set by the launcher
 };
 constexpr int kPrep0MaxJobs = kMaxPictures;
 struct Prep0Batch {
     Prep0Job job[kPrep0MaxJobs];
-    int njobs, total_tiles;
+    int njobs, total_tiles;  // total_tiles: set by the launcher
 };
-cudaError_t launch_prep0(const Prep0Batch &b, cudaStream_t s);
+cudaError_t launch_prep0(Prep0Batch &b, cudaStream_t s);
 
 // ---- scales 1..4: decimation and mode filter ------------------------------------------------------------------------
 struct DecJob {

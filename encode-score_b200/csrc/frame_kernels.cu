@@ -87,73 +87,7 @@ __global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ Unp
     }
 }
 
-// ---------------------------------------------------------------------------------------------------------------
-// Box sums over a 64 x 32 tile with a 4-pixel margin, edge pixels repeated (src/kernels.cu:346-428 and
-// reference/encode_score/compare.py:77-108). The horizontal 3- and 9-sums of the region are built in shared memory
-// (the 9-sum from three 3-sums); the vertical sums are running sums in registers. A block of 256 threads: warp w owns
-// window (w % 4, w / 4) of the tile, lane l its column l % 16 and rows (l / 16) * 8 .. + 8.
-// ---------------------------------------------------------------------------------------------------------------
-constexpr int kTW = 64, kTH = 32, kM = 4;
-constexpr int kRW = kTW + 2 * kM, kRH = kTH + 2 * kM;  // 72 x 40
-constexpr int kH3 = kTW + 6;                           // 3-sums centred at x0-3 .. x0+66
-
-struct BoxSmem {
-    uint16_t y[kRH][kRW];   // values on the 10-bit scale (or running sums of them)
-    uint16_t h3[kRH][kH3];  // h3[r][j]: 3-sum centred at x0 - 3 + j
-    uint16_t h9[kRH][kTW];  // h9[r][c]: 9-sum centred at x0 + c
-};
-
-// Loads a plane's region (clamped coordinates), shifted left by `up`; a null plane reads 0.
-__device__ __forceinline__ void load_region(uint16_t (*dst)[kRW], const uint16_t *src, int w, int h, int up, int x0, int y0)
-{
-    for (int i = threadIdx.x; i < kRH * kRW; i += 256) {
-        const int r = i / kRW, c = i - r * kRW;
-        const int x = min(max(x0 - kM + c, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
-        dst[r][c] = src ? (uint16_t)(src[(size_t)y * w + x] << up) : (uint16_t)0;
-    }
-}
-
-// h3 and h9 of the region in sm.y; the caller synchronises before and after.
-__device__ __forceinline__ void horizontal_sums(BoxSmem &sm)
-{
-    for (int i = threadIdx.x; i < kRH * kH3; i += 256) {
-        const int r = i / kH3, j = i - r * kH3;
-        sm.h3[r][j] = (uint16_t)(sm.y[r][j] + sm.y[r][j + 1] + sm.y[r][j + 2]);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kRH * kTW; i += 256) {
-        const int r = i >> 6, c = i & (kTW - 1);
-        sm.h9[r][c] = (uint16_t)(sm.h3[r][c] + sm.h3[r][c + 3] + sm.h3[r][c + 6]);
-    }
-}
-
-// 3x3 sums at tile column c (+ dc) for the N tile rows r_first .. r_first + N - 1.
-template <int N>
-__device__ __forceinline__ void column_s3(const BoxSmem &sm, int c, int dc, int r_first, int (&out)[N])
-{
-    int v[N + 2];
-#pragma unroll
-    for (int i = 0; i < N + 2; i++) v[i] = sm.h3[r_first + kM - 1 + i][c + 3 + dc];
-#pragma unroll
-    for (int i = 0; i < N; i++) out[i] = v[i] + v[i + 1] + v[i + 2];
-}
-
-// 9x9 sums at tile column c for the 8 tile rows r0 .. r0 + 7 (a running sum down the column).
-__device__ __forceinline__ void column_s9(const BoxSmem &sm, int c, int r0, int (&out)[8])
-{
-    int v[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = sm.h9[r0 + i][c];
-    int s = 0;
-#pragma unroll
-    for (int i = 0; i < 9; i++) s += v[i];
-    out[0] = s;
-#pragma unroll
-    for (int i = 1; i < 8; i++) {
-        s += v[i + 8] - v[i - 1];
-        out[i] = s;
-    }
-}
+constexpr int kM = 4;  // margin of a staged region: the 9 x 9 box reaches 4 pixels
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v)
@@ -344,94 +278,137 @@ __global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_const
 
 // ---------------------------------------------------------------------------------------------------------------
 // Lasting texture: src/kernels.cu:435-451, exact, from running luma sums (see PersistJob).
+//
+// A block of 256 threads takes a 64 x 64 tile (4 x 4 windows): it advances the running sums E and O over the tile and
+// its 4-pixel margin (coordinates clamped, so the margins repeat the edges) and writes them for the tile's own pixels;
+// then, as in window_stats, the horizontal 3- and 9-sums of E, of O and of each picture are built in shared memory and
+// thread (c, g) walks tile column c down window row g with running vertical sums of the mid-detail numerators.
 // ---------------------------------------------------------------------------------------------------------------
-// mid detail x 81 (9 S3 - S9) of the region in sm.y at the thread's 8 pixels
-__device__ __forceinline__ void mids_of(BoxSmem &sm, int c, int r0, int (&mid)[8])
+// mid-detail numerators 9 S3 - S9 of the 16 rows from tile row r0 at tile column c, from the horizontal sums
+__device__ __forceinline__ void window_mids(const WinSmem &sm, int c, int r0, int (&m)[kWin])
 {
-    int s3[8], s9[8];
-    column_s3<8>(sm, c, 0, r0, s3);
-    column_s9(sm, c, r0, s9);
+    auto h3c = [&](int t) { return (int)sm.h3[t + kM][c + 1]; };
+    auto h9c = [&](int t) { return (int)sm.h9[t + kM][c]; };
+    int s3 = h3c(r0 - 1) + h3c(r0) + h3c(r0 + 1);
+    int s9 = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) mid[i] = 9 * s3[i] - s9[i];
+    for (int k = -4; k <= 4; k++) s9 += h9c(r0 + k);
+#pragma unroll
+    for (int i = 0; i < kWin; i++) {
+        const int t = r0 + i;
+        m[i] = 9 * s3 - s9;
+        if (i + 1 < kWin) {
+            s3 += h3c(t + 2) - h3c(t - 1);
+            s9 += h9c(t + 5) - h9c(t - 4);
+        }
+    }
 }
 
-__global__ void __launch_bounds__(256) persist_kernel(const __grid_constant__ PersistBatch B)
+__global__ void __launch_bounds__(256, 2) persist_kernel(const __grid_constant__ PersistBatch B)
 {
-    __shared__ BoxSmem sm;
-    __shared__ uint16_t o_reg[kRH][kRW];
+    __shared__ __align__(16) WinSmem sm;
+    __shared__ __align__(16) uint16_t o_reg[kWR][kWS];
     int jb = 0;
     while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_block) jb++;
     const PersistJob &J = B.job[jb];
     const int bid = blockIdx.x - J.first_block;
     const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
-    const int tiles_x = (w + kTW - 1) / kTW;
-    const int x0 = (bid % tiles_x) * kTW, y0 = (bid / tiles_x) * kTH;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // advance the running sums over the region (clamped coordinates, so the margins repeat the edges)
-    for (int i = threadIdx.x; i < kRH * kRW; i += 256) {
-        const int r = i / kRW, cc = i - r * kRW;
-        const int x = min(max(x0 - kM + cc, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
-        const size_t k = (size_t)y * w + x;
-        const int ym13 = J.y_m13 ? (int)(J.y_m13[k] << J.up) : 0, ym7 = J.y_m7 ? (int)(J.y_m7[k] << J.up) : 0;
-        const int yc = J.y_c ? (int)(J.y_c[k] << J.up) : 0, yf = J.y_f ? (int)(J.y_f[k] << J.up) : 0;
-        const int e = (int)J.o_old[k] - yc + yf;     // E(c) = O(c-1) - y(c) + y(c+6)
-        const int o = (int)J.e_old[k] - ym13 + ym7;  // O(c) = E(c-1) - y(c-7) + y(c-1)
-        sm.y[r][cc] = (uint16_t)e;
-        o_reg[r][cc] = (uint16_t)o;
-        const int xi = x0 - kM + cc, yi = y0 - kM + r;
-        if (xi >= x0 && xi < x0 + kTW && yi >= y0 && yi < y0 + kTH && xi < w && yi < h) {
-            J.e_new[k] = (uint16_t)e;
-            J.o_new[k] = (uint16_t)o;
+    const int tiles_x = (w + kWT - 1) / kWT;
+    const int x0 = (bid % tiles_x) * kWT, y0 = (bid / tiles_x) * kWT;
+    const int tid = threadIdx.x, lane = tid & 31;
+    // advance the running sums over the region: E(c) = O(c-1) - y(c) + y(c+6), O(c) = E(c-1) - y(c-7) + y(c-1)
+    const uint16_t *pl[4] = {J.y_m13, J.y_m7, J.y_c, J.y_f};
+    uintptr_t align = (uintptr_t)J.e_old | (uintptr_t)J.o_old | (uintptr_t)J.e_new | (uintptr_t)J.o_new;
+    for (int k = 0; k < 4; k++) align |= (uintptr_t)pl[k];
+    if (x0 >= kM && x0 + kWT + kM <= w && (w & 3) == 0 && (align & 7) == 0) {
+        // interior columns: 18 groups of 4 pixels per region row, packed 16-bit arithmetic (no element leaves 0..65535)
+        for (int i = tid; i < kWR * 18; i += 256) {
+            const int r = i / 18, q = i - r * 18, yu = y0 - kM + r, y = min(max(yu, 0), h - 1);
+            const size_t k = (size_t)y * w + (x0 - kM) + 4 * q;
+            uint2 v[4];
+#pragma unroll
+            for (int n = 0; n < 4; n++) {
+                v[n] = pl[n] ? __ldg((const uint2 *)(pl[n] + k)) : make_uint2(0, 0);
+                v[n].x <<= J.up;
+                v[n].y <<= J.up;
+            }
+            const uint2 oo = __ldg((const uint2 *)(J.o_old + k)), eo = __ldg((const uint2 *)(J.e_old + k));
+            const uint2 e = make_uint2(__vadd2(__vsub2(oo.x, v[2].x), v[3].x), __vadd2(__vsub2(oo.y, v[2].y), v[3].y));
+            const uint2 o = make_uint2(__vadd2(__vsub2(eo.x, v[0].x), v[1].x), __vadd2(__vsub2(eo.y, v[0].y), v[1].y));
+            *(uint2 *)&sm.y[r][4 * q] = e;
+            *(uint2 *)&o_reg[r][4 * q] = o;
+            if (r >= kM && r < kM + kWT && yu < h && q >= 1 && q <= 16) {
+                *(uint2 *)(J.e_new + k) = e;
+                *(uint2 *)(J.o_new + k) = o;
+            }
+        }
+    } else {
+        for (int i = tid; i < kWR * kWR; i += 256) {
+            const int r = i / kWR, cc = i - r * kWR;
+            const int xi = x0 - kM + cc, yi = y0 - kM + r;
+            const int x = min(max(xi, 0), w - 1), y = min(max(yi, 0), h - 1);
+            const size_t k = (size_t)y * w + x;
+            int yv[4];
+#pragma unroll
+            for (int n = 0; n < 4; n++) yv[n] = pl[n] ? (int)(pl[n][k] << J.up) : 0;
+            const int e = (int)J.o_old[k] - yv[2] + yv[3];
+            const int o = (int)J.e_old[k] - yv[0] + yv[1];
+            sm.y[r][cc] = (uint16_t)e;
+            o_reg[r][cc] = (uint16_t)o;
+            if (xi >= x0 && xi < x0 + kWT && yi >= y0 && yi < y0 + kWT && xi < w && yi < h) {
+                J.e_new[k] = (uint16_t)e;
+                J.o_new[k] = (uint16_t)o;
+            }
         }
     }
     if (!J.stats) return;
-    const int wx = x0 / kWin + (warp & 3), wy = y0 / kWin + (warp >> 2);
+    const int c = tid & (kWT - 1), r0 = (tid >> 6) * kWin;
+    const int wx = (x0 + c) / kWin, wy = (y0 + r0) / kWin;
     const bool inside = wx < ww && wy < wh;
-    const int c = (warp & 3) * kWin + (lane & 15), r0 = (warp >> 2) * kWin + (lane >> 4) * 8;
-    int a[8], bb[8], t[8];
+    int a[kWin], bb[kWin], t[kWin];
     __syncthreads();
-    horizontal_sums(sm);
+    window_horizontal_sums(sm);
     __syncthreads();
-    mids_of(sm, c, r0, a);  // A x 486 = mid x 81 of E
+    window_mids(sm, c, r0, a);  // A x 486 = mid x 81 of E
     __syncthreads();
-    for (int i = threadIdx.x; i < kRH * kRW; i += 256) sm.y[i / kRW][i % kRW] = o_reg[i / kRW][i % kRW];
+    for (int i = tid; i < kWR * kWS / 8; i += 256) ((uint4 *)&sm.y[0][0])[i] = ((const uint4 *)&o_reg[0][0])[i];
     __syncthreads();
-    horizontal_sums(sm);
+    window_horizontal_sums(sm);
     __syncthreads();
-    mids_of(sm, c, r0, bb);  // B x 486
+    window_mids(sm, c, r0, bb);  // B x 486
     long long sab = 0, saa = 0, sbb = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < kWin; i++) {
         t[i] = a[i] + bb[i];  // T x 972
         sab += (long long)a[i] * bb[i];
         saa += (long long)a[i] * a[i];
         sbb += (long long)bb[i] * bb[i];
     }
-    sab = warp_sum(sab);
-    saa = warp_sum(saa);
-    sbb = warp_sum(sbb);
+    sab = half_warp_sum(sab);
+    saa = half_warp_sum(saa);
+    sbb = half_warp_sum(sbb);
     long long own = 0;
     for (int p = 0; p <= J.nenc; p++) {
         const uint16_t *plane = p == 0 ? J.y_c : J.yd[p - 1];
         __syncthreads();
-        load_region(sm.y, plane, w, h, J.up, x0, y0);
+        stage_window_region(sm, plane, w, h, J.up, x0, y0);
         __syncthreads();
-        horizontal_sums(sm);
+        window_horizontal_sums(sm);
         __syncthreads();
-        int m[8];
-        mids_of(sm, c, r0, m);
-        long long s = 0;
+        int m[kWin];
+        window_mids(sm, c, r0, m);
+        long long sp = 0;
 #pragma unroll
-        for (int i = 0; i < 8; i++) s += (long long)m[i] * t[i];
-        s = warp_sum(s);
+        for (int i = 0; i < kWin; i++) sp += (long long)m[i] * t[i];
+        sp = half_warp_sum(sp);
         if (p == 0) {
-            own = s;
+            own = sp;
             continue;
         }
-        if (inside && lane == 0) {
+        if (inside && (lane & 15) == 0) {
             float *o = J.out[p - 1] + ((size_t)wy * ww + wx) * 5;
             o[0] = exact_ratio(own, 78732.0);
-            o[1] = exact_ratio(s, 78732.0);
+            o[1] = exact_ratio(sp, 78732.0);
             o[2] = exact_ratio(sab, 236196.0);
             o[3] = exact_ratio(saa, 236196.0);
             o[4] = exact_ratio(sbb, 236196.0);
@@ -728,7 +705,7 @@ cudaError_t launch_persist(PersistBatch &b, cudaStream_t s)
     for (int j = 0; j < b.njobs; j++) {
         PersistJob &J = b.job[j];
         J.first_block = blocks;
-        blocks += ((J.w + kTW - 1) / kTW) * ((J.h + kTH - 1) / kTH);
+        blocks += ((J.w + kWT - 1) / kWT) * ((J.h + kWT - 1) / kWT);
     }
     if (blocks == 0) return cudaSuccess;
     LaunchTimer t("persist_stats", s);
