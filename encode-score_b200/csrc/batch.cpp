@@ -86,6 +86,9 @@ struct es_batch {
     const uint32_t *net_frags = nullptr;
     int total_tiles = 0, total_tiles0 = 0;   // c-value tiles of every scale / of scale 0, all pictures
     DeviceBuffer<float> pred;                // per scale-0 tile
+    DeviceBuffer<unsigned> need;             // per scale-0 tile
+    DeviceBuffer<float2> feat;               // feature maps, picture by picture
+    std::vector<size_t> feat_at;             // each picture's map offset
     DeviceBuffer<uint8_t> kind;              // per tile
     DeviceBuffer<unsigned> lists;            // list_a, then list_b (total_tiles each)
     DeviceBuffer<unsigned> counters;         // count_a, count_b, next_a, next_b, n_audit[kMaxJobs], n_skip[kMaxJobs]
@@ -225,9 +228,11 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
         j.tiles_x = (pic.w + kCvTX - 1) / kCvTX;
         j.tiles_y = (pic.h + kCvTY - 1) / kCvTY;
         j.first_tile = t0;
+        j.feat = b.feat.ptr + b.feat_at[run[r]];
         t0 += j.tiles_x * j.tiles_y;
     }
     pb.total_tiles = t0;
+    pb.need = b.need.ptr;
     pb.band = cb.band;
     pb.params = b.net_params;
     pb.frags = b.net_frags;
@@ -747,6 +752,14 @@ int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_o
             b->total_tiles0 = tiles0;
             const int P = (int)b->pictures.size();
             b->pred.reset(tiles0);
+            b->need.reset(tiles0);
+            size_t fs = 0;
+            b->feat_at.clear();
+            for (auto &pp : b->pictures) {
+                b->feat_at.push_back(fs);
+                fs += feature_map_size(pp->w, pp->h);
+            }
+            b->feat.reset(fs);
             b->kind.reset(tiles);
             b->lists.reset(2 * (size_t)tiles);
             b->counters.reset(4 + 2 * kMaxJobs);

@@ -269,16 +269,21 @@ constexpr int kNetFrags = kNetFrags12 + 9 * 2 * 32;
 struct PredJob {
     const uint16_t *word;  // scale-0 words of a picture
     int w, h, tiles_x, tiles_y, first_tile;
+    float2 *feat;          // its feature map: ceil(h / 4) x ceil(w / 4) (mean, mask share) pairs
+    int first_block;       // set by the features launcher
 };
 struct PredBatch {
     PredJob job[kMaxPictures];
     int njobs, total_tiles;
     Band band;
     const float *params;    // bfloat16-rounded parameters (as floats)
-    const uint32_t *frags;  // B fragments of layers 1 and 2
+    const uint32_t *frags;  // B fragments of layers 1, 2 and 3
+    unsigned *need;         // per scale-0 tile: non-zero when a pixel of it needs a c-value (zeroed by the launcher)
     float *pred;            // per scale-0 tile: the prediction, -inf where no pixel needs a c-value
 };
-cudaError_t launch_predict(const PredBatch &b, cudaStream_t s);
+// Both kernels of a prediction: the feature maps (and need flags) of every picture, then the network per tile.
+cudaError_t launch_predict(PredBatch &b, cudaStream_t s);
+inline size_t feature_map_size(int w, int h) { return (size_t)((w + 3) / 4) * ((h + 3) / 4); }
 
 // Features of n crops: crop i covers scale-0 pixels from (xy[2 i], xy[2 i + 1]) on, fw x fh feature pixels of 4 x 4.
 cudaError_t launch_net_features(const uint16_t *word, int w, int h, const int *xy, int n, int fw, int fh, float *out,

@@ -20,6 +20,9 @@ struct es_proposal_net {
     int cap_n = 0, cap_h = 0, cap_w = 0;
     DeviceBuffer<float> a1, a2, a3, z, g3, g2, g1, gz, loss_parts;
     PinnedBuffer<float> h_loss;
+    // es_proposal_predict's feature map and need flags, sized for the largest picture seen
+    DeviceBuffer<float2> feat;
+    DeviceBuffer<unsigned> need;
 };
 
 namespace {
@@ -190,6 +193,10 @@ int es_proposal_predict(es_proposal_net *net, uint64_t words, int w, int h, floa
             pb.band.tvi[d] = p.tvi[d];
             pb.band.weight[d] = p.weight[d];
         }
+        if (net->feat.count < feature_map_size(w, h)) net->feat.reset(feature_map_size(w, h));
+        if (net->need.count < (size_t)pb.total_tiles) net->need.reset(pb.total_tiles);
+        j.feat = net->feat.ptr;
+        pb.need = net->need.ptr;
         pb.params = proposal_net_rounded(net, s);
         pb.frags = net->frags.ptr;
         pb.pred = pred;

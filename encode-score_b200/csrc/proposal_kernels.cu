@@ -89,6 +89,37 @@ __global__ void __launch_bounds__(256) net_features_kernel(const uint16_t *word,
     }
 }
 
+// The feature map of every picture of a prediction (one thread per 4 x 4 block) and the need flag of each scale-0 tile.
+__global__ void __launch_bounds__(256) feature_map_kernel(const __grid_constant__ PredBatch b)
+{
+    __shared__ uint32_t needbits[32];
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int code = (warp + 8 * k) * 32 + lane;
+            const unsigned m = __ballot_sync(0xffffffffu, code < b.band.band_size && needs_cvalue(code, b.band));
+            if (lane == 0) needbits[warp + 8 * k] = m;
+        }
+    }
+    __syncthreads();
+    int j = 0;
+    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
+    const PredJob &J = b.job[j];
+    const int fw = (J.w + 3) / 4, fh = (J.h + 3) / 4;
+    const int i = (blockIdx.x - J.first_block) * 256 + threadIdx.x;
+    if (i >= fw * fh) return;
+    const int v = i / fw, u = i - v * fw;
+    float f0, f1;
+    bool need;
+    block_features(J.word, J.w, J.h, 4 * u, 4 * v, &b.band, needbits, f0, f1, need);
+    J.feat[i] = make_float2(f0, f1);
+    if (need) {  // most blocks of a tile that needs c-values find the flag already set: read before the atomic
+        unsigned *flag = &b.need[J.first_tile + (v >> 4) * J.tiles_x + (u >> 4)];
+        if (!*(volatile unsigned *)flag) atomicOr(flag, 1u);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Training: valid 3 x 3 convolutions on NCHW float crops, weights rounded to bfloat16.
 // ---------------------------------------------------------------------------------------------------------------
@@ -247,7 +278,6 @@ struct PredSmem {
     __align__(16) uint32_t a1[22 * 22 * 8];       // layer-0 output, [pixel][16 channels] bfloat16; later layer 2's
     __align__(16) uint32_t a2[20 * 20 * 8];       // layer-1 output
     uint32_t frags[kNetFrags];                    // B fragments of layers 1, 2 and 3
-    uint32_t needbits[32];                        // codes that need a c-value
     float part[kPT / 32];
 };
 
@@ -264,6 +294,10 @@ __device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t &r0, uint32_
                  : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
                  : "r"(addr));
 }
+
+// Activation planes hold pixel p's 16 channels in 32 bytes, its two 16-byte halves swapped when bit 2 of p is set,
+// so the 8 rows an ldmatrix phase reads (consecutive pixels) fall on different banks.
+__device__ __forceinline__ int phys_half(int p, int half) { return half ^ ((p >> 2) & 1); }
 
 // One 16 -> 16 layer: input plane `in` (iw x iw pixels of 16 bfloat16 channels, 32 bytes each), output plane `out`
 // (ow x ow, ow = iw - 2), bias, ReLU, bfloat16. Warp w takes m tiles w, w + 4, ...: 16 output pixels each, numbered
@@ -284,7 +318,7 @@ __device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *
         for (int k = 0; k < 9; k++) {
             const int q = (oy + k / 3) * iw + ox + k % 3;
             uint32_t a0, a1, a2, a3;
-            ldmatrix_x4(base + q * 32 + khalf * 16, a0, a1, a2, a3);
+            ldmatrix_x4(base + q * 32 + phys_half(q, khalf) * 16, a0, a1, a2, a3);
             const uint32_t *fk = frags + k * 4 * 32 + lane;  // this tap's fragments: (n tile, register) x lane
             mma_bf16(c[0], a0, a1, a2, a3, fk[0], fk[32]);
             mma_bf16(c[1], a0, a1, a2, a3, fk[64], fk[96]);
@@ -297,7 +331,7 @@ __device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *
                 const int pr = 16 * mt + g + 8 * hrow;
                 if (pr >= npx) continue;
                 const float v0 = fmaxf(c[j][2 * hrow] + bias[ch], 0.0f), v1 = fmaxf(c[j][2 * hrow + 1] + bias[ch + 1], 0.0f);
-                out[pr * 8 + ch / 2] = pack_bf16(v0, v1);
+                out[pr * 8 + phys_half(pr, j) * 4 + t] = pack_bf16(v0, v1);  // channels 8 j + 2 t, + 1
             }
         }
     }
@@ -318,7 +352,7 @@ __device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *fr
         for (int k = 0; k < 9; k++) {
             const int q = (mt + k / 3) * 18 + mrow + k % 3;
             uint32_t a0, a1, a2, a3;
-            ldmatrix_x4(base + q * 32 + khalf * 16, a0, a1, a2, a3);
+            ldmatrix_x4(base + q * 32 + phys_half(q, khalf) * 16, a0, a1, a2, a3);
             const uint32_t *fk = frags + k * 2 * 32 + lane;
             mma_bf16(c, a0, a1, a2, a3, fk[0], fk[32]);
         }
@@ -337,37 +371,24 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
     while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
     const PredJob &J = b.job[j];
     const int tile = blockIdx.x - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
-    const int X0 = 64 * tx - 16, Y0 = 64 * ty - 16;
-    {
-        const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int code = (warp + 4 * k) * 32 + lane;
-            const unsigned m = __ballot_sync(kFull, code < b.band.band_size && needs_cvalue(code, b.band));
-            if (lane == 0) sm.needbits[warp + 4 * k] = m;
-        }
+    if (!b.need[blockIdx.x]) {  // no pixel of the tile needs a c-value: nothing to predict (the same for the block)
+        if (tid == 0) b.pred[blockIdx.x] = -INFINITY;
+        return;
     }
-    __syncthreads();
-    // features of the 24 x 24 window, and whether a pixel of the tile itself needs a c-value
-    bool need = false;
+    // the 24 x 24 feature window: map pixels 16 tx - 4 .. 16 tx + 19 (a tile is 16 map pixels; 0 outside the map)
+    const int fw = (J.w + 3) / 4, fh = (J.h + 3) / 4;
     for (int i = tid; i < kFeatTile * kFeatTile; i += kPT) {
-        const int v = i / kFeatTile, u = i - v * kFeatTile;
-        float f0, f1;
-        bool nd;
-        const bool own = u >= 4 && u < 20 && v >= 4 && v < 20;
-        block_features(J.word, J.w, J.h, X0 + 4 * u, Y0 + 4 * v, own ? &b.band : nullptr, sm.needbits, f0, f1, nd);
-        sm.f[0][v][u] = f0;
-        sm.f[1][v][u] = f1;
-        need |= nd;
+        const int v = i / kFeatTile, u = i - v * kFeatTile, gu = 16 * tx - 4 + u, gv = 16 * ty - 4 + v;
+        float2 f = make_float2(0.0f, 0.0f);
+        if (gu >= 0 && gu < fw && gv >= 0 && gv < fh) f = J.feat[(size_t)gv * fw + gu];
+        sm.f[0][v][u] = f.x;
+        sm.f[1][v][u] = f.y;
     }
     for (int i = tid; i < 304; i += kPT) sm.w0[i] = b.params[net_w(0) + i];
     for (int i = tid; i < 145; i += kPT) sm.w3[i] = b.params[net_w(3) + i];
     if (tid < 32) sm.b12[tid >> 4][tid & 15] = b.params[(tid < 16 ? net_b(1) : net_b(2)) + (tid & 15)];
     for (int i = tid; i < kNetFrags; i += kPT) sm.frags[i] = b.frags[i];
-    if (!__syncthreads_or(need)) {
-        if (tid == 0) b.pred[blockIdx.x] = -INFINITY;
-        return;
-    }
+    __syncthreads();
     // layer 0: 2 -> 16, 22 x 22 outputs; warp g computes channels 4 g .. 4 g + 3 with their weights in registers
     {
         const int lane = tid & 31, cg = tid >> 5;
@@ -388,7 +409,7 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
 #pragma unroll
                 for (int c = 0; c < 4; c++) acc[c] = __fmaf_rn(v, wr[c][ck], acc[c]);
             }
-            *(uint2 *)(sm.a1 + p * 8 + 2 * cg) = make_uint2(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)),
+            *(uint2 *)(sm.a1 + p * 8 + phys_half(p, cg >> 1) * 4 + (cg & 1) * 2) = make_uint2(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)),
                                                             pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)));
         }
     }
@@ -524,9 +545,22 @@ unsigned grid_for(size_t total) { return (unsigned)((total + 255) / 256 < 148 * 
 
 }  // namespace
 
-cudaError_t launch_predict(const PredBatch &b, cudaStream_t s)
+cudaError_t launch_predict(PredBatch &b, cudaStream_t s)
 {
     if (b.total_tiles <= 0) return cudaSuccess;
+    int blocks = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        b.job[j].first_block = blocks;
+        blocks += (int)((feature_map_size(b.job[j].w, b.job[j].h) + 255) / 256);
+    }
+    cudaError_t e = cudaMemsetAsync(b.need, 0, sizeof(unsigned) * b.total_tiles, s);
+    if (e != cudaSuccess) return e;
+    {
+        LaunchTimer t("proposal_features", s);
+        feature_map_kernel<<<blocks, 256, 0, s>>>(b);
+    }
+    e = after_launch();
+    if (e != cudaSuccess) return e;
     LaunchTimer t("proposal_predict", s);
     predict_kernel<<<b.total_tiles, kPT, 0, s>>>(b);
     return after_launch();
