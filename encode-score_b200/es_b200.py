@@ -31,6 +31,8 @@ SYMBOLS = (
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
     "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
     "es_windows_create", "es_windows_compute", "es_windows_figures", "es_windows_destroy",
+    "es_per_frame_json", "es_cambi_cache_open", "es_cambi_cache_find", "es_cambi_cache_add", "es_cambi_cache_file",
+    "es_cambi_cache_close",
     "es_batch_graph_launches", "es_batch_destroy", "es_batch_set_proposal", "es_batch_proposal_stats",
 )
 
@@ -158,6 +160,14 @@ def lib() -> ctypes.CDLL:
         L.es_proposal_features.argtypes = [U64, I, I, P, I, I, I, P, P]
         L.es_proposal_predict.argtypes = [P, U64, I, I, P, P]
         L.es_proposal_net_destroy.argtypes = [P]
+        L.es_per_frame_json.argtypes = [P, P, P, P, ctypes.c_long, ctypes.c_char_p, ctypes.c_size_t]
+        L.es_per_frame_json.restype = ctypes.c_size_t
+        L.es_cambi_cache_open.argtypes = [ctypes.c_char_p, I, I, I, I, I, ctypes.c_char_p, ctypes.POINTER(P)]
+        L.es_cambi_cache_find.argtypes = [P, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]
+        L.es_cambi_cache_add.argtypes = [P, ctypes.c_int64, ctypes.c_double]
+        L.es_cambi_cache_file.argtypes = [P]
+        L.es_cambi_cache_file.restype = ctypes.c_char_p
+        L.es_cambi_cache_close.argtypes = [P]
         L.es_windows_create.argtypes = [I, I, ctypes.POINTER(P)]
         L.es_windows_compute.argtypes = [P, U64, U64, I, P]
         L.es_windows_figures.argtypes = [P, I, I, P, P]
@@ -311,6 +321,43 @@ class Windows:
     def close(self) -> None:
         if self.handle:
             lib().es_windows_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+def per_frame_json(cambi, cambi_source, psnr_y, vmaf=None) -> str:
+    """The per_frame JSON object of the reference's report (src/main.cpp:767-774)."""
+    import numpy as np
+    arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (vmaf, cambi, cambi_source, psnr_y)]
+    n = len(arrs[1])
+    ptrs = [None if a is None else a.ctypes.data for a in arrs]
+    size = lib().es_per_frame_json(*ptrs, n, None, 0)
+    buf = ctypes.create_string_buffer(size + 1)
+    lib().es_per_frame_json(*ptrs, n, buf, size + 1)
+    return buf.value.decode()
+
+
+class CambiCache:
+    """class CambiCache (src/cache.hpp) through the C ABI: the source's CAMBI per frame on disk."""
+
+    def __init__(self, path: str, x0: int, y0: int, w: int, h: int, depth: int, directory: str | None = None):
+        self.handle = ctypes.c_void_p()
+        check(lib().es_cambi_cache_open(path.encode(), x0, y0, w, h, depth, directory.encode() if directory else None,
+                                        ctypes.byref(self.handle)))
+
+    def find(self, pts: int):
+        v = ctypes.c_double()
+        return v.value if lib().es_cambi_cache_find(self.handle, pts, ctypes.byref(v)) else None
+
+    def add(self, pts: int, score: float) -> None:
+        check(lib().es_cambi_cache_add(self.handle, pts, score))
+
+    @property
+    def file(self) -> str:
+        return lib().es_cambi_cache_file(self.handle).decode()
+
+    def close(self) -> None:
+        if self.handle:
+            lib().es_cambi_cache_close(self.handle)
             self.handle = ctypes.c_void_p()
 
 

@@ -168,6 +168,31 @@ void es_accum_score(const es_accum *a, const es_weights *weights, es_parts *out)
  * writing at most `size` bytes. */
 size_t es_accum_json(const es_accum *a, char *buf, size_t size);
 
+/* The per_frame object of src/main.cpp:767-774 for n frames ({"vmaf": [...], "cambi": [...], "cambi_source": [...],
+ * "psnr_y": [...]}, same digits); vmaf NULL writes "vmaf": null (VMAF is outside this library). Returns the length it
+ * needs (excluding the NUL), writing at most `size` bytes. */
+size_t es_per_frame_json(const double *vmaf, const double *cambi, const double *cambi_source, const double *psnr_y, long n,
+                         char *buf, size_t size);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Source-CAMBI cache: class CambiCache (src/cache.hpp:9-29, src/cache.cpp:13-88), same key and file format. The
+ * source's CAMBI per frame, kept on disk so a later run against the same source skips it (es_frame_queue /
+ * es_batch_queue with the source's CAMBI off and the cached value given to collect). Host only.
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct es_cambi_cache es_cambi_cache;
+/* CambiCache(path, x0, y0, w, h, depth): `path` is the source file (its size and first and last MiB key the cache);
+ * dir NULL = $XDG_CACHE_HOME/encode-score or $HOME/.cache/encode-score. A cache that cannot be opened works as an empty
+ * one that stores nothing. */
+int es_cambi_cache_open(const char *path, int x0, int y0, int w, int h, int depth, const char *dir, es_cambi_cache **out);
+/* CambiCache::find: 1 and *score when frame `pts` is cached, else 0 (INT64_MIN, a frame without a timestamp, is never
+ * cached). */
+int es_cambi_cache_find(const es_cambi_cache *c, int64_t pts, double *score);
+/* CambiCache::add: kept in memory, written every 240 scores and on close. */
+int es_cambi_cache_add(es_cambi_cache *c, int64_t pts, double score);
+/* CambiCache::file: the cache file's path ("" when there is none). */
+const char *es_cambi_cache_file(const es_cambi_cache *c);
+void es_cambi_cache_close(es_cambi_cache *c);
+
 /* PSNR as src/main.cpp:272-277: 10 log10(peak^2 / mse) capped at 6 depth + 12. */
 double es_psnr(uint64_t sse, uint64_t n, int depth);
 
