@@ -370,6 +370,7 @@ def main() -> None:
     ap.add_argument("--pool", type=int, default=6, help="distinct frame steps cycled through")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only-head", action="store_true", help="time only the headline form (for profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -503,19 +504,21 @@ def main() -> None:
 
     pairs = args.steps * n_enc * world
     forms = {}
-    plain = PlainForm()
-    ms_plain, launches_plain, clk_plain, f = time_form(plain, 0)
-    forms["plain"] = {"value": pairs / (ms_plain / 1000.0), "ms_per_step": ms_plain / args.steps, "form": plain.name,
-                      "gpu_launches": int(launches_plain)}
-    plain.close()
-    batched = BatchedForm()
-    ms_b, launches_b, clk, _ = time_form(batched, 0)
-    batched.close()
-    forms["batched"] = {"value": pairs / (ms_b / 1000.0), "ms_per_step": ms_b / args.steps, "form": batched.name,
-                        "gpu_launches": int(launches_b)}
-    head = "batched"
-    ms, launches = ms_b, launches_b
-    if os.path.exists(os.path.join(ROOT, "encode-score_b200", "proposal_net.npy")):
+    have_net = os.path.exists(os.path.join(ROOT, "encode-score_b200", "proposal_net.npy"))
+    if not (args.only_head and have_net):
+        plain = PlainForm()
+        ms_plain, launches_plain, clk_plain, f = time_form(plain, 0)
+        forms["plain"] = {"value": pairs / (ms_plain / 1000.0), "ms_per_step": ms_plain / args.steps, "form": plain.name,
+                          "gpu_launches": int(launches_plain)}
+        plain.close()
+        batched = BatchedForm()
+        ms_b, launches_b, clk, _ = time_form(batched, 0)
+        batched.close()
+        forms["batched"] = {"value": pairs / (ms_b / 1000.0), "ms_per_step": ms_b / args.steps, "form": batched.name,
+                            "gpu_launches": int(launches_b)}
+        head = "batched"
+        ms, launches = ms_b, launches_b
+    if have_net:
         learned = LearnedForm()
         ms_l, launches_l, clk, _ = time_form(learned, 0)
         learned.close()

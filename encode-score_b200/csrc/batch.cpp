@@ -73,7 +73,11 @@ struct es_batch {
     Stream main, side;
     Event start, fork, join, done[2];
     bool use_graphs = true;
-    std::map<std::pair<int, uint32_t>, cudaGraphExec_t> graphs;  // (ring phase, skipped sources) -> step
+    struct Step {
+        cudaGraphExec_t exec;
+        long long kernels;  // kernel nodes of the graph, counted as launches at each replay
+    };
+    std::map<std::pair<int, uint32_t>, Step> graphs;  // (ring phase, skipped sources) -> step
     uint32_t skipped[2] = {0, 0};
     long queued[2] = {-1, -1};
     long next = 0, last_collected = -1;
@@ -100,7 +104,7 @@ struct es_batch {
 
     ~es_batch()
     {
-        for (auto &g : graphs) cudaGraphExecDestroy(g.second);
+        for (auto &g : graphs) cudaGraphExecDestroy(g.second.exec);
     }
     int encode_picture(int s, int e) const { return sources[s]->picture + 1 + e; }
 };
@@ -538,6 +542,7 @@ void queue_step(es_batch &b, long f, uint32_t skip)
     auto it = b.graphs.find(key);
     if (it == b.graphs.end()) {
         cudaGraph_t g = nullptr;
+        const unsigned long long counted = es_launch_count();
         cuda_check(cudaStreamBeginCapture(b.main.s, cudaStreamCaptureModeThreadLocal), "capturing a step");
         try {
             record_step(b, f, skip);
@@ -546,14 +551,27 @@ void queue_step(es_batch &b, long f, uint32_t skip)
             if (g) cudaGraphDestroy(g);
             throw;
         }
+        count_launches(-(long long)(es_launch_count() - counted));  // recorded, not launched
         cuda_check(cudaStreamEndCapture(b.main.s, &g), "capturing a step");
+        size_t n = 0;
+        long long kernels = 0;
+        cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+        if (e == cudaSuccess && n) {
+            std::vector<cudaGraphNode_t> nodes(n);
+            e = cudaGraphGetNodes(g, nodes.data(), &n);
+            for (size_t i = 0; e == cudaSuccess && i < n; i++) {
+                cudaGraphNodeType type;
+                if (cudaGraphNodeGetType(nodes[i], &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) kernels++;
+            }
+        }
         cudaGraphExec_t exec = nullptr;
-        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
         cuda_check(e, "instantiating a step graph");
-        it = b.graphs.emplace(key, exec).first;
+        it = b.graphs.emplace(key, es_batch::Step{exec, kernels}).first;
     }
-    cuda_check(cudaGraphLaunch(it->second, b.main.s), "launching a step graph");
+    cuda_check(cudaGraphLaunch(it->second.exec, b.main.s), "launching a step graph");
+    count_launches(it->second.kernels);
     b.graph_launches++;
 }
 
@@ -730,7 +748,7 @@ int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_o
                 "es_batch_set_proposal: audit rates are per mille, 0 to 1000");
         require(o.tolerance >= 0, "es_batch_set_proposal: tolerance must be >= 0");
         cuda_check(cudaStreamSynchronize(b->main.s), "es_batch_set_proposal");
-        for (auto &g : b->graphs) cudaGraphExecDestroy(g.second);  // captured steps belong to the old setting
+        for (auto &g : b->graphs) cudaGraphExecDestroy(g.second.exec);  // captured steps belong to the old setting
         b->graphs.clear();
         b->net = net;
         b->popt = o;

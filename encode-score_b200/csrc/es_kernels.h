@@ -12,6 +12,9 @@ namespace es {
 
 // Every launcher below ends with after_launch(): it counts the launch (es_launch_count) and returns its error.
 void count_launch();
+// Adds n (which may be negative) to the launch count: a graph replay counts its kernel nodes, a capture takes back
+// the launches its recording counted.
+void count_launches(long long n);
 inline cudaError_t after_launch()
 {
     count_launch();

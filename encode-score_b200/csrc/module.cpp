@@ -20,6 +20,7 @@ std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
 // ---- kernel timing (diagnostics) -------------------------------------------------------------------------------------
 namespace {

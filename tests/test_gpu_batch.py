@@ -106,9 +106,14 @@ def test_batch_equals_one_frame_per_source(cuda, module, steps):
 
 
 def test_batch_without_graphs_equals_with(cuda, module, steps):
+    l0 = es_b200.launch_count()
     a, aacc, ga = run_batch(cuda, module, steps, use_graphs=False)
+    l1 = es_b200.launch_count()
     b, bacc, gb = run_batch(cuda, module, steps, use_graphs=True)
+    l2 = es_b200.launch_count()
     assert ga == 0 and gb == FRAMES - 14
+    # a replayed step counts its graph's kernel nodes: the same launches as the step launched one by one
+    assert l2 - l1 == l1 - l0 > 0
     for s in range(len(SOURCES)):
         assert a[s][0] == b[s][0]
     assert [accum_bytes(x) for x in aacc] == [accum_bytes(x) for x in bacc]
