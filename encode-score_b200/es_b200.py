@@ -13,7 +13,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libes_b200.so")
+# ES_B200_LIB selects another build of the library (another optimisation level, a profiling build)
+LIB_PATH = os.environ.get("ES_B200_LIB") or os.path.join(HERE, "libes_b200.so")
 
 ES_OK, ES_ERR_INVALID, ES_ERR_CUDA, ES_ERR_ALLOC, ES_ERR_STATE, ES_ERR_DEVICE = range(6)
 HIST_BINS = 20001
