@@ -35,12 +35,12 @@ __host__ __device__ constexpr int cv_rw(int pad) { return kCvTX + 2 * pad; }
 __host__ __device__ constexpr int cv_stride(int pad) { return (cv_rw(pad) + 7 + 7) & ~7; }
 __host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // rank plane row (scan width)
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
-__host__ __device__ constexpr size_t max_sz(size_t a, size_t b) { return a > b ? a : b; }
 
-// Shared memory: the rank plane and the per-code and per-rank tables, then a union of the staged codes (dead once
-// the rank plane is built) and the pass buffers.
+// Shared memory: the rank plane, the per-code and per-rank tables and the pass buffers. (The band codes are read from
+// global memory twice, once for the code tables and once for the rank plane, instead of being staged: the smaller
+// footprint lets 4 blocks share an SM.)
 struct CvLayout {
-    size_t rplane, rank, rcode, nbr, relneed, codes, wcount, prefix, list, total;
+    size_t rplane, rank, rcode, nbr, relneed, wcount, prefix, list, total;
 };
 __host__ __device__ inline CvLayout cv_layout(int pad)
 {
@@ -51,11 +51,10 @@ __host__ __device__ inline CvLayout cv_layout(int pad)
     l.rcode = align16(l.rank + (size_t)kMaxBand * 2);
     l.nbr = align16(l.rcode + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
-    l.codes = align16(l.relneed + (size_t)kMaxBand * 2);
-    l.wcount = l.codes;
+    l.wcount = align16(l.relneed + (size_t)kMaxBand * 2);
     l.prefix = align16(l.wcount + (size_t)kCvChunk * (kCvBins / 2) * kCvTX * 4);
     l.list = align16(l.prefix + (size_t)kWarps * cv_cs(pad) * 4);
-    l.total = align16(max_sz(l.codes + (size_t)cv_stride(pad) * rh * 2, l.list + (size_t)kListCap * 4));
+    l.total = align16(l.list + (size_t)kListCap * 4);
     return l;
 }
 
@@ -70,7 +69,7 @@ __device__ __forceinline__ void pair_match(uint32_t quad, uint32_t ta4, uint32_t
     ma = hit ^ mb;
 }
 
-__global__ void __launch_bounds__(kCvThreads, 3) cvalues_kernel(const __grid_constant__ CvBatch b)
+__global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_constant__ CvBatch b)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t occ[32], srv[32], rel[32], needbits[32];
@@ -145,7 +144,6 @@ __global__ void __launch_bounds__(kCvThreads, 3) cvalues_kernel(const __grid_con
     uint16_t *rcode = (uint16_t *)(smem + L.rcode);      // rank -> code
     uint32_t *nbr = (uint32_t *)(smem + L.nbr);          // rank -> neighbour rank offsets
     uint16_t *relneed = (uint16_t *)(smem + L.relneed);  // rank -> ranks read (bit 4: itself); 0: not served
-    uint16_t *codes = (uint16_t *)(smem + L.codes);      // [RH][S]: element e of row r is pixel (xs + e, y0 - P + r)
     uint32_t *wcount = (uint32_t *)(smem + L.wcount);    // [chunk row][rank pair][column] packed window counts
     uint32_t *prefix = (uint32_t *)(smem + L.prefix);    // per-warp prefix rows
     float *blist = (float *)(smem + L.list);
@@ -153,35 +151,34 @@ __global__ void __launch_bounds__(kCvThreads, 3) cvalues_kernel(const __grid_con
     if (tid == 0) list_n = 0;
     __syncthreads();
 
-    // 2. stage the region, 8 elements per thread and step
+    // the band codes of region row r, pixels xs + 8 v .. + 7 (16-byte loads where the row allows)
+    auto load8 = [&](int r, int v, uint16_t (&cs)[8]) {
+        const int y = y0 - P + r, xv = xs + 8 * v;
+        if (vec && y >= 0 && y < h && xv >= 0 && xv + 8 <= w) {
+            const uint4 q = __ldg((const uint4 *)(J.word + (size_t)y * w + xv));
+            cs[0] = code_of(q.x & 0xFFFFu, bd);
+            cs[1] = code_of(q.x >> 16, bd);
+            cs[2] = code_of(q.y & 0xFFFFu, bd);
+            cs[3] = code_of(q.y >> 16, bd);
+            cs[4] = code_of(q.z & 0xFFFFu, bd);
+            cs[5] = code_of(q.z >> 16, bd);
+            cs[6] = code_of(q.w & 0xFFFFu, bd);
+            cs[7] = code_of(q.w >> 16, bd);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int x = xv + k;
+                cs[k] = (y >= 0 && y < h && x >= 0 && x < w) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
+            }
+        }
+    };
+    // 2. the codes the region holds (occ) and the codes own pixels need (srv), 8 elements per thread and step
     {
         const int nv = S >> 3, total = RH * nv;
         for (int i = tid; i < total; i += kCvThreads) {
-            const int r = i / nv, v = i - r * nv, y = y0 - P + r, xv = xs + 8 * v;
+            const int r = i / nv, v = i - r * nv, xv = xs + 8 * v;
             uint16_t cs[8];
-            if (vec && y >= 0 && y < h && xv >= 0 && xv + 8 <= w) {
-                const uint4 q = __ldg((const uint4 *)(J.word + (size_t)y * w + xv));
-                cs[0] = code_of(q.x & 0xFFFFu, bd);
-                cs[1] = code_of(q.x >> 16, bd);
-                cs[2] = code_of(q.y & 0xFFFFu, bd);
-                cs[3] = code_of(q.y >> 16, bd);
-                cs[4] = code_of(q.z & 0xFFFFu, bd);
-                cs[5] = code_of(q.z >> 16, bd);
-                cs[6] = code_of(q.w & 0xFFFFu, bd);
-                cs[7] = code_of(q.w >> 16, bd);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int x = xv + k;
-                    cs[k] = (y >= 0 && y < h && x >= 0 && x < w) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
-                }
-            }
-            uint4 st;
-            st.x = cs[0] | ((unsigned)cs[1] << 16);
-            st.y = cs[2] | ((unsigned)cs[3] << 16);
-            st.z = cs[4] | ((unsigned)cs[5] << 16);
-            st.w = cs[6] | ((unsigned)cs[7] << 16);
-            *(uint4 *)(codes + r * S + 8 * v) = st;
+            load8(r, v, cs);
             const bool row_in_tile = r >= P && r < P + rows;
             uint16_t prev = kNone, prev_srv = kNone;
 #pragma unroll
@@ -254,34 +251,28 @@ __global__ void __launch_bounds__(kCvThreads, 3) cvalues_kernel(const __grid_con
     }
     // the rank plane: absolute ranks once for the tile when they fit in a byte, else per pass relative to the pass
     const bool per_pass = R > kMaxPlaneRank + 1;
-    auto build_plane = [&](int b0) {  // b0 < 0: absolute ranks from the staged codes; else pass ranks from the words
-        for (int i = tid; i < RH * (CS / 4); i += kCvThreads) {
-            const int r = i / (CS / 4), j0 = 4 * (i - r * (CS / 4));
-            uint32_t quad = 0;
+    auto build_plane = [&](int b0) {  // b0 < 0: absolute ranks; else ranks of the pass from b0 (others: no rank)
+        for (int i = tid; i < RH * CS / 16; i += kCvThreads) ((uint4 *)rplane)[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        __syncthreads();
+        const int nv = S >> 3, total = RH * nv;
+        for (int i = tid; i < total; i += kCvThreads) {
+            const int r = i / nv, v = i - r * nv;
+            uint16_t cs[8];
+            load8(r, v, cs);
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int jj = j0 + k;
-                unsigned v = kNoRank;
-                if (jj < RW) {
-                    uint16_t code;
-                    if (b0 < 0) {
-                        code = codes[r * S + jj + ox];
-                    } else {
-                        const int x = x0 - P + jj, y = y0 - P + r;
-                        code = (x >= 0 && x < w && y >= 0 && y < h) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
-                    }
-                    if (code != kNone && rank[code] != kNone) {
-                        const int rk = rank[code] - (b0 < 0 ? 0 : b0);
-                        if (b0 < 0 || (rk >= 0 && rk < kCvBins)) v = (unsigned)rk;
-                    }
-                }
-                quad |= v << (8 * k);
+            for (int k = 0; k < 8; k++) {
+                const int j = 8 * v + k - ox;  // region column
+                if (j < 0 || j >= RW || cs[k] == kNone) continue;
+                const int rk0 = rank[cs[k]];
+                if (rk0 == kNone) continue;
+                const int rk = b0 < 0 ? rk0 : rk0 - b0;
+                if (b0 >= 0 && (rk < 0 || rk >= kCvBins)) continue;
+                rplane[r * CS + j] = (uint8_t)rk;
             }
-            *(uint32_t *)(rplane + r * CS + j0) = quad;
         }
     };
     if (!per_pass) build_plane(-1);
-    __syncthreads();  // the staged codes are dead from here: their space holds the pass buffers
+    __syncthreads();
 
     unsigned long long my_sum = 0;
     unsigned my_cnt = 0;
