@@ -102,3 +102,38 @@ def test_window_figures_against_the_reference_and_fp64(cuda, ref):
     # the product rounds each figure once; the reference's FP32 sums differ by more, but stay close
     assert mine_err.max() <= 2 ** -24
     assert ref_err.max() < 1e-3
+
+
+def test_b200_cambi_is_faster_than_the_reference_kernels(cuda, module, ref):
+    """The four 3840x2160 10-bit pictures of a c2 frame step scored by the reference's own Cambi class (its kernels
+    compiled unmodified for sm_100a) and by es_cambi, each after a warm-up launch: scores equal to 1e-9 relative, and
+    each picture scored faster here (wall time of launch + finish, which is what a caller waits for). Prints both."""
+    import time
+
+    import es_synth
+
+    step = es_synth.c2_step(0)
+    pics = [step.source] + list(step.encodes)
+    stream = cuda.cuda.current_stream().cuda_stream
+    rows = []
+    c = es_b200.Cambi(module, 3840, 2160, 10)
+    for i, pic in enumerate(pics):
+        t = to_dev(cuda, pic.y)
+        ref.cambi_score(t.data_ptr(), 3840, 2160, 10)  # warm-up
+        t0 = time.perf_counter()
+        want = ref.cambi_score(t.data_ptr(), 3840, 2160, 10)
+        t_ref = time.perf_counter() - t0
+        c.launch(t.data_ptr(), 3840, stream)
+        c.finish()
+        cuda.cuda.synchronize()
+        t0 = time.perf_counter()
+        c.launch(t.data_ptr(), 3840, stream)
+        got = c.finish()
+        t_b200 = time.perf_counter() - t0
+        rows.append((i, want, got, 1000 * t_ref, 1000 * t_b200))
+        assert abs(got - want) <= 1e-9 * max(abs(want), 1e-12), (i, got, want)
+    c.close()
+    print("\npicture  CAMBI (reference)  CAMBI (b200)  reference ms  b200 ms")
+    for r in rows:
+        print(f"{r[0]:7d}  {r[1]:17.9f}  {r[2]:12.9f}  {r[3]:12.3f}  {r[4]:7.3f}")
+    assert all(r[4] < r[3] for r in rows)
