@@ -371,6 +371,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only-head", action="store_true", help="time only the headline form (for profiling runs)")
+    ap.add_argument("--budget", type=float, default=None, help="learned form: score budget of skipped tiles (default: the network's)")
+    ap.add_argument("--tolerance", type=float, default=None, help="learned form: audit tolerance (default: the network's)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -454,15 +456,19 @@ def main() -> None:
             self.b.close()
 
     class LearnedForm(BatchedForm):
-        name = ("batched + learned proposal (es_batch with es_batch_set_proposal: c-values of scales 0-1 on the network's "
-                "proposed tiles plus a 5%/20% audit, fallback to every tile above an estimated 0.025 change of CAMBI)")
-
         def __init__(self):
             super().__init__()
             import eval_proposal
             self.net, meta = eval_proposal.load_net(es_b200)
             self.threshold = meta["threshold"]
-            self.b.set_proposal(self.net, threshold=self.threshold)
+            self.budget = meta.get("budget", 0.0) if args.budget is None else args.budget
+            self.tolerance = meta.get("tolerance", 0.025) if args.tolerance is None else args.tolerance
+            self.b.set_proposal(self.net, threshold=self.threshold, tolerance=self.tolerance, budget=self.budget)
+            skip = (f"tiles predicted below {self.threshold:g}" +
+                    (f" or, per picture, predicted to add at most {self.budget:g} to CAMBI" if self.budget else ""))
+            self.name = ("batched + learned proposal (es_batch with es_batch_set_proposal: c-values of scales 0-1 skip the "
+                         f"{skip}, except a 5%/20% audit; fallback to every tile above an estimated {self.tolerance:g} "
+                         "change of CAMBI)")
 
         def close(self):
             super().close()
@@ -523,7 +529,8 @@ def main() -> None:
         ms_l, launches_l, clk, _ = time_form(learned, 0)
         learned.close()
         forms["learned"] = {"value": pairs / (ms_l / 1000.0), "ms_per_step": ms_l / args.steps, "form": learned.name,
-                            "gpu_launches": int(launches_l), "threshold": learned.threshold}
+                            "gpu_launches": int(launches_l), "threshold": learned.threshold, "budget": learned.budget,
+                            "tolerance": learned.tolerance}
         head = "learned"
         ms, launches = ms_l, launches_l
     value = forms[head]["value"]

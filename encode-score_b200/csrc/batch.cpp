@@ -98,6 +98,7 @@ struct es_batch {
     DeviceBuffer<unsigned> counters;         // count_a, count_b, next_a, next_b, n_audit[kMaxJobs], n_skip[kMaxJobs]
     DeviceBuffer<unsigned long long> tile_mass, frame;
     DeviceBuffer<int> run_flags;
+    DeviceBuffer<float> pic_threshold;       // per picture, budget mode
     DeviceBuffer<ProposalStats> stats;
     PinnedBuffer<ProposalStats> h_stats[2];
     PinnedBuffer<unsigned long long> h_frame[2];
@@ -242,6 +243,27 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
     pb.frags = b.net_frags;
     pb.pred = b.pred.ptr;
     cuda_check(launch_predict(pb, s), "tile predictions");
+    const bool budget = b.popt.budget > 0;
+    if (budget) {
+        BudgetBatch bb{};
+        for (int r = 0; r < np; r++) {
+            const Picture &pic = *b.pictures[run[r]];
+            BudgetJob &j = bb.job[bb.njobs++];
+            j.pred_first = pb.job[r].first_tile;
+            j.tiles_x = pb.job[r].tiles_x;
+            j.tiles_y = pb.job[r].tiles_y;
+            j.w = pic.w;
+            j.h = pic.h;
+            j.picture = run[r];
+            const double k0 = (double)topk_count((unsigned long long)pic.sw[0] * pic.sh[0], pic.p.topk);
+            j.scale = 16.0 / (k0 * (double)pic.p.window * (double)pic.p.window);
+        }
+        bb.pred = b.pred.ptr;
+        bb.threshold = b.popt.threshold;
+        bb.budget = b.popt.budget;
+        bb.pic_threshold = b.pic_threshold.ptr;
+        cuda_check(launch_budget(bb, s), "tile budget");
+    }
     ProposeBatch qb{};
     AuditBatch ab{};
     for (int r = 0; r < np; r++) {
@@ -272,6 +294,7 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
     qb.total_tiles = cb.total_tiles;
     qb.pred = b.pred.ptr;
     qb.threshold = b.popt.threshold;
+    qb.pic_threshold = budget ? b.pic_threshold.ptr : nullptr;
     qb.audit_permille[0] = (unsigned)b.popt.audit_permille[0];
     qb.audit_permille[1] = (unsigned)b.popt.audit_permille[1];
     qb.frame = b.frame.ptr;
@@ -747,6 +770,7 @@ int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_o
         require(o.audit_permille[0] >= 0 && o.audit_permille[0] <= 1000 && o.audit_permille[1] >= 0 && o.audit_permille[1] <= 1000,
                 "es_batch_set_proposal: audit rates are per mille, 0 to 1000");
         require(o.tolerance >= 0, "es_batch_set_proposal: tolerance must be >= 0");
+        require(o.budget >= 0, "es_batch_set_proposal: budget must be >= 0");
         cuda_check(cudaStreamSynchronize(b->main.s), "es_batch_set_proposal");
         for (auto &g : b->graphs) cudaGraphExecDestroy(g.second.exec);  // captured steps belong to the old setting
         b->graphs.clear();
@@ -784,6 +808,7 @@ int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_o
             b->tile_mass.reset(tiles);
             b->frame.reset(1);
             b->run_flags.reset(P);
+            b->pic_threshold.reset(P);
             b->stats.reset(P);
             for (int i = 0; i < 2; i++) {
                 b->h_stats[i].reset(P);

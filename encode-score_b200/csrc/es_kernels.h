@@ -319,6 +319,7 @@ struct ProposeBatch {
     int njobs, total_tiles;
     const float *pred;
     float threshold;
+    const float *pic_threshold;           // per picture (budget mode), else null: threshold for all
     unsigned audit_permille[2];           // per scale 0, 1
     const unsigned long long *frame;      // device: the step's frame number (seeds the audit sample)
     unsigned *list_a, *count_a;           // tiles to run now
@@ -327,6 +328,23 @@ struct ProposeBatch {
     unsigned *n_audit, *n_skip;           // per job (zeroed before the launch, with the counts)
 };
 cudaError_t launch_propose(const ProposeBatch &b, cudaStream_t s);
+// Budget mode: per picture, the skip threshold T >= `threshold` of the predictions such that the predicted score
+// contribution of the scale-0 tiles below T, sum of scale * expm1(pred) * pixels, stays within `budget`.
+constexpr int kBudgetBins = 1024;
+constexpr float kBudgetBinsPerUnit = 128.0f;  // bins cover predictions 0 .. 8
+struct BudgetJob {
+    int pred_first, tiles_x, tiles_y, w, h, picture;
+    double scale;  // score per unit of scale-0 c-value mass: 16 / (k0 window^2)
+};
+struct BudgetBatch {
+    BudgetJob job[kMaxPictures];
+    int njobs;
+    const float *pred;
+    float threshold;
+    double budget;
+    float *pic_threshold;  // out, by picture
+};
+cudaError_t launch_budget(const BudgetBatch &b, cudaStream_t s);
 struct AuditJob {
     int job[2];         // the picture's scale-0 and scale-1 jobs in the propose table
     int first_tile[2];  // their global tile ranges

@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(256) propose_kernel(const __grid_constant__ Pr
                     best = fmaxf(best, b.pred[J.pred_first + y * J.pred_tiles_x + x]);
             if (best == -INFINITY) {
                 kind = kTileEmpty;  // scale 0: nothing to compute; scale 1: left to the fallback, unaudited
-            } else if (best < b.threshold) {
+            } else if (best < (b.pic_threshold ? b.pic_threshold[J.picture] : b.threshold)) {
                 const unsigned long long hsh = mix64(frame * 0x100000001B3ull ^ ((unsigned long long)J.picture << 40) ^
                                                      ((unsigned long long)s << 36) ^ (unsigned long long)tile);
                 kind = (unsigned)(hsh % 1000ull) < b.audit_permille[s] ? kTileAudit : kTileSkip;
@@ -465,6 +465,58 @@ __global__ void __launch_bounds__(256) propose_kernel(const __grid_constant__ Pr
         b.kind[gt] = kind;
         if (kind == kTileRun || kind == kTileAudit) b.list_a[atomicAdd(b.count_a, 1u)] = (unsigned)gt;
         else if (kind == kTileSkip || (kind == kTileEmpty && J.scale == 1)) b.list_b[atomicAdd(b.count_b, 1u)] = (unsigned)gt;
+    }
+}
+
+// One block per picture: the largest skip threshold whose skipped scale-0 tiles are predicted to change the score by
+// at most the budget. Predicted contributions are binned by prediction (kBudgetBinsPerUnit bins per unit from 0, the
+// last bin open above) in fixed point (2^-40 of a score point), so the result does not depend on the order of adds.
+__global__ void __launch_bounds__(kBudgetBins) budget_kernel(const __grid_constant__ BudgetBatch b)
+{
+    __shared__ unsigned long long bins[kBudgetBins];
+    __shared__ unsigned long long warp_sums[kBudgetBins / 32];
+    const BudgetJob &J = b.job[blockIdx.x];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    bins[tid] = 0;
+    __syncthreads();
+    const int tiles = J.tiles_x * J.tiles_y;
+    for (int t = tid; t < tiles; t += kBudgetBins) {
+        const float p = b.pred[J.pred_first + t];
+        if (p == -INFINITY) continue;  // nothing to compute in the tile
+        const int tx = t % J.tiles_x, ty = t / J.tiles_x;
+        const int px = min(kCvTX, J.w - tx * kCvTX) * min(kCvTY, J.h - ty * kCvTY);
+        const double c = J.scale * expm1((double)fmaxf(p, 0.0f)) * (double)px;
+        const double fx = fmin(c * 1099511627776.0, 2.0e15);  // 2^40 units; 8192 tiles at the cap stay below 2^64
+        const int bin = min(kBudgetBins - 1, max(0, (int)(p * kBudgetBinsPerUnit)));
+        atomicAdd(&bins[bin], (unsigned long long)fx);
+    }
+    __syncthreads();
+    // inclusive prefix over the bins: bin `tid` in thread tid
+    unsigned long long v = bins[tid];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long u = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_sums[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long w = warp_sums[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long u = __shfl_up_sync(kFull, w, o);
+            if (lane >= o) w += u;
+        }
+        warp_sums[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const unsigned long long incl = v + (warp ? warp_sums[warp - 1] : 0ull);
+    const unsigned long long budget = (unsigned long long)fmin(b.budget * 1099511627776.0, 1.8e19);
+    // bins 0 .. n - 1 fit the budget; the threshold is the lower edge of bin n
+    const int n = __syncthreads_count(incl <= budget);
+    if (tid == 0) {
+        const float t = n >= kBudgetBins ? INFINITY : (float)n / kBudgetBinsPerUnit;
+        b.pic_threshold[J.picture] = fmaxf(t, b.threshold);
     }
 }
 
@@ -647,6 +699,14 @@ cudaError_t launch_propose(const ProposeBatch &b, cudaStream_t s)
     if (b.total_tiles <= 0) return cudaSuccess;
     LaunchTimer t("proposal_lists", s);
     propose_kernel<<<(b.total_tiles + 255) / 256, 256, 0, s>>>(b);
+    return after_launch();
+}
+
+cudaError_t launch_budget(const BudgetBatch &b, cudaStream_t s)
+{
+    if (b.njobs <= 0) return cudaSuccess;
+    LaunchTimer t("proposal_budget", s);
+    budget_kernel<<<b.njobs, kBudgetBins, 0, s>>>(b);
     return after_launch();
 }
 

@@ -96,7 +96,8 @@ class BatchSource(ctypes.Structure):
 
 
 class ProposalOptions(ctypes.Structure):
-    _fields_ = [("threshold", ctypes.c_float), ("audit_permille", ctypes.c_int * 2), ("tolerance", ctypes.c_double)]
+    _fields_ = [("threshold", ctypes.c_float), ("audit_permille", ctypes.c_int * 2), ("tolerance", ctypes.c_double),
+                ("budget", ctypes.c_double)]
 
 
 class ProposalStats(ctypes.Structure):
@@ -555,9 +556,10 @@ class Batch:
         check(lib().es_batch_scale_pooled(self.handle, picture, out))
         return list(out)
 
-    def set_proposal(self, net, threshold: float = 0.05, audit=(50, 200), tolerance: float = 0.025) -> None:
-        """Switches the learned tile proposal on (net: ProposalNet) or off (net None)."""
-        opt = ProposalOptions(threshold, (ctypes.c_int * 2)(*audit), tolerance)
+    def set_proposal(self, net, threshold: float = 0.05, audit=(50, 200), tolerance: float = 0.025, budget: float = 0.0) -> None:
+        """Switches the learned tile proposal on (net: ProposalNet) or off (net None); budget > 0 also skips, per
+        picture, the lowest-predicted scale-0 tiles while their predicted contribution to the score stays within it."""
+        opt = ProposalOptions(threshold, (ctypes.c_int * 2)(*audit), tolerance, budget)
         check(lib().es_batch_set_proposal(self.handle, net.handle if net is not None else None, ctypes.byref(opt)))
 
     def proposal_stats(self, picture: int) -> dict:

@@ -40,13 +40,14 @@ def planar(torch, es_b200, y):
     return view, (y, u, v)
 
 
-def run(torch, es_b200, module, frames: int, seed: int, net, threshold: float, audit=(50, 200), tolerance: float = 0.025):
+def run(torch, es_b200, module, frames: int, seed: int, net, threshold: float, audit=(50, 200), tolerance: float = 0.025,
+        budget: float = 0.0):
     """Scores `frames` frame pairs with the exact and the proposal form; returns per-picture rows and timings."""
     import es_synth_gpu
 
     exact = es_b200.Batch(module, [(W, H, 10, 1)])
     prop = es_b200.Batch(module, [(W, H, 10, 1)])
-    prop.set_proposal(net, threshold=threshold, audit=audit, tolerance=tolerance)
+    prop.set_proposal(net, threshold=threshold, audit=audit, tolerance=tolerance, budget=budget)
     stream = torch.cuda.current_stream().cuda_stream
     rows = []
     t_exact = t_prop = 0.0
@@ -104,6 +105,9 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=90_000_000)
     ap.add_argument("--net", default=None)
     ap.add_argument("--untrained", action="store_true", help="also run a He-initialised network at the same threshold")
+    ap.add_argument("--budget", type=float, default=None, help="score budget of the skipped tiles (default: the network's)")
+    ap.add_argument("--tolerance", type=float, default=0.025)
+    ap.add_argument("--sweep", default=None, help="budget,tolerance pairs 'b:t,b:t,...' to evaluate instead of one setting")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
 
@@ -115,11 +119,30 @@ def main() -> None:
     module = es_b200.Module()
     net, meta = load_net(es_b200, args.net)
     t0 = time.time()
-    rows, timing = run(torch, es_b200, module, args.frames, args.seed, net, meta["threshold"])
-    out = {"threshold": meta["threshold"], "trained": summarize(rows, timing), "seconds": time.time() - t0}
+    budget = meta.get("budget", 0.0) if args.budget is None else args.budget
+    if args.sweep:
+        out = {"threshold": meta["threshold"], "sweep": []}
+        for item in args.sweep.split(","):
+            b, t = (float(v) for v in item.split(":"))
+            rows, timing = run(torch, es_b200, module, args.frames, args.seed, net, meta["threshold"], tolerance=t, budget=b)
+            out["sweep"].append({"budget": b, "tolerance": t, **summarize(rows, timing)})
+            print(json.dumps(out["sweep"][-1]), flush=True)
+        out["seconds"] = time.time() - t0
+        net.close()
+        module.close()
+        text = json.dumps(out, indent=1)
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(text)
+        return
+    rows, timing = run(torch, es_b200, module, args.frames, args.seed, net, meta["threshold"], tolerance=args.tolerance,
+                       budget=budget)
+    out = {"threshold": meta["threshold"], "budget": budget, "tolerance": args.tolerance, "trained": summarize(rows, timing),
+           "seconds": time.time() - t0}
     if args.untrained:
         raw = es_b200.ProposalNet(seed=12345)
-        rows_u, timing_u = run(torch, es_b200, module, args.frames, args.seed, raw, meta["threshold"])
+        rows_u, timing_u = run(torch, es_b200, module, args.frames, args.seed, raw, meta["threshold"], tolerance=args.tolerance,
+                               budget=budget)
         out["untrained"] = summarize(rows_u, timing_u)
         raw.close()
     net.close()

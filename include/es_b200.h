@@ -314,11 +314,14 @@ int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5]);
  * above `tolerance` the skipped tiles run too (the fallback), so the score is then exact. Scale-0 tiles with no pixel
  * that needs a c-value are skipped in every mode (they add nothing). net NULL switches the proposal off. The network
  * must stay alive while the batch uses it; after training it further, call this again. Every queued step must have
- * been collected. options NULL = {threshold 0.05, audit 50 and 200 per mille, tolerance 0.025}. */
+ * been collected. options NULL = {threshold 0.05, audit 50 and 200 per mille, tolerance 0.025, no budget}. */
 typedef struct {
     float threshold;       /* in the network's label space, log1p(mean c-value of the tile) */
     int audit_permille[2]; /* scales 0 and 1 */
     double tolerance;      /* estimated change of the score above which the fallback runs */
+    double budget;         /* > 0: per picture, also skip the scale-0 tiles of lowest prediction while their predicted
+                              contribution to the score, 16 expm1(prediction) pixels / (k window^2) summed, stays
+                              within this budget (the threshold becomes a floor); 0: the threshold alone */
 } es_proposal_options;
 int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_options *options);
 typedef struct {

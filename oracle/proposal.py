@@ -18,6 +18,8 @@ Only tests and the training script import this module.
 
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 CHANNELS = (2, 16, 16, 16, 1)
@@ -194,3 +196,36 @@ class Adam:
 def label_of(mass_fx: np.ndarray, pixels: np.ndarray) -> np.ndarray:
     """Tile label log1p(sum of the tile's positive c-values / its pixel count), from the exact sum in 2^-24 units."""
     return np.log1p(mass_fx.astype(np.float64) / 16777216.0 / np.maximum(pixels, 1))
+
+
+def budget_threshold(pred: np.ndarray, w: int, h: int, k0: int, window: int, threshold: float, budget: float,
+                     tile: int = 64, bins: int = 1024, per_unit: float = 128.0) -> float:
+    """The budget mode's skip threshold of one picture (test restatement of the device's): scale-0 tile t of predicted
+    label p_t (row-major over ceil(w / tile) x ceil(h / tile) tiles, -inf where nothing needs a c-value) is predicted to
+    add scale * expm1(max(p_t, 0)) * pixels_t to the score, scale = 16 / (k0 window^2); contributions are binned by
+    prediction (per_unit bins per unit from 0, the last bin open above) in 2^-40 fixed point, and the threshold is the
+    lower edge of the first bin whose inclusion would exceed the budget (infinity when none does), at least
+    `threshold`."""
+    tx = (w + tile - 1) // tile
+    ty = (h + tile - 1) // tile
+    scale = 16.0 / (k0 * window * window)
+    acc = [0] * bins
+    p = np.asarray(pred, np.float32).reshape(ty, tx)
+    for y in range(ty):
+        for x in range(tx):
+            v = float(p[y, x])
+            if v == -np.inf:
+                continue
+            px = min(tile, w - x * tile) * min(tile, h - y * tile)
+            c = scale * math.expm1(max(v, 0.0)) * px
+            fx = int(min(c * 2.0 ** 40, 2.0e15))
+            b = min(bins - 1, max(0, int(np.float32(v) * np.float32(per_unit))))
+            acc[b] += fx
+    limit = int(min(budget * 2.0 ** 40, 1.8e19))
+    n, incl = 0, 0
+    for b in range(bins):
+        incl += acc[b]
+        if incl <= limit:
+            n += 1
+    t = np.inf if n >= bins else n / per_unit
+    return float(max(np.float32(t), np.float32(threshold)))

@@ -51,9 +51,9 @@ def run_plain(cuda, module, steps, source_cambi=None):
     return out, accs
 
 
-def run_batch(cuda, module, steps, use_graphs=True, source_cambi=None):
+def run_batch(cuda, module, steps, use_graphs=True, source_cambi=None, tuning=None):
     stream = cuda.cuda.current_stream().cuda_stream
-    b = es_b200.Batch(module, SOURCES, use_graphs=use_graphs)
+    b = es_b200.Batch(module, SOURCES, use_graphs=use_graphs, tuning=tuning)
     accs = [es_b200.new_accum() for _ in range(b.n_encodes)]
     per_source = [([], []) for _ in SOURCES]
     for f in range(FRAMES):
@@ -117,6 +117,14 @@ def test_batch_without_graphs_equals_with(cuda, module, steps):
     for s in range(len(SOURCES)):
         assert a[s][0] == b[s][0]
     assert [accum_bytes(x) for x in aacc] == [accum_bytes(x) for x in bacc]
+
+
+def test_short_cvalue_tiles_equal_the_plain_step(cuda, module, steps):
+    """The autotuner's shorter c-value tiles (16 or 32 rows at some scales) give the same results as the plain step."""
+    plain, pacc = run_plain(cuda, module, steps)
+    tuning = {(w, h): rows for (w, h, _, _), rows in zip(SOURCES, ([16, 32, 16, 32, 16], [32, 16, 64, 16, 32], [16, 16, 32, 64, 16]))}
+    batch, bacc, _ = run_batch(cuda, module, steps, tuning=tuning)
+    compare(plain, pacc, batch, bacc)
 
 
 def test_batch_skipped_source_cambi_uses_the_cached_value(cuda, module, steps):

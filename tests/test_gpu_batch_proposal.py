@@ -8,7 +8,7 @@ import pytest
 
 import es_b200
 import es_synth
-from gpu_util import step_to_dev
+from gpu_util import step_to_dev, to_dev
 
 pytestmark = pytest.mark.gpu
 
@@ -93,3 +93,49 @@ def test_fallback_restores_the_exact_scores(cuda, module, steps, exact, net):
             if s["audited"][0] + s["audited"][1] and s["estimate"] > 0:
                 assert s["fallback"] == 1
     assert fell > 0
+
+
+def test_budget_skips_the_tiles_the_oracle_picks(cuda, module, steps, exact, net):
+    """Budget mode with every skip candidate audited: per picture, the scale-0 tiles audited are exactly those whose
+    prediction (es_proposal_predict on the same picture's scale-0 words) lies below the oracle's budget threshold, the
+    others run, and the scores stay exact (audited tiles run too); the candidates grow with the budget."""
+    import proposal as op
+
+    torch = cuda
+    stream = torch.cuda.current_stream().cuda_stream
+    frames = (0, FRAMES - 1)
+    preds = {}
+    for f in frames:
+        pic = 0
+        for s, (w, h, pd, n) in enumerate(SOURCES):
+            for plane in [steps[f][s].source] + list(steps[f][s].encodes):
+                cam = es_b200.Cambi(module, w, h, pd)
+                y = to_dev(torch, plane.y)
+                cam.launch(y.data_ptr(), w, stream)
+                cam.finish()
+                p = torch.empty(((w + 63) // 64) * ((h + 63) // 64), dtype=torch.float32, device="cuda")
+                net.predict(cam.scale_words(0), w, h, p.data_ptr(), stream)
+                torch.cuda.synchronize()
+                window = es_b200.derive_params(w, h).window
+                k0 = max(1, min(w * h, int(0.6 * w * h)))
+                preds[(f, pic)] = (p.cpu().numpy(), w, h, k0, window)
+                cam.close()
+                pic += 1
+    last = None
+    for budget in (1e-9, 1e-6, 1e-4, 1e30):
+        got = run(cuda, module, steps, net, threshold=-1e30, audit=(1000, 1000), tolerance=1e30, budget=budget)
+        audited = []
+        for f in frames:
+            (r, p, st), (re, pe, _) = got[f], exact[f]
+            assert r == re and p == pe
+            for pic, s in enumerate(st):
+                pr, w, h, k0, window = preds[(f, pic)]
+                t = op.budget_threshold(pr, w, h, k0, window, -1e30, budget)
+                finite = pr[pr != -np.inf]
+                assert s["audited"][0] == int((finite < t).sum()), (budget, f, pic, s, t)
+                assert s["run"][0] == int((finite >= t).sum()), (budget, f, pic, s, t)
+                audited.append(s["audited"][0])
+        if last is not None:
+            assert all(a >= b for a, b in zip(audited, last))
+        last = audited
+    assert all(s["run"][0] == 0 for s in got[frames[-1]][2])

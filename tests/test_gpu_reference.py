@@ -137,3 +137,72 @@ def test_b200_cambi_is_faster_than_the_reference_kernels(cuda, module, ref):
     for r in rows:
         print(f"{r[0]:7d}  {r[1]:17.9f}  {r[2]:12.9f}  {r[3]:12.3f}  {r[4]:7.3f}")
     assert all(r[4] < r[3] for r in rows)
+
+
+def test_texture_kernels_at_4k_against_the_reference(cuda, module, ref):
+    """A 3840x2160 10-bit c2 frame step (1 source, 3 encodes; every frame the same step, so the 13-frame texture
+    window holds one picture) through the reference's window_stats, persist_stats, plane_sse and color_sums (compiled
+    unmodified for sm_100a, launched as src/main.cpp:540-566 launches them) and through es_frame: the reference's FP32
+    window and lasting figures within 1e-3 (of each figure's largest value) of the product's exact ones. Prints each
+    group's device time per frame step: the reference's launches bracketed by CUDA events one by one, the product's
+    kernels timed one by one by es_kernel_timing."""
+    torch = cuda
+    W, H, E = 3840, 2160, 3
+    step = es_synth.c2_step(0, n_encodes=E)
+    keep, views = es_b200.device_step(torch, step)
+    stream = torch.cuda.current_stream().cuda_stream
+    fr = es_b200.Frame(module, W, H, 10, E)
+    acc = [es_b200.new_accum() for _ in range(E)]
+    for f in range(16):
+        fr.queue(f, views[0], views[1:], stream)
+        fr.collect(f, acc, acc)
+    es_b200.kernel_timing(True, serial=True)
+    for f in range(16, 18):
+        fr.queue(f, views[0], views[1:], stream)
+        fr.collect(f, acc, acc)
+    times = es_b200.kernel_times()
+    es_b200.kernel_timing(False)
+    mine = [fr.read_windows(e, persist=True) for e in range(E)]
+    fr.close()
+    ours = {k: times[k][0] / 2 for k in ("window_stats", "persist_stats", "pair_sums", "frame_unpack") if k in times}
+
+    ys = to_dev(torch, step.source.y)
+    us, vs = to_dev(torch, step.source.u), to_dev(torch, step.source.v)
+    ring = torch.zeros((13, H, W), dtype=torch.float32, device="cuda")
+    ws = (W // 16) * (H // 16)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ref_ms = {"window_stats": 0.0, "persist_stats": 0.0, "plane_sse + color_sums": 0.0}
+
+    def timed(group, call):
+        ev[0].record()
+        call()
+        ev[1].record()
+        torch.cuda.synchronize()
+        ref_ms[group] += ev[0].elapsed_time(ev[1])
+
+    sse = zeros_dev(torch, (3,), np.float64)
+    sums = zeros_dev(torch, (3,), np.float64)
+    n = W * H
+    timed("plane_sse + color_sums", lambda: ref.color_sums(us.data_ptr(), vs.data_ptr(), n // 4, 0, sums.data_ptr()))
+    for e in range(E):
+        enc = step.encodes[e]
+        ye, ue, ve = to_dev(torch, enc.y), to_dev(torch, enc.u), to_dev(torch, enc.v)
+        mid_d = torch.zeros((H, W), dtype=torch.float32, device="cuda")
+        st = zeros_dev(torch, (ws, 8), np.float32)
+        ps = zeros_dev(torch, (ws, 5), np.float32)
+        ref.window_stats(ys.data_ptr(), ye.data_ptr(), 0, W, H, ring[0].data_ptr(), mid_d.data_ptr(), st.data_ptr())  # warm-up
+        timed("window_stats", lambda: ref.window_stats(ys.data_ptr(), ye.data_ptr(), 0, W, H, ring[0].data_ptr(),
+                                                       mid_d.data_ptr(), st.data_ptr()))
+        ring[1:].copy_(ring[0].expand(12, H, W))
+        timed("persist_stats", lambda: ref.persist_stats(ring.data_ptr(), n, 6, mid_d.data_ptr(), W, H, ps.data_ptr()))
+        for a, b, m in ((ys, ye, n), (us, ue, n // 4), (vs, ve, n // 4)):
+            timed("plane_sse + color_sums", lambda: ref.plane_sse(a.data_ptr(), b.data_ptr(), m, sse.data_ptr()))
+        timed("plane_sse + color_sums", lambda: ref.color_sums(ue.data_ptr(), ve.data_ptr(), n // 4, 0, sums.data_ptr()))
+        for got, want in ((from_dev(st, np.float32), mine[e][0]), (from_dev(ps, np.float32), mine[e][1])):
+            scale = np.abs(want.astype(np.float64)).max(axis=0) + 1e-30
+            err = np.abs(got.astype(np.float64) - want.astype(np.float64)) / scale
+            assert err.max() < 1e-3, (e, err.max(axis=0))
+    print("\nper 4K10 frame step (1 source, 3 encodes)   reference ms   b200 ms")
+    print(f"window figures                               {ref_ms['window_stats']:12.3f}   {ours.get('window_stats', 0):7.3f}")
+    print(f"lasting texture                              {ref_ms['persist_stats']:12.3f}   {ours.get('persist_stats', 0):7.3f}")
+    print(f"PSNR squared errors + color                  {ref_ms['plane_sse + color_sums']:12.3f}   {ours.get('pair_sums', 0):7.3f}")

@@ -81,3 +81,21 @@ def test_training_lowers_the_loss():
         _, g = proposal.loss_and_grads(x, labels, params)
         params = opt.step(params, g)
     assert proposal.loss_and_grads(x, labels, params)[0] < 0.5 * l0
+
+
+def test_budget_threshold_known_answers():
+    """Two scale-0 tiles of a 128 x 64 picture predicted at 0.5 and 2.0: a budget below the first tile's predicted
+    contribution stops at the first tile's bin (0.5), one between the first and both stops at the second's (2.0), one
+    above both skips everything (infinity); the threshold is a floor throughout, and tiles without a prediction add
+    nothing."""
+    import math
+
+    w, h, k0, window = 128, 64, 4915, 9
+    scale = 16.0 / (k0 * window * window)
+    c1, c2 = scale * math.expm1(0.5) * 4096, scale * math.expm1(2.0) * 4096
+    pred = np.array([0.5, 2.0], np.float32)
+    assert proposal.budget_threshold(pred, w, h, k0, window, -1e30, 0.5 * c1) == 0.5
+    assert proposal.budget_threshold(pred, w, h, k0, window, -1e30, c1 + 0.5 * c2) == 2.0
+    assert proposal.budget_threshold(pred, w, h, k0, window, -1e30, 2 * (c1 + c2)) == np.inf
+    assert proposal.budget_threshold(pred, w, h, k0, window, 1.0, 0.5 * c1) == 1.0
+    assert proposal.budget_threshold(np.array([-np.inf, 2.0], np.float32), w, h, k0, window, -1e30, 0.5 * c2) == 2.0
