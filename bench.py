@@ -461,7 +461,7 @@ def main() -> None:
             import eval_proposal
             self.net, meta = eval_proposal.load_net(es_b200)
             self.threshold = meta["threshold"]
-            self.budget = meta.get("budget", 0.0) if args.budget is None else args.budget
+            self.budget = meta.get("skip_budget", 0.0) if args.budget is None else args.budget
             self.tolerance = meta.get("tolerance", 0.025) if args.tolerance is None else args.tolerance
             self.b.set_proposal(self.net, threshold=self.threshold, tolerance=self.tolerance, budget=self.budget)
             skip = (f"tiles predicted below {self.threshold:g}" +

@@ -794,7 +794,7 @@ int es_batch_set_proposal(es_batch *b, es_proposal_net *net, const es_proposal_o
             b->total_tiles0 = tiles0;
             const int P = (int)b->pictures.size();
             b->pred.reset(tiles0);
-            b->need.reset(tiles0);
+            b->need.reset(tiles0 + 1);  // + predict_kernel's tile counter
             size_t fs = 0;
             b->feat_at.clear();
             for (auto &pp : b->pictures) {

@@ -35,7 +35,7 @@ constexpr int kP0T = 64;                    // output tile side
 constexpr int kP0C = kP0T + 12, kP0R = kP0T + 8;  // staged columns (76) and rows (72)
 constexpr int kP0F = kP0T + 6;              // flat pixels per side: x0-3 .. x0+66, y0-3 .. y0+66
 
-__global__ void __launch_bounds__(256, 3) prep0_kernel(const __grid_constant__ Prep0Batch b)
+__global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ Prep0Batch b)
 {
     __shared__ __align__(16) uint16_t raw[kP0R][kP0C];
     __shared__ __align__(16) uint16_t pre8[kP0R - 1][kP0C];
@@ -102,31 +102,32 @@ __global__ void __launch_bounds__(256, 3) prep0_kernel(const __grid_constant__ P
     __syncthreads();
     const int c = tid & (kP0T - 1), g = tid >> 6, x = x0 + c;
     if (x >= w) return;
-    // flat counts of the 7 columns around x in flat rows 16 g .. 16 g + 21 (bit c of a row is column x - 3)
-    int h7[22];
+    // flat count of the 7 columns around x in flat row 16 g + q (bit c of a row is column x - 3), and the horizontal
+    // mode of picture row y0 + 16 g - 1 + k (staged row 16 g + 2 + k); both recomputed as the window moves, so few
+    // registers stay live and more blocks share an SM
     const int kw = c >> 5, sh = c & 31;
-#pragma unroll
-    for (int q = 0; q < 22; q++) h7[q] = __popc(__funnelshift_r(flatbits[16 * g + q][kw], flatbits[16 * g + q][kw + 1], sh) & 0x7Fu);
-    // horizontal modes of picture rows y0 + 16 g - 1 .. y0 + 16 g + 16 (staged rows 16 g + 2 .. 16 g + 19)
-    uint16_t hm[18];
+    auto h7 = [&](int q) { return __popc(__funnelshift_r(flatbits[16 * g + q][kw], flatbits[16 * g + q][kw + 1], sh) & 0x7Fu); };
     const bool edge_x = x == 0 || x == w - 1;
-#pragma unroll
-    for (int k = 0; k < 18; k++) {
+    auto hmode = [&](int k) -> uint16_t {
         const uint16_t *row = pre[16 * g + 2 + k];
-        hm[k] = edge_x ? row[c + 4] : mode3(row[c + 3], row[c + 4], row[c + 5]);
-    }
+        return edge_x ? row[c + 4] : mode3(row[c + 3], row[c + 4], row[c + 5]);
+    };
     int cnt = 0;
 #pragma unroll
-    for (int q = 0; q < 6; q++) cnt += h7[q];
-#pragma unroll
+    for (int q = 0; q < 6; q++) cnt += h7(q);
+    uint16_t m0 = hmode(0), m1 = hmode(1);
+#pragma unroll 4
     for (int i = 0; i < 16; i++) {
-        cnt += h7[i + 6];
+        cnt += h7(i + 6);
+        const uint16_t m2 = hmode(i + 2);
         const int y = y0 + 16 * g + i;
         if (y < h) {
-            const uint16_t v = (y == 0 || y == h - 1) ? pre[16 * g + 3 + i][c + 4] : mode3(hm[i], hm[i + 1], hm[i + 2]);
+            const uint16_t v = (y == 0 || y == h - 1) ? pre[16 * g + 3 + i][c + 4] : mode3(m0, m1, m2);
             J.word[(size_t)y * w + x] = (uint16_t)(v | (cnt > J.mask_index ? kMaskBit : 0));
         }
-        cnt -= h7[i];
+        cnt -= h7(i);
+        m0 = m1;
+        m1 = m2;
     }
 }
 
@@ -199,17 +200,21 @@ __global__ void slots_reset_kernel(CvSlot *slots, int nslots, const unsigned lon
 }
 
 // One radix round over every slot whose positive count exceeds k; block b takes the b-th share of each such slot's list.
-__global__ void __launch_bounds__(256) select_hist_kernel(CvSlot *slots, int nslots, int shift, int width)
+// One block of kSelThreads per SM: each block merges one shared histogram per slot into the slot's, so fewer, larger
+// blocks mean fewer global atomics for the same reads.
+constexpr int kSelThreads = 1024, kSelBlocks = 148;
+
+__global__ void __launch_bounds__(kSelThreads) select_hist_kernel(CvSlot *slots, int nslots, int shift, int width)
 {
     __shared__ unsigned hist[2048];
     const int nb = 1 << width;
     for (int sl = 0; sl < nslots; sl++) {
         CvSlot &S = slots[sl];
         if (S.count <= S.k) continue;  // the same for the whole block
-        for (int i = threadIdx.x; i < nb; i += 256) hist[i] = 0;
+        for (int i = threadIdx.x; i < nb; i += kSelThreads) hist[i] = 0;
         __syncthreads();
         const unsigned *v = (const unsigned *)S.list;
-        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
+        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * kSelThreads;
         const unsigned mask = S.mask, prefix = S.prefix;
         // neighbouring c-values of the list are often equal (they come from the same tile), so each thread adds runs
         // of equal digits at once; 4 values per 16-byte load
@@ -225,17 +230,17 @@ __global__ void __launch_bounds__(256) select_hist_kernel(CvSlot *slots, int nsl
             last = d;
             run = 1;
         };
-        for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+        for (unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n4; i += stride) {
             const uint4 q = __ldg((const uint4 *)v + i);
             add(q.x);
             add(q.y);
             add(q.z);
             add(q.w);
         }
-        for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(v[i]);
+        for (unsigned long long i = n4 * 4 + (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n; i += stride) add(v[i]);
         if (run) atomicAdd(&hist[last], run);
         __syncthreads();
-        for (int i = threadIdx.x; i < nb; i += 256)
+        for (int i = threadIdx.x; i < nb; i += kSelThreads)
             if (hist[i]) atomicAdd(&S.hist[i], hist[i]);
         __syncthreads();
     }
@@ -273,13 +278,13 @@ __global__ void __launch_bounds__(256) select_pick_kernel(CvSlot *slots, int shi
     for (int i = t; i < nb; i += 256) S.hist[i] = 0;
 }
 
-__global__ void __launch_bounds__(256) sum_above_kernel(CvSlot *slots, int nslots)
+__global__ void __launch_bounds__(kSelThreads) sum_above_kernel(CvSlot *slots, int nslots)
 {
     for (int sl = 0; sl < nslots; sl++) {
         CvSlot &S = slots[sl];
         if (S.count <= S.k) continue;
         const float threshold = __uint_as_float(S.prefix);
-        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * 256ull;
+        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * kSelThreads;
         unsigned long long s = 0, c = 0;
         auto add = [&](float v) {
             if (v > threshold) {
@@ -287,14 +292,14 @@ __global__ void __launch_bounds__(256) sum_above_kernel(CvSlot *slots, int nslot
                 c++;
             }
         };
-        for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+        for (unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n4; i += stride) {
             const float4 q = __ldg((const float4 *)S.list + i);
             add(q.x);
             add(q.y);
             add(q.z);
             add(q.w);
         }
-        for (unsigned long long i = n4 * 4 + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride) add(S.list[i]);
+        for (unsigned long long i = n4 * 4 + (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n; i += stride) add(S.list[i]);
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
             s += __shfl_down_sync(0xffffffffu, s, o);
@@ -379,7 +384,7 @@ cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width,
     if (nslots <= 0) return cudaSuccess;
     {
         LaunchTimer t("cambi_select_hist", s);
-        select_hist_kernel<<<148 * 8, 256, 0, s>>>(slots, nslots, shift, width);
+        select_hist_kernel<<<kSelBlocks, kSelThreads, 0, s>>>(slots, nslots, shift, width);
     }
     cudaError_t e = after_launch();
     if (e != cudaSuccess) return e;
@@ -392,7 +397,7 @@ cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s)
 {
     if (nslots <= 0) return cudaSuccess;
     LaunchTimer t("cambi_sum_above", s);
-    sum_above_kernel<<<148 * 8, 256, 0, s>>>(slots, nslots);
+    sum_above_kernel<<<kSelBlocks, kSelThreads, 0, s>>>(slots, nslots);
     return after_launch();
 }
 

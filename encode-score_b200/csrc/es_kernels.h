@@ -281,7 +281,8 @@ struct PredBatch {
     Band band;
     const float *params;    // bfloat16-rounded parameters (as floats)
     const uint32_t *frags;  // B fragments of layers 1, 2 and 3
-    unsigned *need;         // per scale-0 tile: non-zero when a pixel of it needs a c-value (zeroed by the launcher)
+    unsigned *need;         // per scale-0 tile: non-zero when a pixel of it needs a c-value, then a tile counter
+                            // (total_tiles + 1 words, zeroed by the launcher)
     float *pred;            // per scale-0 tile: the prediction, -inf where no pixel needs a c-value
 };
 // Both kernels of a prediction: the feature maps (and need flags) of every picture, then the network per tile.

@@ -186,9 +186,22 @@ __device__ __forceinline__ T half_warp_sum(T v)
     return v;
 }
 
-__global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_constant__ WindowBatch B)
+// Dynamic shared memory: the region planes, then the source's fine and mid numerators of each thread's 16 rows, kept
+// for the encodes' cross products (|fine| <= 9 x 1023 fits 16 bits) in shared memory so that three blocks fit an SM's
+// registers.
+struct WinStatsSmem {
+    WinSmem sm;
+    int mr[kWin][256];
+    int16_t fr[kWin][256];
+};
+
+__global__ void __launch_bounds__(256, 3) window_stats_kernel(const __grid_constant__ WindowBatch B)
 {
-    __shared__ __align__(16) WinSmem sm;
+    extern __shared__ __align__(16) unsigned char win_dyn[];
+    WinStatsSmem &ws = *(WinStatsSmem *)win_dyn;
+    WinSmem &sm = ws.sm;
+    auto &fr_s = ws.fr;
+    auto &mr_s = ws.mr;
     int jb = 0;
     while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_block) jb++;
     const WindowJob &J = B.job[jb];
@@ -202,7 +215,6 @@ __global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_const
     const bool inside = wx < ww && wy < wh;
     const int x = x0 + c;
     const bool gx_on = x > 0 && x < w - 1;
-    int fr[kWin], mr[kWin];
     unsigned long long src_f = 0, src_m = 0, src_xx = 0, src_yy = 0;
     long long src_xy = 0;
     for (int p = 0; p <= J.nenc; p++) {
@@ -235,11 +247,11 @@ __global__ void __launch_bounds__(256, 2) window_stats_kernel(const __grid_const
             const int gx = gx_on ? s3r - s3l : 0;
             const int gy = (y > 0 && y < h - 1) ? s3_next - s3_prev : 0;
             if (p == 0) {
-                fr[i] = f;
-                mr[i] = m;
+                fr_s[i][tid] = (int16_t)f;
+                mr_s[i][tid] = m;
             } else {
-                fine_x += f * fr[i];
-                mid_x += (long long)m * mr[i];
+                fine_x += f * (int)fr_s[i][tid];
+                mid_x += (long long)m * mr_s[i][tid];
             }
             fine_sq += (unsigned)(f * f);
             mid_sq += (unsigned long long)((long long)m * m);
@@ -304,7 +316,7 @@ __device__ __forceinline__ void window_mids(const WinSmem &sm, int c, int r0, in
     }
 }
 
-__global__ void __launch_bounds__(256, 2) persist_kernel(const __grid_constant__ PersistBatch B)
+__global__ void __launch_bounds__(256, 3) persist_kernel(const __grid_constant__ PersistBatch B)
 {
     __shared__ __align__(16) WinSmem sm;
     __shared__ __align__(16) uint16_t o_reg[kWR][kWS];
@@ -694,8 +706,11 @@ cudaError_t launch_window_stats(WindowBatch &b, cudaStream_t s)
         if (ww > 0 && wh > 0 && J.nenc > 0) blocks += ((ww + 3) / 4) * ((wh + 3) / 4);
     }
     if (blocks == 0) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(window_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sizeof(WinStatsSmem));
+    if (e != cudaSuccess) return e;
     LaunchTimer t("window_stats", s);
-    window_stats_kernel<<<blocks, 256, 0, s>>>(b);
+    window_stats_kernel<<<blocks, 256, sizeof(WinStatsSmem), s>>>(b);
     return after_launch();
 }
 

@@ -194,7 +194,7 @@ int es_proposal_predict(es_proposal_net *net, uint64_t words, int w, int h, floa
             pb.band.weight[d] = p.weight[d];
         }
         if (net->feat.count < feature_map_size(w, h)) net->feat.reset(feature_map_size(w, h));
-        if (net->need.count < (size_t)pb.total_tiles) net->need.reset(pb.total_tiles);
+        if (net->need.count < (size_t)pb.total_tiles + 1) net->need.reset(pb.total_tiles + 1);  // + the tile counter
         j.feat = net->feat.ptr;
         pb.need = net->need.ptr;
         pb.params = proposal_net_rounded(net, s);

@@ -271,6 +271,7 @@ __global__ void net_adam_kernel(float *P, float *R, const float *G, float *M, fl
 // Inference: one block of 128 threads per scale-0 tile, all four layers in shared memory.
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kPT = 128;
+constexpr int kPredBlocks = 148 * 4;  // persistent grid: 4 blocks of 46 KB per SM
 struct PredSmem {
     float f[2][kFeatTile][kFeatTile];             // features
     float w0[304], w3[145];                       // layers 0 and 3, weights then biases (bfloat16 values)
@@ -363,66 +364,76 @@ __device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *fr
     return sum;
 }
 
+// Persistent: each block loads the parameters once, then takes tiles from a counter (need[total_tiles]) until none
+// is left.
 __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ PredBatch b)
 {
     __shared__ PredSmem sm;
+    __shared__ int next;
     const int tid = threadIdx.x;
-    int j = 0;
-    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
-    const PredJob &J = b.job[j];
-    const int tile = blockIdx.x - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
-    if (!b.need[blockIdx.x]) {  // no pixel of the tile needs a c-value: nothing to predict (the same for the block)
-        if (tid == 0) b.pred[blockIdx.x] = -INFINITY;
-        return;
-    }
-    // the 24 x 24 feature window: map pixels 16 tx - 4 .. 16 tx + 19 (a tile is 16 map pixels; 0 outside the map)
-    const int fw = (J.w + 3) / 4, fh = (J.h + 3) / 4;
-    for (int i = tid; i < kFeatTile * kFeatTile; i += kPT) {
-        const int v = i / kFeatTile, u = i - v * kFeatTile, gu = 16 * tx - 4 + u, gv = 16 * ty - 4 + v;
-        float2 f = make_float2(0.0f, 0.0f);
-        if (gu >= 0 && gu < fw && gv >= 0 && gv < fh) f = J.feat[(size_t)gv * fw + gu];
-        sm.f[0][v][u] = f.x;
-        sm.f[1][v][u] = f.y;
-    }
     for (int i = tid; i < 304; i += kPT) sm.w0[i] = b.params[net_w(0) + i];
     for (int i = tid; i < 145; i += kPT) sm.w3[i] = b.params[net_w(3) + i];
     if (tid < 32) sm.b12[tid >> 4][tid & 15] = b.params[(tid < 16 ? net_b(1) : net_b(2)) + (tid & 15)];
     for (int i = tid; i < kNetFrags; i += kPT) sm.frags[i] = b.frags[i];
-    __syncthreads();
-    // layer 0: 2 -> 16, 22 x 22 outputs; warp g computes channels 4 g .. 4 g + 3 with their weights in registers
-    {
-        const int lane = tid & 31, cg = tid >> 5;
-        float wr[4][18], br[4];
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            br[c] = sm.w0[288 + 4 * cg + c];
-#pragma unroll
-            for (int ck = 0; ck < 18; ck++) wr[c][ck] = sm.w0[(4 * cg + c) * 18 + ck];  // [co][ci][k] = co * 18 + ci * 9 + k
+    for (;;) {
+        __syncthreads();  // every thread is done with the previous tile (and with `next`)
+        if (tid == 0) next = (int)atomicAdd(b.need + b.total_tiles, 1u);
+        __syncthreads();
+        const int gt = next;
+        if (gt >= b.total_tiles) break;
+        if (!b.need[gt]) {  // no pixel of the tile needs a c-value: nothing to predict (the same for the block)
+            if (tid == 0) b.pred[gt] = -INFINITY;
+            continue;
         }
-        for (int p = lane; p < 22 * 22; p += 32) {
-            const int y = p / 22, x = p - y * 22;
-            float acc[4] = {br[0], br[1], br[2], br[3]};
+        int j = 0;
+        while (j + 1 < b.njobs && gt >= b.job[j + 1].first_tile) j++;
+        const PredJob &J = b.job[j];
+        const int tile = gt - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
+        // the 24 x 24 feature window: map pixels 16 tx - 4 .. 16 tx + 19 (a tile is 16 map pixels; 0 outside the map)
+        const int fw = (J.w + 3) / 4, fh = (J.h + 3) / 4;
+        for (int i = tid; i < kFeatTile * kFeatTile; i += kPT) {
+            const int v = i / kFeatTile, u = i - v * kFeatTile, gu = 16 * tx - 4 + u, gv = 16 * ty - 4 + v;
+            float2 f = make_float2(0.0f, 0.0f);
+            if (gu >= 0 && gu < fw && gv >= 0 && gv < fh) f = J.feat[(size_t)gv * fw + gu];
+            sm.f[0][v][u] = f.x;
+            sm.f[1][v][u] = f.y;
+        }
+        __syncthreads();
+        // layer 0: 2 -> 16, 22 x 22 outputs; warp g computes channels 4 g .. 4 g + 3 with their weights in registers
+        {
+            const int lane = tid & 31, cg = tid >> 5;
+            float wr[4][18], br[4];
 #pragma unroll
-            for (int ck = 0; ck < 18; ck++) {
-                const int ci = ck / 9, k = ck % 9;
-                const float v = sm.f[ci][y + k / 3][x + k % 3];
+            for (int c = 0; c < 4; c++) {
+                br[c] = sm.w0[288 + 4 * cg + c];
 #pragma unroll
-                for (int c = 0; c < 4; c++) acc[c] = __fmaf_rn(v, wr[c][ck], acc[c]);
+                for (int ck = 0; ck < 18; ck++) wr[c][ck] = sm.w0[(4 * cg + c) * 18 + ck];  // [co][ci][k] = co * 18 + ci * 9 + k
             }
-            *(uint2 *)(sm.a1 + p * 8 + phys_half(p, cg >> 1) * 4 + (cg & 1) * 2) = make_uint2(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)),
-                                                            pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)));
+            for (int p = lane; p < 22 * 22; p += 32) {
+                const int y = p / 22, x = p - y * 22;
+                float acc[4] = {br[0], br[1], br[2], br[3]};
+#pragma unroll
+                for (int ck = 0; ck < 18; ck++) {
+                    const int ci = ck / 9, k = ck % 9;
+                    const float v = sm.f[ci][y + k / 3][x + k % 3];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[c] = __fmaf_rn(v, wr[c][ck], acc[c]);
+                }
+                *(uint2 *)(sm.a1 + p * 8 + phys_half(p, cg >> 1) * 4 + (cg & 1) * 2) = make_uint2(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)),
+                                                                pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)));
+            }
         }
+        __syncthreads();
+        mma_layer(sm.a1, 22, sm.a2, 20, sm.frags, sm.b12[0]);                   // layer 1: 20 x 20
+        __syncthreads();
+        mma_layer(sm.a2, 20, sm.a1, 18, sm.frags + 9 * 2 * 2 * 32, sm.b12[1]);  // layer 2: 18 x 18, into a1
+        __syncthreads();
+        // layer 3: 16 -> 1 on 16 x 16 (tensor cores), then the tile mean (a fixed order of additions)
+        const float s = mma_head(sm.a1, sm.frags + kNetFrags12);
+        if ((tid & 31) == 0) sm.part[tid >> 5] = s;
+        __syncthreads();
+        if (tid == 0) b.pred[gt] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f + sm.w3[144];
     }
-    __syncthreads();
-    mma_layer(sm.a1, 22, sm.a2, 20, sm.frags, sm.b12[0]);                   // layer 1: 20 x 20
-    __syncthreads();
-    mma_layer(sm.a2, 20, sm.a1, 18, sm.frags + 9 * 2 * 2 * 32, sm.b12[1]);  // layer 2: 18 x 18, into a1
-    __syncthreads();
-    // layer 3: 16 -> 1 on 16 x 16 (tensor cores), then the tile mean (a fixed order of additions)
-    const float s = mma_head(sm.a1, sm.frags + kNetFrags12);
-    if ((tid & 31) == 0) sm.part[tid >> 5] = s;
-    __syncthreads();
-    if (tid == 0) b.pred[blockIdx.x] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f + sm.w3[144];
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -605,7 +616,7 @@ cudaError_t launch_predict(PredBatch &b, cudaStream_t s)
         b.job[j].first_block = blocks;
         blocks += (int)((feature_map_size(b.job[j].w, b.job[j].h) + 255) / 256);
     }
-    cudaError_t e = cudaMemsetAsync(b.need, 0, sizeof(unsigned) * b.total_tiles, s);
+    cudaError_t e = cudaMemsetAsync(b.need, 0, sizeof(unsigned) * (b.total_tiles + 1), s);
     if (e != cudaSuccess) return e;
     {
         LaunchTimer t("proposal_features", s);
@@ -614,7 +625,7 @@ cudaError_t launch_predict(PredBatch &b, cudaStream_t s)
     e = after_launch();
     if (e != cudaSuccess) return e;
     LaunchTimer t("proposal_predict", s);
-    predict_kernel<<<b.total_tiles, kPT, 0, s>>>(b);
+    predict_kernel<<<b.total_tiles < kPredBlocks ? b.total_tiles : kPredBlocks, kPT, 0, s>>>(b);
     return after_launch();
 }
 

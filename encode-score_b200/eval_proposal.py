@@ -119,7 +119,7 @@ def main() -> None:
     module = es_b200.Module()
     net, meta = load_net(es_b200, args.net)
     t0 = time.time()
-    budget = meta.get("budget", 0.0) if args.budget is None else args.budget
+    budget = meta.get("skip_budget", 0.0) if args.budget is None else args.budget
     if args.sweep:
         out = {"threshold": meta["threshold"], "sweep": []}
         for item in args.sweep.split(","):
