@@ -247,7 +247,9 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             packed |= nib << (4 * i);
         }
         nbr[rc] = packed;
-        relneed[rc] = (uint16_t)mask;
+        // with no neighbour code in the region its c-value is 0 (pm = 0 for every distance): not served, so rows of
+        // such pixels (whole plateaus, codes requantised in steps over 4) count nothing
+        relneed[rc] = mask == (1u << 4) ? (uint16_t)0 : (uint16_t)mask;
     }
     // the rank plane: absolute ranks once for the tile when they fit in a byte, else per pass relative to the pass
     const bool per_pass = R > kMaxPlaneRank + 1;
