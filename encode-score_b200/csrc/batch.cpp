@@ -112,6 +112,19 @@ struct es_batch {
 
 namespace {
 
+Band band_of(const es_cambi_params &p)
+{
+    Band bd{};
+    bd.band_base = p.band_base;
+    bd.band_size = p.band_size;
+    bd.vlt = p.vlt;
+    for (int d = 0; d < kDiffs; d++) {
+        bd.tvi[d] = p.tvi[d];
+        bd.weight[d] = p.weight[d];
+    }
+    return bd;
+}
+
 void check_view(const es_frame_view &v, int pd, const char *what)
 {
     require(v.y != nullptr && v.u != nullptr && (v.semi || v.v != nullptr), std::string(what) + ": missing plane");
@@ -242,6 +255,7 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
     pb.params = b.net_params;
     pb.frags = b.net_frags;
     pb.pred = b.pred.ptr;
+    pb.features_ready = 1;  // made by the scale-0 launch
     cuda_check(launch_predict(pb, s), "tile predictions");
     const bool budget = b.popt.budget > 0;
     if (budget) {
@@ -337,8 +351,9 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
         if (pic.encode >= 0 || !((skip >> pic.source) & 1u)) run.push_back(i);
     }
     if (run.empty()) return;
+    const Band band = band_of(b.pictures[0]->p);
     Prep0Batch pb{};
-    int tiles = 0;
+    int pred_tiles = 0;  // with the proposal, scale 0 also makes the feature maps and the tiles' need flags
     for (int i : run) {
         const Picture &pic = *b.pictures[i];
         Prep0Job &j = pb.job[pb.njobs++];
@@ -349,11 +364,13 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
         j.depth = pic.depth;
         j.mask_index = pic.p.mask_index;
         j.word = pic.words[0].ptr;
-        j.tiles_x = (pic.w + 63) / 64;
-        j.first_tile = tiles;
-        tiles += j.tiles_x * ((pic.h + 31) / 32);
+        if (b.net) {
+            j.feat = b.feat.ptr + b.feat_at[i];
+            j.need = b.need.ptr + pred_tiles;
+            pred_tiles += ((pic.w + kCvTX - 1) / kCvTX) * ((pic.h + kCvTY - 1) / kCvTY);
+        }
     }
-    pb.total_tiles = tiles;
+    pb.band = band;
     cuda_check(launch_prep0(pb, s), "batch scale 0");
     const int nslots = (int)b.pictures.size() * kScales;
     cuda_check(launch_slots_reset(b.slots.ptr, nslots, b.slot_n.ptr, b.slot_k.ptr, s), "batch reset");
@@ -376,7 +393,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
         cuda_check(launch_decimate_mode(db, s), "batch scales");
     }
     CvBatch cb{};
-    tiles = 0;
+    int tiles = 0;
     for (int i : run) {
         const Picture &pic = *b.pictures[i];
         for (int sc = 0; sc < kScales; sc++) {
@@ -395,14 +412,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
     }
     cb.total_tiles = tiles;
     cb.max_pad = b.max_pad;
-    const es_cambi_params &p0 = b.pictures[0]->p;
-    cb.band.band_base = p0.band_base;
-    cb.band.band_size = p0.band_size;
-    cb.band.vlt = p0.vlt;
-    for (int d = 0; d < kDiffs; d++) {
-        cb.band.tvi[d] = p0.tvi[d];
-        cb.band.weight[d] = p0.weight[d];
-    }
+    cb.band = band;
     cb.lut = b.lut.ptr;
     cb.slots = b.slots.ptr;
     if (!b.net) {

@@ -11,6 +11,7 @@
 //  * the c-values themselves are in cvalues_kernels.cu;
 //  * select_round_kernel / select_pick_kernel / sum_above_kernel find the exact k-th largest value on the device when
 //    more than k values are positive (no host round trips), and score_kernel pools and weights the scales.
+#include "cambi_codes.h"
 #include "es_kernels.h"
 
 namespace es {
@@ -40,6 +41,7 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
     __shared__ __align__(16) uint16_t raw[kP0R][kP0C];
     __shared__ __align__(16) uint16_t pre8[kP0R - 1][kP0C];
     __shared__ uint32_t flatbits[kP0F][3];
+    __shared__ uint32_t needbits[32];
     int j = 0;
     while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
     const Prep0Job &J = b.job[j];
@@ -47,6 +49,14 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
     const int lane = tid & 31, warp = tid >> 5;
     const int x0 = (t % J.tiles_x) * kP0T, y0 = (t / J.tiles_x) * kP0T;
     const int xs = x0 - 4, ys = y0 - 3;
+    if (J.feat) {  // the codes that need c-values, bit c of word c / 32 (warp w makes words w, w + 8, ...)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int code = (warp + 8 * k) * 32 + lane;
+            const unsigned m = __ballot_sync(0xffffffffu, code < b.band.band_size && needs_cvalue(code, b.band));
+            if (lane == 0) needbits[warp + 8 * k] = m;
+        }
+    }
     const bool inside = xs >= 0 && xs + kP0C <= w && ys >= 0 && ys + kP0R <= h && (J.pitch & 3) == 0 && (((uintptr_t)J.img) & 7) == 0;
     if (inside) {
         for (int i = tid; i < kP0R * (kP0C / 4); i += 256) {
@@ -101,7 +111,8 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
     }
     __syncthreads();
     const int c = tid & (kP0T - 1), g = tid >> 6, x = x0 + c;
-    if (x >= w) return;
+    const bool feat = J.feat != nullptr;  // the same for the whole block
+    if (x >= w && !feat) return;
     // flat count of the 7 columns around x in flat row 16 g + q (bit c of a row is column x - 3), and the horizontal
     // mode of picture row y0 + 16 g - 1 + k (staged row 16 g + 2 + k); both recomputed as the window moves, so few
     // registers stay live and more blocks share an SM
@@ -116,18 +127,49 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
 #pragma unroll
     for (int q = 0; q < 6; q++) cnt += h7(q);
     uint16_t m0 = hmode(0), m1 = hmode(1);
+    // features of the 4 x 4 blocks (the proposal's block_features): value sum, masked and counted pixels of this
+    // column's 4 rows, then summed over the block's 4 columns (lanes c .. c + 3 of one warp)
+    unsigned fpack = 0;  // value sum (bits 0-15, at most 16 x 1023), masked pixels (16-20), counted pixels (24-28)
+    bool need = false;
+    const bool need_range = b.need_span >= 0;
+    const unsigned need_lo = (unsigned)b.need_lo, need_span = (unsigned)b.need_span;
 #pragma unroll 4
     for (int i = 0; i < 16; i++) {
         cnt += h7(i + 6);
         const uint16_t m2 = hmode(i + 2);
         const int y = y0 + 16 * g + i;
-        if (y < h) {
+        if (y < h && x < w) {
             const uint16_t v = (y == 0 || y == h - 1) ? pre[16 * g + 3 + i][c + 4] : mode3(m0, m1, m2);
-            J.word[(size_t)y * w + x] = (uint16_t)(v | (cnt > J.mask_index ? kMaskBit : 0));
+            const uint16_t word = (uint16_t)(v | (cnt > J.mask_index ? kMaskBit : 0));
+            J.word[(size_t)y * w + x] = word;
+            if (feat) {
+                fpack += (unsigned)v | ((unsigned)(word >> 15) << 16) | (1u << 24);
+                if (need_range) {
+                    need |= (word >> 15) && (unsigned)v - need_lo <= need_span;
+                } else {
+                    const uint16_t code = code_of(word, b.band);
+                    need |= code != kNone && ((needbits[code >> 5] >> (code & 31)) & 1u);
+                }
+            }
         }
         cnt -= h7(i);
         m0 = m1;
         m1 = m2;
+        if (feat && (i & 3) == 3) {
+            fpack += __shfl_xor_sync(0xffffffffu, fpack, 1);
+            fpack += __shfl_xor_sync(0xffffffffu, fpack, 2);
+            const int fw = (w + 3) / 4, fh = (h + 3) / 4, u = x >> 2, v4 = (y0 + 16 * g + i - 3) >> 2;
+            if ((c & 3) == 0 && u < fw && v4 < fh) {
+                const unsigned fsum = fpack & 0xFFFFu, fmask = (fpack >> 16) & 0xFFu, fn = fpack >> 24;
+                J.feat[(size_t)v4 * fw + u] = make_float2(fn ? (float)(((double)fsum / (double)fn - 512.0) / 256.0) : 0.0f,
+                                                          (float)((double)fmask / 16.0));
+            }
+            fpack = 0;
+        }
+    }
+    if (feat) {
+        need = __syncthreads_or(need);
+        if (tid == 0) J.need[t] = need ? 1u : 0u;
     }
 }
 
@@ -351,6 +393,17 @@ cudaError_t launch_prep0(Prep0Batch &b, cudaStream_t s)
     }
     b.total_tiles = tiles;
     if (b.total_tiles <= 0) return cudaSuccess;
+    // the values whose codes need c-values, as one range when they are one (they are for CAMBI's thresholds)
+    int lo = -1, hi = -2;
+    bool one_range = true;
+    for (int code = 0; code < b.band.band_size; code++) {
+        if (!cvalue_dists(code, b.band)) continue;
+        if (lo < 0) lo = code;
+        else if (code != hi + 1) one_range = false;
+        hi = code;
+    }
+    b.need_lo = lo < 0 ? 0 : lo + b.band.band_base;
+    b.need_span = !one_range ? -1 : lo < 0 ? -1 : hi - lo;
     LaunchTimer t("cambi_prep0", s);
     prep0_kernel<<<b.total_tiles, 256, 0, s>>>(b);
     return after_launch();

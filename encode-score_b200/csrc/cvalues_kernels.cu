@@ -224,6 +224,7 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
     __syncthreads();
     // per rank: its code; for a served code the rank offsets (+4) of its neighbours u-4 .. u-1, u+1 .. u+4 (15 = none)
     // and the mask of the ranks rank-4 .. rank+4 its c-value reads (bit 4 is its own)
+    bool any_served = false;
     for (int c = tid; c < bd.band_size; c += kCvThreads) {
         const int rc = rank[c];
         if (rc == kNone) continue;
@@ -250,6 +251,12 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         // with no neighbour code in the region its c-value is 0 (pm = 0 for every distance): not served, so rows of
         // such pixels (whole plateaus, codes requantised in steps over 4) count nothing
         relneed[rc] = mask == (1u << 4) ? (uint16_t)0 : (uint16_t)mask;
+        any_served |= mask != (1u << 4);
+    }
+    // every c-value of the tile is 0: nothing to count
+    if (!__syncthreads_or(any_served)) {
+        if (b.tile_mass && tid == 0) b.tile_mass[gt] = 0;
+        return;
     }
     // the rank plane: absolute ranks once for the tile when they fit in a byte, else per pass relative to the pass
     const bool per_pass = R > kMaxPlaneRank + 1;

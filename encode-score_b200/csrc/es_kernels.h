@@ -59,11 +59,18 @@ struct Prep0Job {
     int pitch, w, h, depth, mask_index;
     uint16_t *word;       // out: w x h, mode-filtered value | mask << 15
     int tiles_x, first_tile;  // set by the launcher
+    // optional (the tile proposal): the feature map of the words, ceil(h / 4) x ceil(w / 4) (mean, mask share) pairs
+    // as the proposal's feature kernel makes it, and per 64 x 64 tile whether a pixel needs a c-value (0 or 1)
+    float2 *feat;
+    unsigned *need;
 };
 constexpr int kPrep0MaxJobs = kMaxPictures;
 struct Prep0Batch {
     Prep0Job job[kPrep0MaxJobs];
     int njobs, total_tiles;  // total_tiles: set by the launcher
+    Band band;               // the codes that need c-values, for the need flags
+    int need_lo, need_span;  // set by the launcher: the needed values are need_lo .. need_lo + need_span when they
+                             // form one range (need_span >= 0), else need_span = -1 and the band's bits decide
 };
 cudaError_t launch_prep0(Prep0Batch &b, cudaStream_t s);
 
@@ -282,7 +289,8 @@ struct PredBatch {
     const float *params;    // bfloat16-rounded parameters (as floats)
     const uint32_t *frags;  // B fragments of layers 1, 2 and 3
     unsigned *need;         // per scale-0 tile: non-zero when a pixel of it needs a c-value, then a tile counter
-                            // (total_tiles + 1 words, zeroed by the launcher)
+                            // (total_tiles + 1 words, zeroed by the launcher unless features_ready)
+    int features_ready;     // the feature maps and need flags were made with scale 0 (prep0): only predict
     float *pred;            // per scale-0 tile: the prediction, -inf where no pixel needs a c-value
 };
 // Both kernels of a prediction: the feature maps (and need flags) of every picture, then the network per tile.

@@ -616,14 +616,19 @@ cudaError_t launch_predict(PredBatch &b, cudaStream_t s)
         b.job[j].first_block = blocks;
         blocks += (int)((feature_map_size(b.job[j].w, b.job[j].h) + 255) / 256);
     }
-    cudaError_t e = cudaMemsetAsync(b.need, 0, sizeof(unsigned) * (b.total_tiles + 1), s);
-    if (e != cudaSuccess) return e;
-    {
-        LaunchTimer t("proposal_features", s);
-        feature_map_kernel<<<blocks, 256, 0, s>>>(b);
+    if (b.features_ready) {  // only the tile counter after the need flags
+        cudaError_t e = cudaMemsetAsync(b.need + b.total_tiles, 0, sizeof(unsigned), s);
+        if (e != cudaSuccess) return e;
+    } else {
+        cudaError_t e = cudaMemsetAsync(b.need, 0, sizeof(unsigned) * (b.total_tiles + 1), s);
+        if (e != cudaSuccess) return e;
+        {
+            LaunchTimer t("proposal_features", s);
+            feature_map_kernel<<<blocks, 256, 0, s>>>(b);
+        }
+        e = after_launch();
+        if (e != cudaSuccess) return e;
     }
-    e = after_launch();
-    if (e != cudaSuccess) return e;
     LaunchTimer t("proposal_predict", s);
     predict_kernel<<<b.total_tiles < kPredBlocks ? b.total_tiles : kPredBlocks, kPT, 0, s>>>(b);
     return after_launch();
