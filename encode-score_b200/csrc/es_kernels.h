@@ -272,9 +272,11 @@ __host__ __device__ constexpr int net_w(int l) { return l == 0 ? 0 : l == 1 ? 30
 __host__ __device__ constexpr int net_b(int l) { return l == 0 ? 288 : l == 1 ? 2608 : l == 2 ? 4928 : 5088; }  // its biases
 constexpr int kFeatTile = 24;  // feature pixels per side around one tile (16 + 2 x 4 halo)
 // mma B fragments: layers 1 and 2 (16 -> 16) [layer][tap][n tile][register][lane], then layer 3 (16 -> 1, its one
-// output channel in column 0 of an 8-wide n tile) [tap][register][lane]
+// output channel in column 0 of an 8-wide n tile) [tap][register][lane], then layer 0 (2 -> 16, k = 4 tap + 2 part +
+// input channel, 36 of 3 k-steps of 16 used) [k-step][n tile][register][lane]
 constexpr int kNetFrags12 = 2 * 9 * 2 * 2 * 32;
-constexpr int kNetFrags = kNetFrags12 + 9 * 2 * 32;
+constexpr int kNetFrags3 = kNetFrags12 + 9 * 2 * 32;
+constexpr int kNetFrags = kNetFrags3 + 3 * 2 * 2 * 32;
 
 struct PredJob {
     const uint16_t *word;  // scale-0 words of a picture

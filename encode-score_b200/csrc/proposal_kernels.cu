@@ -273,8 +273,8 @@ __global__ void net_adam_kernel(float *P, float *R, const float *G, float *M, fl
 constexpr int kPT = 128;
 constexpr int kPredBlocks = 148 * 4;  // persistent grid: 4 blocks of 46 KB per SM
 struct PredSmem {
-    float f[2][kFeatTile][kFeatTile];             // features
-    float w0[304], w3[145];                       // layers 0 and 3, weights then biases (bfloat16 values)
+    uint32_t f[kFeatTile * kFeatTile][2];         // features per pixel: (head, remainder) bfloat16 pairs of channels 0, 1
+    float b0[16], w3[145];                        // layer 0's biases; layer 3's weights then bias (bfloat16 values)
     float b12[2][16];
     __align__(16) uint32_t a1[22 * 22 * 8];       // layer-0 output, [pixel][16 channels] bfloat16; later layer 2's
     __align__(16) uint32_t a2[20 * 20 * 8];       // layer-1 output
@@ -338,6 +338,48 @@ __device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *
     }
 }
 
+// Layer 0 (2 -> 16) on the tensor cores, 22 x 22 outputs from the 24 x 24 feature window: each FP32 feature enters as
+// a bfloat16 head and the bfloat16 of its remainder (k = 4 tap + 2 part + channel), so the products keep about 16 bits
+// of it; one 32-bit load gives a lane both channels of a pixel's part. Warp w takes m tiles w, w + 4, ...
+__device__ __forceinline__ void mma_layer0(const uint32_t (*fin)[2], uint32_t *out, const uint32_t *frags, const float *bias)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int ow = 22, iw = kFeatTile, npx = ow * ow, tiles = (npx + 15) / 16;
+    const int g = lane >> 2, t = lane & 3, part = t & 1;
+    for (int mt = warp; mt < tiles; mt += kPT / 32) {
+        int base[2];
+#pragma unroll
+        for (int hrow = 0; hrow < 2; hrow++) {
+            const int p = min(16 * mt + g + 8 * hrow, npx - 1);  // rows past the last pixel read a valid one, not stored
+            const int oy = p / ow;
+            base[hrow] = oy * iw + (p - oy * ow);
+        }
+        float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+        for (int ks = 0; ks < 3; ks++) {
+            const int ta = 4 * ks + (t >> 1), tb = ta + 2;  // the taps of k 16 ks + 2 t and 16 ks + 2 t + 8
+            auto ld = [&](int hrow, int tap) -> uint32_t {
+                return tap < 9 ? fin[base[hrow] + (tap / 3) * iw + tap % 3][part] : 0u;
+            };
+            const uint32_t a0 = ld(0, ta), a1 = ld(1, ta), a2 = ld(0, tb), a3 = ld(1, tb);
+            const uint32_t *fk = frags + ks * 4 * 32 + lane;
+            mma_bf16(c[0], a0, a1, a2, a3, fk[0], fk[32]);
+            mma_bf16(c[1], a0, a1, a2, a3, fk[64], fk[96]);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int ch = 8 * j + 2 * t;
+#pragma unroll
+            for (int hrow = 0; hrow < 2; hrow++) {
+                const int pr = 16 * mt + g + 8 * hrow;
+                if (pr >= npx) continue;
+                const float v0 = fmaxf(c[j][2 * hrow] + bias[ch], 0.0f), v1 = fmaxf(c[j][2 * hrow + 1] + bias[ch + 1], 0.0f);
+                out[pr * 8 + phys_half(pr, j) * 4 + t] = pack_bf16(v0, v1);
+            }
+        }
+    }
+}
+
 // Layer 3 (16 -> 1) on the 16 x 16 output from the 18 x 18 plane `in`: one 8-wide n tile whose column 0 holds the
 // output channel. Returns this warp's sum of its output pixels (lanes with lane % 4 == 0 hold column 0 of rows g and
 // g + 8), bias excluded.
@@ -371,7 +413,7 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
     __shared__ PredSmem sm;
     __shared__ int next;
     const int tid = threadIdx.x;
-    for (int i = tid; i < 304; i += kPT) sm.w0[i] = b.params[net_w(0) + i];
+    if (tid < 16) sm.b0[tid] = b.params[net_b(0) + tid];
     for (int i = tid; i < 145; i += kPT) sm.w3[i] = b.params[net_w(3) + i];
     if (tid < 32) sm.b12[tid >> 4][tid & 15] = b.params[(tid < 16 ? net_b(1) : net_b(2)) + (tid & 15)];
     for (int i = tid; i < kNetFrags; i += kPT) sm.frags[i] = b.frags[i];
@@ -395,34 +437,12 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
             const int v = i / kFeatTile, u = i - v * kFeatTile, gu = 16 * tx - 4 + u, gv = 16 * ty - 4 + v;
             float2 f = make_float2(0.0f, 0.0f);
             if (gu >= 0 && gu < fw && gv >= 0 && gv < fh) f = J.feat[(size_t)gv * fw + gu];
-            sm.f[0][v][u] = f.x;
-            sm.f[1][v][u] = f.y;
+            const float h0 = bf16r(f.x), h1 = bf16r(f.y);
+            sm.f[i][0] = pack_bf16(h0, h1);
+            sm.f[i][1] = pack_bf16(f.x - h0, f.y - h1);  // the remainders are exact in FP32
         }
         __syncthreads();
-        // layer 0: 2 -> 16, 22 x 22 outputs; warp g computes channels 4 g .. 4 g + 3 with their weights in registers
-        {
-            const int lane = tid & 31, cg = tid >> 5;
-            float wr[4][18], br[4];
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                br[c] = sm.w0[288 + 4 * cg + c];
-#pragma unroll
-                for (int ck = 0; ck < 18; ck++) wr[c][ck] = sm.w0[(4 * cg + c) * 18 + ck];  // [co][ci][k] = co * 18 + ci * 9 + k
-            }
-            for (int p = lane; p < 22 * 22; p += 32) {
-                const int y = p / 22, x = p - y * 22;
-                float acc[4] = {br[0], br[1], br[2], br[3]};
-#pragma unroll
-                for (int ck = 0; ck < 18; ck++) {
-                    const int ci = ck / 9, k = ck % 9;
-                    const float v = sm.f[ci][y + k / 3][x + k % 3];
-#pragma unroll
-                    for (int c = 0; c < 4; c++) acc[c] = __fmaf_rn(v, wr[c][ck], acc[c]);
-                }
-                *(uint2 *)(sm.a1 + p * 8 + phys_half(p, cg >> 1) * 4 + (cg & 1) * 2) = make_uint2(pack_bf16(fmaxf(acc[0], 0.f), fmaxf(acc[1], 0.f)),
-                                                                pack_bf16(fmaxf(acc[2], 0.f), fmaxf(acc[3], 0.f)));
-            }
-        }
+        mma_layer0(sm.f, sm.a1, sm.frags + kNetFrags3, sm.b0);                  // layer 0: 22 x 22
         __syncthreads();
         mma_layer(sm.a1, 22, sm.a2, 20, sm.frags, sm.b12[0]);                   // layer 1: 20 x 20
         __syncthreads();
@@ -591,6 +611,13 @@ __global__ void net_pack_kernel(const float *R, uint32_t *frags)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kNetFrags) return;
+    if (i >= kNetFrags3) {  // layer 0: word [ks][j][r][lane]: n = 8 j + lane / 4, k rows 16 ks + 2 (lane % 4) + 8 r, + 1
+        const int q = i - kNetFrags3, lane = q & 31, r = (q >> 5) & 1, j = (q >> 6) & 1, ks = q >> 7;
+        const int n = 8 * j + (lane >> 2), tap = 4 * ks + 2 * r + ((lane & 3) >> 1);  // k = 4 tap + 2 part + channel
+        const float *W = R + net_w(0);
+        frags[i] = tap < 9 ? pack_bf16(W[(n * 2 + 0) * 9 + tap], W[(n * 2 + 1) * 9 + tap]) : 0u;
+        return;
+    }
     if (i >= kNetFrags12) {  // layer 3: word [k][r][lane], column n = lane / 4 holds the weights when n == 0, else 0
         const int q = i - kNetFrags12, lane = q & 31, r = (q >> 5) & 1, k = q >> 6;
         const int n = lane >> 2, c = 2 * (lane & 3) + 8 * r;
