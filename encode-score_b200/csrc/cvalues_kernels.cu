@@ -4,16 +4,17 @@
 // One 256-thread block per 64 x 64 tile of any scale of any picture (a table of jobs):
 //  1. a pre-check of the tile's own pixels (16-byte loads) lets tiles with nothing to compute -- most tiles of most
 //     pictures -- leave after reading them;
-//  2. the tile and its window margins are staged in shared memory as band codes (value - band_base of a masked pixel
-//     in the band, kNone otherwise) with 16-byte loads from an 8-pixel-aligned start; the codes that can matter --
-//     occurring within kDiffs of a code whose c-value is needed -- are ranked in order, each rank gets its code, the
-//     rank offsets of its 8 neighbour codes and the mask of ranks its c-value reads, and the region becomes a plane
-//     of 8-bit ranks;
-//  3. per pass over 32 ranks, rank pair p (two ranks) belongs to warp p % 8: the warp keeps the pair's column counts
-//     (ranks occurring in the 2 pad + 1 window rows of each column, 8 bits per column and rank, 4 columns per lane) in
-//     registers, slides them down the rows with byte-parallel compares of the leaving and entering rows, and on rows
-//     whose pixels read the pair turns them into window counts of the 64 tile columns (a prefix sum over the columns,
-//     two ranks per 32-bit lane). Every 4 rows all 8 warps compute the 256 c-values from those counts.
+//  2. the band codes (value - band_base of a masked pixel in the band, kNone otherwise) of the tile and its window
+//     margins are read with 16-byte loads from an 8-pixel-aligned start; the codes that can matter -- occurring within
+//     kDiffs of a code whose c-value is needed -- are ranked in order, each rank gets its code, the rank offsets of
+//     its 8 neighbour codes and the mask of ranks its c-value reads (tiles where no code has a neighbour code leave:
+//     their c-values are all 0), and a second read of the codes makes the region a shared-memory plane of 8-bit
+//     ranks;
+//  3. per pass over 32 ranks, the ranks' column counts (8 bits per column and rank: pixels of the 2 pad + 1 window rows)
+//     sit in shared memory as a 32 x region-width byte matrix and slide down the rows (the leaving and entering row's
+//     rank per column); on rows whose pixels read the pass's ranks, the window counts of the 64 tile columns are one
+//     exact integer matrix product on the tensor cores (mma.sync u8, counts x a band of ones 2 pad + 1 wide), each warp
+//     making 8 columns. Every 4 rows all 8 warps compute the 256 c-values from those counts.
 // Positive c-values are summed exactly (they are multiples of 2^-24) and counted, and each block appends them to its
 // scale's list (for the top-k selection) through a bounded shared-memory buffer; nothing per pixel is written unless
 // the caller asks for the c-value planes.
@@ -33,14 +34,20 @@ constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks
 __host__ __device__ constexpr int cv_rw(int pad) { return kCvTX + 2 * pad; }
 // the staged region starts at the multiple of 8 at or left of x0 - pad; its row stride is a whole number of vectors
 __host__ __device__ constexpr int cv_stride(int pad) { return (cv_rw(pad) + 7 + 7) & ~7; }
-__host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // rank plane row (scan width)
+__host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // rank plane row
+// k-steps of 32 region columns, and the row of the column counts (bytes; 16 more than the k-steps, so the 8 rows an
+// ldmatrix phase reads fall on different banks)
+__host__ __device__ constexpr int cv_nk(int pad) { return (cv_rw(pad) + 31) >> 5; }
+__host__ __device__ constexpr int cv_cstr(int pad) { return 32 * cv_nk(pad) + 16; }
+constexpr int kCvMaxK = cv_nk(kMaxPad);
+constexpr int kCvWS = kCvTX + 2;  // window-count row (u16): an odd number of words, so ranks fall on different banks
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 // Shared memory: the rank plane, the per-code and per-rank tables and the pass buffers. (The band codes are read from
 // global memory twice, once for the code tables and once for the rank plane, instead of being staged: the smaller
 // footprint lets 4 blocks share an SM.)
 struct CvLayout {
-    size_t rplane, rank, rcode, nbr, relneed, wcount, prefix, list, total;
+    size_t rplane, rank, rcode, nbr, relneed, wcount, cols, list, total;
 };
 __host__ __device__ inline CvLayout cv_layout(int pad)
 {
@@ -52,21 +59,26 @@ __host__ __device__ inline CvLayout cv_layout(int pad)
     l.nbr = align16(l.rcode + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
     l.wcount = align16(l.relneed + (size_t)kMaxBand * 2);
-    l.prefix = align16(l.wcount + (size_t)kCvChunk * (kCvBins / 2) * kCvTX * 4);
-    l.list = align16(l.prefix + (size_t)kWarps * cv_cs(pad) * 4);
+    l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * kCvWS * 2);
+    l.list = align16(l.cols + (size_t)kCvBins * cv_cstr(pad));
     l.total = align16(l.list + (size_t)kListCap * 4);
     return l;
 }
 
 
-// Bytes of `quad` equal to a (ma) and to a + 1 (mb), a even, ta4 = a in every byte: 1 per matching byte.
-__device__ __forceinline__ void pair_match(uint32_t quad, uint32_t ta4, uint32_t &ma, uint32_t &mb)
+__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
 {
-    const uint32_t z = quad ^ ta4;                                             // 0 for a, 1 for a + 1
-    const uint32_t t = ((z & 0x7E7E7E7Eu) + 0x7F7F7F7Fu) | (z & 0xFEFEFEFEu);  // bit 7 set: byte not in {a, a + 1}
-    const uint32_t hit = (~t >> 7) & 0x01010101u;
-    mb = hit & z;
-    ma = hit ^ mb;
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+// d += a (16 x 32 u8, row-major) x b (32 x 8 u8, column-major), exact in 32-bit integers.
+__device__ __forceinline__ void mma_u8(int (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                 : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
 __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_constant__ CvBatch b)
@@ -136,7 +148,7 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         return;
     }
 
-    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P), NQ = CS / 128;
+    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P);
     const int xs = ((x0 - P) >> 3) << 3, ox = (x0 - P) - xs;  // region start (aligned) and the offset of x0 - P in it
     const CvLayout L = cv_layout(P);
     uint8_t *rplane = smem + L.rplane;                   // [RH][CS]: rank (- offset) of pixel (x0 - P + j, y0 - P + r)
@@ -144,8 +156,6 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
     uint16_t *rcode = (uint16_t *)(smem + L.rcode);      // rank -> code
     uint32_t *nbr = (uint32_t *)(smem + L.nbr);          // rank -> neighbour rank offsets
     uint16_t *relneed = (uint16_t *)(smem + L.relneed);  // rank -> ranks read (bit 4: itself); 0: not served
-    uint32_t *wcount = (uint32_t *)(smem + L.wcount);    // [chunk row][rank pair][column] packed window counts
-    uint32_t *prefix = (uint32_t *)(smem + L.prefix);    // per-warp prefix rows
     float *blist = (float *)(smem + L.list);
     if (tid < 32) occ[tid] = srv[tid] = 0;
     if (tid == 0) list_n = 0;
@@ -297,12 +307,36 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         __syncthreads();
     };
 
-    uint32_t *wpre = prefix + warp * CS;
+    // Window counts on the tensor cores: per row, W[rank][x] = sum over region columns j of C[rank][j] B[j][x], where C
+    // holds the ranks' column counts (8 bits: at most 2 pad + 1 rows) and B[j][x] = 1 for x <= j <= x + 2 pad; exact
+    // in the 32-bit accumulators. Warp w makes output columns 8 w .. 8 w + 7 (one n tile) for ranks 0-15 and 16-31 (two
+    // m tiles), over the k-steps of 32 region columns its window reaches.
+    uint8_t *colc = smem + L.cols;                       // [rank][CSTR]: column counts of the pass's ranks
+    uint16_t *wc16 = (uint16_t *)(smem + L.wcount);      // [chunk row][rank][kCvWS]: window counts
+    const int NK = cv_nk(P), CSTR = cv_cstr(P);
+    const int g = lane >> 2, t = lane & 3;
+    uint32_t bfrag[kCvMaxK][2];  // this lane's B fragments: rows (region columns) 32 ks + 16 r + 4 t + i, column 8 w + g
+#pragma unroll
+    for (int ks = 0; ks < kCvMaxK; ks++)
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int j = 32 * ks + 16 * r + 4 * t + i, x = 8 * warp + g;
+                word |= (uint32_t)(j >= x && j <= x + 2 * P) << (8 * i);
+            }
+            bfrag[ks][r] = word;
+        }
+    const int ks_lo = (8 * warp) >> 5, ks_hi = min(NK - 1, (8 * warp + 7 + 2 * P) >> 5);
+    const uint32_t cbase = (uint32_t)__cvta_generic_to_shared(colc);
+    const int lrow = ((lane >> 3) & 1) * 8 + (lane & 7), lcol = (lane >> 4) * 16;  // this lane's ldmatrix row address
     for (int b0 = 0;;) {
         const int lo = b0 ? b0 + kDiffs : 0, hi = b0 + kCvBins >= R ? R : b0 + kCvBins - kDiffs;
         const int off = per_pass ? 0 : b0;  // plane value of pass rank k: k + off
         if (per_pass) build_plane(b0);
         if (tid < kCvTY) rowneed[tid] = 0;
+        for (int i = tid; i < kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
         __syncthreads();
         // the pass ranks each row's pixels read: a warp covers 32 pixels of one row
         for (int i = tid; i < kCvTY * kCvTX; i += kCvThreads) {
@@ -323,74 +357,50 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             if (lane == 0 && need) atomicOr(&rowneed[r], need);
         }
         __syncthreads();
-        // this warp's rank pairs w and w + 8, if some row reads them: column counts of 4 columns per lane and quad
-        const uint32_t pass_need = __reduce_or_sync(kFull, rowneed[lane] | rowneed[lane + 32]);
-        const uint32_t pairs_used = (pass_need | (pass_need >> 1)) & 0x55555555u;
-        bool act[2];
-        uint32_t t4[2];
-        uint32_t cnt[2][2][2];  // [owned pair][quad][rank a, a + 1]: 8-bit counts of 4 columns
-#pragma unroll
-        for (int s = 0; s < 2; s++) {
-            const int p = warp + kWarps * s;
-            act[s] = (pairs_used >> (2 * p)) & 1u;
-            t4[s] = (unsigned)(2 * p + off) * 0x01010101u;
-#pragma unroll
-            for (int q = 0; q < 2; q++) cnt[s][q][0] = cnt[s][q][1] = 0;
-        }
-        auto count_row = [&](int r, bool enter) {  // adds (enter) or removes the ranks of region row r
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                if (q >= NQ) break;
-                const uint32_t quad = *(const uint32_t *)(rplane + r * CS + 128 * q + 4 * lane);
-#pragma unroll
-                for (int s = 0; s < 2; s++) {
-                    if (!act[s]) continue;
-                    uint32_t ma, mb;
-                    pair_match(quad, t4[s], ma, mb);
-                    if (enter) {
-                        cnt[s][q][0] += ma;
-                        cnt[s][q][1] += mb;
-                    } else {
-                        cnt[s][q][0] -= ma;
-                        cnt[s][q][1] -= mb;
-                    }
-                }
-            }
+        const bool pass_any = __syncthreads_or(tid < kCvTY && rowneed[tid] != 0);
+        // pass rank (0 .. 31) of region pixel (c, rr), or -1
+        auto rank_at = [&](int rr, int c) -> int {
+            const unsigned v = rplane[rr * CS + c];
+            const int k = (int)v - off;
+            return (v != kNoRank && k >= 0 && k < kCvBins) ? k : -1;
         };
-        if (act[0] || act[1]) {
+        if (pass_any) {  // column counts of the first 2 pad + 1 region rows
             const int last = min(2 * P, RH - 1);
-            for (int r = 0; r <= last; r++) count_row(r, true);
-        }
-        // window counts of owned pair s at chunk row i into wcount
-        auto window_counts = [&](int s, int i) {
-            const int p = warp + kWarps * s;
-            unsigned carry = 0;
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                if (q >= NQ) break;
-                const uint32_t fa = cnt[s][q][0], fb = cnt[s][q][1];
-                const uint32_t a0 = fa & 0x00FF00FFu, c0 = fb & 0x00FF00FFu, a1 = (fa >> 8) & 0x00FF00FFu, c1 = (fb >> 8) & 0x00FF00FFu;
-                // column 4 lane + i of rank 2p in the low 16 bits, of rank 2p + 1 in the high 16 bits
-                const unsigned s1 = __byte_perm(a0, c0, 0x5410), s2 = s1 + __byte_perm(a1, c1, 0x5410),
-                               s3 = s2 + __byte_perm(a0, c0, 0x7632), s4 = s3 + __byte_perm(a1, c1, 0x7632);
-                unsigned incl = s4;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const unsigned v = __shfl_up_sync(kFull, incl, o);
-                    if (lane >= o) incl += v;
+            for (int c = tid; c < RW; c += kCvThreads)
+                for (int rr = 0; rr <= last; rr++) {
+                    const int k = rank_at(rr, c);
+                    if (k >= 0) colc[k * CSTR + c]++;
                 }
-                const unsigned ex = incl - s4 + carry;
-                *(uint4 *)(wpre + 128 * q + 4 * lane) = make_uint4(ex + s1, ex + s2, ex + s3, ex + s4);
-                carry += __shfl_sync(kFull, incl, 31);
-            }
-            __syncwarp();
-            uint32_t *wrow = wcount + (i * (kCvBins / 2) + p) * kCvTX;
+        }
+        __syncthreads();
+        // window counts of chunk row i, for the m tiles the row reads
+        auto window_counts = [&](int i, uint32_t need) {
+            const bool m0 = (need & 0xFFFFu) != 0, m1 = (need >> 16) != 0;
+            int acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll
-            for (int h2 = 0; h2 < 2; h2++) {
-                const int x = lane + 32 * h2;
-                wrow[x] = wpre[x + 2 * P] - (x > 0 ? wpre[x - 1] : 0u);
+            for (int ks = 0; ks < kCvMaxK; ks++) {
+                if (ks < ks_lo || ks > ks_hi) continue;
+                const uint32_t at = cbase + lrow * CSTR + 32 * ks + lcol;
+                uint32_t a0, a1, a2, a3;
+                if (m0) {
+                    ldmatrix_x4(at, a0, a1, a2, a3);
+                    mma_u8(acc[0], a0, a1, a2, a3, bfrag[ks][0], bfrag[ks][1]);
+                }
+                if (m1) {
+                    ldmatrix_x4(at + 16 * CSTR, a0, a1, a2, a3);
+                    mma_u8(acc[1], a0, a1, a2, a3, bfrag[ks][0], bfrag[ks][1]);
+                }
             }
-            __syncwarp();
+            // rank 16 m + g (+ 8) at columns 8 w + 2 t and + 1
+            uint16_t *wrow = wc16 + (size_t)i * kCvBins * kCvWS + 8 * warp + 2 * t;
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                if (!(m ? m1 : m0)) continue;
+#pragma unroll
+                for (int h2 = 0; h2 < 2; h2++)
+                    *(uint32_t *)(wrow + (16 * m + g + 8 * h2) * kCvWS) =
+                        ((uint32_t)acc[m][2 * h2] & 0xFFFFu) | ((uint32_t)acc[m][2 * h2 + 1] << 16);
+            }
         };
         const int ci = tid >> 6, cc = tid & (kCvTX - 1);  // this thread's pixel in a chunk
         for (int r0 = 0; r0 < rows; r0 += kCvChunk) {
@@ -398,15 +408,20 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             bool chunk_any = false;
             for (int i = 0; i < n_rows; i++) {
                 const int r = r0 + i;
-                if (r > 0 && (act[0] || act[1])) {
-                    count_row(r - 1, false);
-                    if (r + 2 * P < RH) count_row(r + 2 * P, true);
+                if (r > 0 && pass_any) {  // slide the column counts down to region rows r .. r + 2 pad
+                    __syncthreads();      // every warp has read the counts of the row before
+                    for (int c = tid; c < RW; c += kCvThreads) {
+                        const int kl = rank_at(r - 1, c), ke = r + 2 * P < RH ? rank_at(r + 2 * P, c) : -1;
+                        if (kl != ke) {
+                            if (kl >= 0) colc[kl * CSTR + c]--;
+                            if (ke >= 0) colc[ke * CSTR + c]++;
+                        }
+                    }
+                    __syncthreads();
                 }
                 const uint32_t need = rowneed[r];
                 chunk_any |= need != 0;
-#pragma unroll
-                for (int s = 0; s < 2; s++)
-                    if (act[s] && ((need >> (2 * (warp + kWarps * s))) & 3u)) window_counts(s, i);
+                if (need) window_counts(i, need);
             }
             if (!chunk_any) continue;
             __syncthreads();
@@ -422,8 +437,8 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
                         served = true;
                         const uint32_t nb = nbr[rk];
                         const int base = k - 4;
-                        const uint32_t *wc = wcount + ci * (kCvBins / 2) * kCvTX + cc;
-                        auto count = [&](int kk) -> unsigned { return (wc[(kk >> 1) * kCvTX] >> ((kk & 1) * 16)) & 0xFFFFu; };
+                        const uint16_t *wc = wc16 + (size_t)ci * kCvBins * kCvWS + cc;
+                        auto count = [&](int kk) -> unsigned { return wc[kk * kCvWS]; };
                         const int value = rcode[rk] + bd.band_base + kDiffs;
                         const unsigned p0 = count(k);
 #pragma unroll

@@ -311,6 +311,11 @@ __device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *
     const int g = lane >> 2, t = lane & 3;
     const int mrow = ((lane >> 3) & 1) * 8 + (lane & 7), khalf = lane >> 4;  // this lane's ldmatrix row and k half
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(in);
+    uint32_t bf[9][4];  // this lane's B fragments of every tap, (n tile, register), kept across the m tiles
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+#pragma unroll
+        for (int r = 0; r < 4; r++) bf[k][r] = frags[k * 4 * 32 + r * 32 + lane];
     for (int mt = warp; mt < tiles; mt += kPT / 32) {
         const int p = min(16 * mt + mrow, npx - 1);
         const int oy = p / ow, ox = p - oy * ow;
@@ -320,9 +325,8 @@ __device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *
             const int q = (oy + k / 3) * iw + ox + k % 3;
             uint32_t a0, a1, a2, a3;
             ldmatrix_x4(base + q * 32 + phys_half(q, khalf) * 16, a0, a1, a2, a3);
-            const uint32_t *fk = frags + k * 4 * 32 + lane;  // this tap's fragments: (n tile, register) x lane
-            mma_bf16(c[0], a0, a1, a2, a3, fk[0], fk[32]);
-            mma_bf16(c[1], a0, a1, a2, a3, fk[64], fk[96]);
+            mma_bf16(c[0], a0, a1, a2, a3, bf[k][0], bf[k][1]);
+            mma_bf16(c[1], a0, a1, a2, a3, bf[k][2], bf[k][3]);
         }
 #pragma unroll
         for (int j = 0; j < 2; j++) {
@@ -388,6 +392,12 @@ __device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *fr
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int mrow = ((lane >> 3) & 1) * 8 + (lane & 7), khalf = lane >> 4;
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(in);
+    uint32_t bf[9][2];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        bf[k][0] = frags[k * 2 * 32 + lane];
+        bf[k][1] = frags[k * 2 * 32 + 32 + lane];
+    }
     float sum = 0.0f;
     for (int mt = warp; mt < 16; mt += kPT / 32) {  // m tile mt: output row mt, 16 pixels
         float c[4] = {0, 0, 0, 0};
@@ -396,8 +406,7 @@ __device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *fr
             const int q = (mt + k / 3) * 18 + mrow + k % 3;
             uint32_t a0, a1, a2, a3;
             ldmatrix_x4(base + q * 32 + phys_half(q, khalf) * 16, a0, a1, a2, a3);
-            const uint32_t *fk = frags + k * 2 * 32 + lane;
-            mma_bf16(c, a0, a1, a2, a3, fk[0], fk[32]);
+            mma_bf16(c, a0, a1, a2, a3, bf[k][0], bf[k][1]);
         }
         if ((lane & 3) == 0) sum += c[0] + c[2];
     }
