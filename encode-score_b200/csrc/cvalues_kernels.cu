@@ -18,6 +18,8 @@
 // Positive c-values are summed exactly (they are multiples of 2^-24) and counted, and each block appends them to its
 // scale's list (for the top-k selection) through a bounded shared-memory buffer; nothing per pixel is written unless
 // the caller asks for the c-value planes.
+#include <type_traits>
+
 #include "cambi_codes.h"
 #include "es_kernels.h"
 
@@ -315,20 +317,21 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
     uint16_t *wc16 = (uint16_t *)(smem + L.wcount);      // [chunk row][rank][kCvWS]: window counts
     const int NK = cv_nk(P), CSTR = cv_cstr(P);
     const int g = lane >> 2, t = lane & 3;
-    uint32_t bfrag[kCvMaxK][2];  // this lane's B fragments: rows (region columns) 32 ks + 16 r + 4 t + i, column 8 w + g
+    const int ks_lo = (8 * warp) >> 5, ks_hi = min(NK - 1, (8 * warp + 7 + 2 * P) >> 5);
+    uint32_t bfrag[kCvMaxK][2];  // this lane's B fragments: rows (region columns) 32 (ks_lo + kk) + 16 r + 4 t + i,
+                                 // column 8 w + g
 #pragma unroll
-    for (int ks = 0; ks < kCvMaxK; ks++)
+    for (int kk = 0; kk < kCvMaxK; kk++)
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             uint32_t word = 0;
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                const int j = 32 * ks + 16 * r + 4 * t + i, x = 8 * warp + g;
+                const int j = 32 * (ks_lo + kk) + 16 * r + 4 * t + i, x = 8 * warp + g;
                 word |= (uint32_t)(j >= x && j <= x + 2 * P) << (8 * i);
             }
-            bfrag[ks][r] = word;
+            bfrag[kk][r] = word;
         }
-    const int ks_lo = (8 * warp) >> 5, ks_hi = min(NK - 1, (8 * warp + 7 + 2 * P) >> 5);
     const uint32_t cbase = (uint32_t)__cvta_generic_to_shared(colc);
     const int lrow = ((lane >> 3) & 1) * 8 + (lane & 7), lcol = (lane >> 4) * 16;  // this lane's ldmatrix row address
     for (int b0 = 0;;) {
@@ -373,33 +376,43 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
                 }
         }
         __syncthreads();
-        // window counts of chunk row i, for the m tiles the row reads
-        auto window_counts = [&](int i, uint32_t need) {
+        // window counts of chunk row i, for the m tiles the row reads, over N k-steps (N the same for the warp)
+        auto window_counts_n = [&](auto n_ksteps, int i, uint32_t need) {
+            constexpr int N = decltype(n_ksteps)::value;
             const bool m0 = (need & 0xFFFFu) != 0, m1 = (need >> 16) != 0;
             int acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+            const uint32_t at0 = cbase + lrow * CSTR + 32 * ks_lo + lcol;
 #pragma unroll
-            for (int ks = 0; ks < kCvMaxK; ks++) {
-                if (ks < ks_lo || ks > ks_hi) continue;
-                const uint32_t at = cbase + lrow * CSTR + 32 * ks + lcol;
+            for (int kk = 0; kk < N; kk++) {
                 uint32_t a0, a1, a2, a3;
                 if (m0) {
-                    ldmatrix_x4(at, a0, a1, a2, a3);
-                    mma_u8(acc[0], a0, a1, a2, a3, bfrag[ks][0], bfrag[ks][1]);
+                    ldmatrix_x4(at0 + 32 * kk, a0, a1, a2, a3);
+                    mma_u8(acc[0], a0, a1, a2, a3, bfrag[kk][0], bfrag[kk][1]);
                 }
                 if (m1) {
-                    ldmatrix_x4(at + 16 * CSTR, a0, a1, a2, a3);
-                    mma_u8(acc[1], a0, a1, a2, a3, bfrag[ks][0], bfrag[ks][1]);
+                    ldmatrix_x4(at0 + 16 * CSTR + 32 * kk, a0, a1, a2, a3);
+                    mma_u8(acc[1], a0, a1, a2, a3, bfrag[kk][0], bfrag[kk][1]);
                 }
             }
-            // rank 16 m + g (+ 8) at columns 8 w + 2 t and + 1
-            uint16_t *wrow = wc16 + (size_t)i * kCvBins * kCvWS + 8 * warp + 2 * t;
-#pragma unroll
-            for (int m = 0; m < 2; m++) {
-                if (!(m ? m1 : m0)) continue;
-#pragma unroll
-                for (int h2 = 0; h2 < 2; h2++)
-                    *(uint32_t *)(wrow + (16 * m + g + 8 * h2) * kCvWS) =
-                        ((uint32_t)acc[m][2 * h2] & 0xFFFFu) | ((uint32_t)acc[m][2 * h2 + 1] << 16);
+            // rank 16 m + g (+ 8) at columns 8 w + 2 t and + 1 (counts below 2^16: the low halves of the accumulators)
+            uint16_t *wrow = wc16 + (size_t)i * kCvBins * kCvWS + g * kCvWS + 8 * warp + 2 * t;
+            if (m0) {
+                *(uint32_t *)wrow = __byte_perm((uint32_t)acc[0][0], (uint32_t)acc[0][1], 0x5410);
+                *(uint32_t *)(wrow + 8 * kCvWS) = __byte_perm((uint32_t)acc[0][2], (uint32_t)acc[0][3], 0x5410);
+            }
+            if (m1) {
+                *(uint32_t *)(wrow + 16 * kCvWS) = __byte_perm((uint32_t)acc[1][0], (uint32_t)acc[1][1], 0x5410);
+                *(uint32_t *)(wrow + 24 * kCvWS) = __byte_perm((uint32_t)acc[1][2], (uint32_t)acc[1][3], 0x5410);
+            }
+        };
+        auto window_counts = [&](int i, uint32_t need) {
+            switch (ks_hi - ks_lo) {  // the same for the whole warp
+            case 0: window_counts_n(std::integral_constant<int, 1>{}, i, need); break;
+            case 1: window_counts_n(std::integral_constant<int, 2>{}, i, need); break;
+            case 2: window_counts_n(std::integral_constant<int, 3>{}, i, need); break;
+            case 3: window_counts_n(std::integral_constant<int, 4>{}, i, need); break;
+            case 4: window_counts_n(std::integral_constant<int, 5>{}, i, need); break;
+            default: window_counts_n(std::integral_constant<int, 6>{}, i, need); break;
             }
         };
         const int ci = tid >> 6, cc = tid & (kCvTX - 1);  // this thread's pixel in a chunk
