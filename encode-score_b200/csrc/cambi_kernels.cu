@@ -36,7 +36,7 @@ constexpr int kP0T = 64;                    // output tile side
 constexpr int kP0C = kP0T + 12, kP0R = kP0T + 8;  // staged columns (76) and rows (72)
 constexpr int kP0F = kP0T + 6;              // flat pixels per side: x0-3 .. x0+66, y0-3 .. y0+66
 
-__global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ Prep0Batch b)
+__global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ Prep0Batch b)
 {
     __shared__ __align__(16) uint16_t raw[kP0R][kP0C];
     __shared__ __align__(16) uint16_t pre8[kP0R - 1][kP0C];
@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
     const bool feat = J.feat != nullptr;  // the same for the whole block
     if (x >= w && !feat) return;
     // flat count of the 7 columns around x in flat row 16 g + q (bit c of a row is column x - 3), and the horizontal
-    // mode of picture row y0 + 16 g - 1 + k (staged row 16 g + 2 + k); both recomputed as the window moves, so few
-    // registers stay live and more blocks share an SM
+    // mode of picture row y0 + 16 g - 1 + k (staged row 16 g + 2 + k), each made once as the window moves down and
+    // kept only while the window holds it, so few registers stay live and 5 blocks share an SM
     const int kw = c >> 5, sh = c & 31;
     auto h7 = [&](int q) { return __popc(__funnelshift_r(flatbits[16 * g + q][kw], flatbits[16 * g + q][kw + 1], sh) & 0x7Fu); };
     const bool edge_x = x == 0 || x == w - 1;
@@ -123,9 +123,12 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
         const uint16_t *row = pre[16 * g + 2 + k];
         return edge_x ? row[c + 4] : mode3(row[c + 3], row[c + 4], row[c + 5]);
     };
-    int cnt = 0;
+    int cnt = 0, hv[22];  // hv[q] = h7(q), each kept for the 7 rows of the window it enters
 #pragma unroll
-    for (int q = 0; q < 6; q++) cnt += h7(q);
+    for (int q = 0; q < 6; q++) {
+        hv[q] = h7(q);
+        cnt += hv[q];
+    }
     uint16_t m0 = hmode(0), m1 = hmode(1);
     // features of the 4 x 4 blocks (the proposal's block_features): value sum, masked and counted pixels of this
     // column's 4 rows, then summed over the block's 4 columns (lanes c .. c + 3 of one warp)
@@ -133,9 +136,10 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
     bool need = false;
     const bool need_range = b.need_span >= 0;
     const unsigned need_lo = (unsigned)b.need_lo, need_span = (unsigned)b.need_span;
-#pragma unroll 4
+#pragma unroll
     for (int i = 0; i < 16; i++) {
-        cnt += h7(i + 6);
+        hv[i + 6] = h7(i + 6);
+        cnt += hv[i + 6];
         const uint16_t m2 = hmode(i + 2);
         const int y = y0 + 16 * g + i;
         if (y < h && x < w) {
@@ -152,7 +156,7 @@ __global__ void __launch_bounds__(256, 6) prep0_kernel(const __grid_constant__ P
                 }
             }
         }
-        cnt -= h7(i);
+        cnt -= hv[i];
         m0 = m1;
         m1 = m2;
         if (feat && (i & 3) == 3) {

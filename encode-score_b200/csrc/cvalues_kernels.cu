@@ -341,23 +341,36 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         if (tid < kCvTY) rowneed[tid] = 0;
         for (int i = tid; i < kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
         __syncthreads();
-        // the pass ranks each row's pixels read: a warp covers 32 pixels of one row
-        for (int i = tid; i < kCvTY * kCvTX; i += kCvThreads) {
-            const int r = i >> 6, c = i & (kCvTX - 1);
-            uint32_t need = 0;
-            if (r < rows && c < cols) {
-                const unsigned v = rplane[(r + P) * CS + c + P];
-                if (v != kNoRank) {
+        // the pass ranks each row's pixels read: first the served pass ranks present in each row (16 lanes per row, 4
+        // pixels per lane from two aligned words of the rank plane), then, per row, the ranks those read
+        for (int i = tid; i < kCvTY * (kCvTX / 4); i += kCvThreads) {
+            const int r = i >> 4, q = i & 15;
+            uint32_t bits = 0;
+            if (r < rows) {
+                const int at = (r + P) * CS + P + 4 * q;  // tile columns 4 q .. 4 q + 3
+                const uint32_t *wp = (const uint32_t *)(rplane + (at & ~3));
+                const uint32_t quad = __funnelshift_r(wp[0], wp[1], 8 * (at & 3));
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const unsigned v = (quad >> (8 * e)) & 0xFFu;
                     const int k = (int)v - off, rk = b0 + k;
-                    if (rk >= lo && rk < hi) {
-                        const uint32_t m = relneed[rk];
-                        const int sh = k - 4;
-                        need = sh >= 0 ? m << sh : m >> -sh;
-                    }
+                    if (v != kNoRank && 4 * q + e < cols && rk >= lo && rk < hi) bits |= 1u << k;
                 }
             }
-            need = __reduce_or_sync(kFull, need);
-            if (lane == 0 && need) atomicOr(&rowneed[r], need);
+#pragma unroll
+            for (int o = 8; o; o >>= 1) bits |= __shfl_xor_sync(kFull, bits, o);
+            if ((lane & 15) == 0 && r < kCvTY) rowneed[r] = bits;
+        }
+        __syncthreads();
+        if (tid < rows) {
+            uint32_t present = rowneed[tid], need = 0;
+            while (present) {
+                const int k = __ffs(present) - 1;
+                present &= present - 1;
+                const uint32_t m = relneed[b0 + k];
+                need |= k >= 4 ? m << (k - 4) : m >> (4 - k);
+            }
+            rowneed[tid] = need;
         }
         __syncthreads();
         const bool pass_any = __syncthreads_or(tid < kCvTY && rowneed[tid] != 0);
