@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
     const int lane = tid & 31, warp = tid >> 5;
     const int x0 = (t % J.tiles_x) * kP0T, y0 = (t / J.tiles_x) * kP0T;
     const int xs = x0 - 4, ys = y0 - 3;
-    if (J.feat) {  // the codes that need c-values, bit c of word c / 32 (warp w makes words w, w + 8, ...)
+    if (J.feat && b.need_span < 0) {  // the codes that need c-values when they are no single range: bit c of word
+                                      // c / 32 (warp w makes words w, w + 8, ...)
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const int code = (warp + 8 * k) * 32 + lane;
@@ -72,7 +73,6 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
     __syncthreads();
     // preprocessed values of x0-4 .. x0+71, y0-3 .. y0+67: an 8-bit plane at 10 bits, the mean of the 2 x 2 block to
     // the lower right (pairs on the last row and column); a 10-bit plane as staged (0 outside the picture)
-    const uint16_t(*pre)[kP0C] = raw;
     if (J.depth == 8) {
         for (int i = tid; i < (kP0R - 1) * (kP0C - 1); i += 256) {
             const int r = i / (kP0C - 1), c = i - r * (kP0C - 1), x = xs + c, y = ys + r;
@@ -88,8 +88,14 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
             pre8[r][c] = (uint16_t)v;
         }
         __syncthreads();
-        pre = pre8;
+        // back into the staged plane, so every later read names one shared array (32-bit shared addressing)
+        for (int i = tid; i < (kP0R - 1) * (kP0C - 1); i += 256) {
+            const int r = i / (kP0C - 1), c = i - r * (kP0C - 1);
+            raw[r][c] = pre8[r][c];
+        }
+        __syncthreads();
     }
+    auto &pre = raw;
     // flat: equal to the right and lower neighbours (the last column / row count as equal); nothing outside
     const bool interior = x0 >= 3 && x0 + kP0T + 3 < w && y0 >= 3 && y0 + kP0T + 3 < h;
     for (int q = warp; q < kP0F; q += 8) {
@@ -165,8 +171,11 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
             const int fw = (w + 3) / 4, fh = (h + 3) / 4, u = x >> 2, v4 = (y0 + 16 * g + i - 3) >> 2;
             if ((c & 3) == 0 && u < fw && v4 < fh) {
                 const unsigned fsum = fpack & 0xFFFFu, fmask = (fpack >> 16) & 0xFFu, fn = fpack >> 24;
-                J.feat[(size_t)v4 * fw + u] = make_float2(fn ? (float)(((double)fsum / (double)fn - 512.0) / 256.0) : 0.0f,
-                                                          (float)((double)fmask / 16.0));
+                // (sum / n - 512) / 256 rounded once to float; for a whole block (n = 16) every step is exact in
+                // float, so the double path is needed only at the picture's edges
+                const float f0 = fn == 16 ? __fmul_rn(__fsub_rn(__fmul_rn((float)fsum, 0.0625f), 512.0f), 0.00390625f)
+                                          : fn ? (float)(((double)fsum / (double)fn - 512.0) / 256.0) : 0.0f;
+                J.feat[(size_t)v4 * fw + u] = make_float2(f0, __fmul_rn((float)fmask, 0.0625f));
             }
             fpack = 0;
         }
@@ -276,7 +285,21 @@ __global__ void __launch_bounds__(kSelThreads) select_hist_kernel(CvSlot *slots,
             last = d;
             run = 1;
         };
-        for (unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n4; i += stride) {
+        // four 16-byte loads in flight per thread, then the rest one by one
+        unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x;
+        for (; i + 3 * stride < n4; i += 4 * stride) {
+            uint4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) q[u] = __ldg((const uint4 *)v + i + u * stride);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                add(q[u].x);
+                add(q[u].y);
+                add(q[u].z);
+                add(q[u].w);
+            }
+        }
+        for (; i < n4; i += stride) {
             const uint4 q = __ldg((const uint4 *)v + i);
             add(q.x);
             add(q.y);
@@ -338,7 +361,21 @@ __global__ void __launch_bounds__(kSelThreads) sum_above_kernel(CvSlot *slots, i
                 c++;
             }
         };
-        for (unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n4; i += stride) {
+        // four 16-byte loads in flight per thread, then the rest one by one
+        unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x;
+        for (; i + 3 * stride < n4; i += 4 * stride) {
+            float4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) q[u] = __ldg((const float4 *)S.list + i + u * stride);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                add(q[u].x);
+                add(q[u].y);
+                add(q[u].z);
+                add(q[u].w);
+            }
+        }
+        for (; i < n4; i += stride) {
             const float4 q = __ldg((const float4 *)S.list + i);
             add(q.x);
             add(q.y);
