@@ -271,14 +271,13 @@ __global__ void net_adam_kernel(float *P, float *R, const float *G, float *M, fl
 // Inference: one block of 128 threads per scale-0 tile, all four layers in shared memory.
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kPT = 128;
-constexpr int kPredBlocks = 148 * 4;  // persistent grid: 4 blocks of 46 KB per SM
+constexpr int kPredBlocks = 148 * 5;  // persistent grid: 5 blocks of 34 KB per SM
 struct PredSmem {
     uint32_t f[kFeatTile * kFeatTile][2];         // features per pixel: (head, remainder) bfloat16 pairs of channels 0, 1
     float b0[16], w3[145];                        // layer 0's biases; layer 3's weights then bias (bfloat16 values)
     float b12[2][16];
     __align__(16) uint32_t a1[22 * 22 * 8];       // layer-0 output, [pixel][16 channels] bfloat16; later layer 2's
     __align__(16) uint32_t a2[20 * 20 * 8];       // layer-1 output
-    uint32_t frags[kNetFrags];                    // B fragments of layers 1, 2 and 3
     float part[kPT / 32];
 };
 
@@ -417,7 +416,7 @@ __device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *fr
 
 // Persistent: each block loads the parameters once, then takes tiles from a counter (need[total_tiles]) until none
 // is left.
-__global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ PredBatch b)
+__global__ void __launch_bounds__(kPT, 5) predict_kernel(const __grid_constant__ PredBatch b)
 {
     __shared__ PredSmem sm;
     __shared__ int next;
@@ -425,7 +424,6 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
     if (tid < 16) sm.b0[tid] = b.params[net_b(0) + tid];
     for (int i = tid; i < 145; i += kPT) sm.w3[i] = b.params[net_w(3) + i];
     if (tid < 32) sm.b12[tid >> 4][tid & 15] = b.params[(tid < 16 ? net_b(1) : net_b(2)) + (tid & 15)];
-    for (int i = tid; i < kNetFrags; i += kPT) sm.frags[i] = b.frags[i];
     for (;;) {
         __syncthreads();  // every thread is done with the previous tile (and with `next`)
         if (tid == 0) next = (int)atomicAdd(b.need + b.total_tiles, 1u);
@@ -451,14 +449,15 @@ __global__ void __launch_bounds__(kPT) predict_kernel(const __grid_constant__ Pr
             sm.f[i][1] = pack_bf16(f.x - h0, f.y - h1);  // the remainders are exact in FP32
         }
         __syncthreads();
-        mma_layer0(sm.f, sm.a1, sm.frags + kNetFrags3, sm.b0);                  // layer 0: 22 x 22
+        // the B fragments come from global memory (L1-resident: 13 KB for all blocks), leaving shared memory to the planes
+        mma_layer0(sm.f, sm.a1, b.frags + kNetFrags3, sm.b0);                   // layer 0: 22 x 22
         __syncthreads();
-        mma_layer(sm.a1, 22, sm.a2, 20, sm.frags, sm.b12[0]);                   // layer 1: 20 x 20
+        mma_layer(sm.a1, 22, sm.a2, 20, b.frags, sm.b12[0]);                    // layer 1: 20 x 20
         __syncthreads();
-        mma_layer(sm.a2, 20, sm.a1, 18, sm.frags + 9 * 2 * 2 * 32, sm.b12[1]);  // layer 2: 18 x 18, into a1
+        mma_layer(sm.a2, 20, sm.a1, 18, b.frags + 9 * 2 * 2 * 32, sm.b12[1]);   // layer 2: 18 x 18, into a1
         __syncthreads();
         // layer 3: 16 -> 1 on 16 x 16 (tensor cores), then the tile mean (a fixed order of additions)
-        const float s = mma_head(sm.a1, sm.frags + kNetFrags12);
+        const float s = mma_head(sm.a1, b.frags + kNetFrags12);
         if ((tid & 31) == 0) sm.part[tid >> 5] = s;
         __syncthreads();
         if (tid == 0) b.pred[gt] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f + sm.w3[144];
