@@ -55,14 +55,16 @@ __host__ __device__ inline CvLayout cv_layout(int pad)
 {
     const size_t rh = (size_t)kCvTY + 2 * pad;
     CvLayout l;
+    // the rank plane, window counts and column counts first: until the plane is built they hold the region's band
+    // codes (16 bits each) when those fit
     l.rplane = 0;
-    l.rank = align16(l.rplane + rh * cv_cs(pad));
+    l.wcount = align16(l.rplane + rh * cv_cs(pad));
+    l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * kCvWS * 2);
+    l.rank = align16(l.cols + (size_t)kCvBins * cv_cstr(pad));
     l.rcode = align16(l.rank + (size_t)kMaxBand * 2);
     l.nbr = align16(l.rcode + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
-    l.wcount = align16(l.relneed + (size_t)kMaxBand * 2);
-    l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * kCvWS * 2);
-    l.list = align16(l.cols + (size_t)kCvBins * cv_cstr(pad));
+    l.list = align16(l.relneed + (size_t)kMaxBand * 2);
     l.total = align16(l.list + (size_t)kListCap * 4);
     return l;
 }
@@ -184,13 +186,20 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             }
         }
     };
-    // 2. the codes the region holds (occ) and the codes own pixels need (srv), 8 elements per thread and step
+    // 2. the codes the region holds (occ) and the codes own pixels need (srv), 8 elements per thread and step; the codes
+    // themselves are kept in shared memory (row r, vector v at 16-bit element r S + 8 v) when they fit below the rank
+    // tables, so the rank plane is built without a second read of the scale
+    uint16_t *codes16 = (uint16_t *)(smem + L.rplane);
+    const bool staged = (size_t)RH * S * 2 <= L.rank;
     {
         const int nv = S >> 3, total = RH * nv;
         for (int i = tid; i < total; i += kCvThreads) {
             const int r = i / nv, v = i - r * nv, xv = xs + 8 * v;
             uint16_t cs[8];
             load8(r, v, cs);
+            if (staged)
+                ((uint4 *)codes16)[i] = make_uint4(cs[0] | ((uint32_t)cs[1] << 16), cs[2] | ((uint32_t)cs[3] << 16),
+                                                   cs[4] | ((uint32_t)cs[5] << 16), cs[6] | ((uint32_t)cs[7] << 16));
             const bool row_in_tile = r >= P && r < P + rows;
             uint16_t prev = kNone, prev_srv = kNone;
 #pragma unroll
@@ -292,7 +301,32 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             }
         }
     };
-    if (!per_pass) build_plane(-1);
+    if (!per_pass && staged) {
+        // the codes, vector by vector, into 8-bit ranks in place: the rank bytes of vector i (row r, bytes r CS + 8 v
+        // + k - ox) lie within the code bytes of vector i or of earlier ones (16 i + 15 at most, as CS <= 2 S), so a
+        // step's writes only cover codes read before its barrier; every region column gets a rank or kNoRank
+        const int nv = S >> 3, total = RH * nv;
+        for (int c0 = 0; c0 < total; c0 += kCvThreads) {
+            const int i = c0 + tid;
+            uint4 q = make_uint4(0, 0, 0, 0);
+            if (i < total) q = ((const uint4 *)codes16)[i];
+            __syncthreads();
+            if (i < total) {
+                const int r = i / nv, v = i - r * nv;
+                const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int j = 8 * v + k - ox;  // region column
+                    if (j < 0 || j >= RW) continue;
+                    const uint16_t code = (uint16_t)(wv[k >> 1] >> (16 * (k & 1)));
+                    const unsigned rk = code == kNone ? kNoRank : rank[code];
+                    rplane[r * CS + j] = (uint8_t)(rk == kNone ? kNoRank : rk);
+                }
+            }
+        }
+    } else if (!per_pass) {
+        build_plane(-1);
+    }
     __syncthreads();
 
     unsigned long long my_sum = 0;
