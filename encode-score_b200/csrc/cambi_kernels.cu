@@ -17,11 +17,13 @@
 namespace es {
 namespace {
 
+// The mode of three values (the smallest when all differ), as selects rather than branches: neighbouring pixels of a
+// warp take different cases.
 __device__ __forceinline__ uint16_t mode3(uint16_t a, uint16_t b, uint16_t c)
 {
-    if (a == b || a == c) return a;
-    if (b == c) return b;
-    return min(a, min(b, c));
+    const unsigned mn = min((unsigned)a, min((unsigned)b, (unsigned)c));
+    const unsigned bc = b == c ? (unsigned)b : mn;
+    return (uint16_t)((a == b || a == c) ? (unsigned)a : bc);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
