@@ -205,8 +205,9 @@ class CpuSampler:
 
     def sample(self) -> tuple[float, str]:
         h = WORKLOADS[self.wl]["h"]
-        jobs = [(self.wl, 1000 + (self.round * self.n + i) // (h // STRIP_ROWS), ((self.round * self.n + i) % (h // STRIP_ROWS)) * STRIP_ROWS,
-                 STRIP_ROWS) for i in range(self.n)]
+        # the strips of one frame step, in turn (each process makes the step once and keeps it, so later rounds time the
+        # oracle alone and the run's wall time stays short)
+        jobs = [(self.wl, 1000, ((self.round * self.n + i) % (h // STRIP_ROWS)) * STRIP_ROWS, STRIP_ROWS) for i in range(self.n)]
         self.round += 1
         res = self.pool.map(cpu_strip, jobs, chunksize=1)
         busy = max(r[1] for r in res)  # the processes run side by side; frame generation is not timed
