@@ -70,7 +70,8 @@ struct es_batch {
     PinnedBuffer<double> h_scores[2];
     DeviceBuffer<UnpackView> views;
     PinnedBuffer<UnpackView> h_views[2];
-    Stream main, side;
+    // the CAMBI chain, the longer one, runs at the higher priority; the texture chain fills the SMs beside it
+    Stream main{true}, side{false};
     Event start, fork, join, done[2];
     bool use_graphs = true;
     struct Step {
@@ -598,7 +599,7 @@ void queue_step(es_batch &b, long f, uint32_t skip)
             }
         }
         cudaGraphExec_t exec = nullptr;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         cuda_check(e, "instantiating a step graph");
         it = b.graphs.emplace(key, es_batch::Step{exec, kernels}).first;

@@ -25,7 +25,7 @@ struct es_cambi {
     DeviceBuffer<float> lut;
     DeviceBuffer<double> score;  // score, then pooled per scale
     PinnedBuffer<double> host;
-    Stream stream;
+    Stream stream{true};  // CAMBI is the longer chain of a frame step: it runs at the higher priority
     Event copied, finished;
     float *planes[kScales] = {};
     unsigned long long *tile_mass = nullptr;

@@ -106,6 +106,13 @@ struct PinnedBuffer {
 struct Stream {
     cudaStream_t s = nullptr;
     Stream() { cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "creating a stream"); }
+    // high: the device's greatest stream priority, else its least
+    explicit Stream(bool high)
+    {
+        int least = 0, greatest = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "reading stream priorities");
+        cuda_check(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high ? greatest : least), "creating a stream");
+    }
     ~Stream() { if (s) cudaStreamDestroy(s); }
     Stream(const Stream &) = delete;
 };
