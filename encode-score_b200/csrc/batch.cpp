@@ -71,8 +71,8 @@ struct es_batch {
     DeviceBuffer<UnpackView> views;
     PinnedBuffer<UnpackView> h_views[2];
     // the CAMBI chain, the longer one, runs at the higher priority; the texture chain fills the SMs beside it
-    Stream main{true}, side{false};
-    Event start, fork, join, done[2];
+    Stream main{true}, side{false}, aux{true};  // aux: the proposal's lists beside the decimation
+    Event start, fork, join, done[2], fork_aux, join_aux;
     bool use_graphs = true;
     struct Step {
         cudaGraphExec_t exec;
@@ -230,10 +230,12 @@ uint16_t *luma_of(const es_batch &b, int picture, long f)
 // The c-values of a step with the learned proposal: predictions of every scale-0 tile, the tile lists, the proposed
 // and audited tiles, the audit, then the skipped tiles of the pictures whose audit asks for the fallback. `run` lists
 // the pictures whose CAMBI runs; cb is the step's c-value job table (scales 0-4 of each, in that order).
-void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cudaStream_t s)
+// The proposal of a step up to its tile lists: features come with scale 0, then the prediction, the optional budget
+// and the lists. Needs scale 0 only, so it runs beside the decimation of scales 1-4. Returns the audit's table.
+AuditBatch record_proposal_lists(es_batch &b, const std::vector<int> &run, CvBatch &cb, cudaStream_t s)
 {
     const int np = (int)run.size();
-    unsigned *count_a = b.counters.ptr, *count_b = count_a + 1, *next_a = count_a + 2, *next_b = count_a + 3;
+    unsigned *count_a = b.counters.ptr, *count_b = count_a + 1;
     unsigned *n_audit = count_a + 4, *n_skip = n_audit + kMaxJobs;
     cuda_check(cudaMemsetAsync(b.counters.ptr, 0, b.counters.bytes(), s), "clearing proposal counters");
     PredBatch pb{};
@@ -321,8 +323,16 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
     qb.n_audit = n_audit;
     qb.n_skip = n_skip;
     cuda_check(launch_propose(qb, s), "tile proposal");
+    return ab;
+}
+
+// The c-values of the proposed and audited tiles, the audit, and the skipped tiles of the pictures that fall back.
+void record_proposal_cvalues(es_batch &b, const CvBatch &cb, AuditBatch ab, cudaStream_t s)
+{
+    unsigned *count_a = b.counters.ptr, *count_b = count_a + 1, *next_a = count_a + 2, *next_b = count_a + 3;
+    unsigned *n_audit = count_a + 4, *n_skip = n_audit + kMaxJobs;
     CvBatch ca = cb;
-    ca.tiles = qb.list_a;
+    ca.tiles = b.lists.ptr;
     ca.tile_count = count_a;
     ca.tile_next = next_a;
     ca.tile_mass = b.tile_mass.ptr;
@@ -336,7 +346,7 @@ void record_proposal(es_batch &b, const std::vector<int> &run, CvBatch &cb, cuda
     ab.stats = b.stats.ptr;
     cuda_check(launch_audit(ab, s), "tile audit");
     CvBatch cf = cb;
-    cf.tiles = qb.list_b;
+    cf.tiles = b.lists.ptr + b.total_tiles;
     cf.tile_count = count_b;
     cf.tile_next = next_b;
     cf.run = b.run_flags.ptr;
@@ -373,26 +383,6 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
     }
     pb.band = band;
     cuda_check(launch_prep0(pb, s), "batch scale 0");
-    const int nslots = (int)b.pictures.size() * kScales;
-    cuda_check(launch_slots_reset(b.slots.ptr, nslots, b.slot_n.ptr, b.slot_k.ptr, s), "batch reset");
-    for (int sc = 1; sc < kScales; sc++) {
-        DecBatch db{};
-        int blocks = 0;
-        for (int i : run) {
-            const Picture &pic = *b.pictures[i];
-            DecJob &dj = db.job[db.njobs++];
-            dj.src = pic.words[sc - 1].ptr;
-            dj.sw = pic.sw[sc - 1];
-            dj.sh = pic.sh[sc - 1];
-            dj.dst = pic.words[sc].ptr;
-            dj.w = pic.sw[sc];
-            dj.h = pic.sh[sc];
-            dj.first_block = blocks;
-            blocks += (dj.w * dj.h + 255) / 256;
-        }
-        db.total_blocks = blocks;
-        cuda_check(launch_decimate_mode(db, s), "batch scales");
-    }
     CvBatch cb{};
     int tiles = 0;
     for (int i : run) {
@@ -416,10 +406,43 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
     cb.band = band;
     cb.lut = b.lut.ptr;
     cb.slots = b.slots.ptr;
+    // with the proposal, its lists are made beside the decimation (they need scale 0 only)
+    const bool split = !serial_streams();
+    AuditBatch ab{};
+    if (b.net) {
+        cudaStream_t a = split ? b.aux.s : s;
+        if (split) {
+            cuda_check(cudaEventRecord(b.fork_aux.e, s), "event");
+            cuda_check(cudaStreamWaitEvent(a, b.fork_aux.e, 0), "event");
+        }
+        ab = record_proposal_lists(b, run, cb, a);
+        if (split) cuda_check(cudaEventRecord(b.join_aux.e, a), "event");
+    }
+    const int nslots = (int)b.pictures.size() * kScales;
+    cuda_check(launch_slots_reset(b.slots.ptr, nslots, b.slot_n.ptr, b.slot_k.ptr, s), "batch reset");
+    for (int sc = 1; sc < kScales; sc++) {
+        DecBatch db{};
+        int blocks = 0;
+        for (int i : run) {
+            const Picture &pic = *b.pictures[i];
+            DecJob &dj = db.job[db.njobs++];
+            dj.src = pic.words[sc - 1].ptr;
+            dj.sw = pic.sw[sc - 1];
+            dj.sh = pic.sh[sc - 1];
+            dj.dst = pic.words[sc].ptr;
+            dj.w = pic.sw[sc];
+            dj.h = pic.sh[sc];
+            dj.first_block = blocks;
+            blocks += (dj.w * dj.h + 255) / 256;
+        }
+        db.total_blocks = blocks;
+        cuda_check(launch_decimate_mode(db, s), "batch scales");
+    }
     if (!b.net) {
         cuda_check(launch_cvalues(cb, s), "batch c-values");
     } else {
-        record_proposal(b, run, cb, s);
+        if (split) cuda_check(cudaStreamWaitEvent(s, b.join_aux.e, 0), "event");
+        record_proposal_cvalues(b, cb, ab, s);
     }
     static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
     for (int round = 0; round < 3; round++)
