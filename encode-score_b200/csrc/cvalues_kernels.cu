@@ -8,8 +8,8 @@
 //     margins are read with 16-byte loads from an 8-pixel-aligned start; the codes that can matter -- occurring within
 //     kDiffs of a code whose c-value is needed -- are ranked in order, each rank gets its code, the rank offsets of
 //     its 8 neighbour codes and the mask of ranks its c-value reads (tiles where no code has a neighbour code leave:
-//     their c-values are all 0), and a second read of the codes makes the region a shared-memory plane of 8-bit
-//     ranks;
+//     their c-values are all 0); the codes, kept as 16-bit values in the shared memory that later holds the rank
+//     plane and the counts (when the region fits there; else read again), become a plane of 8-bit ranks in place;
 //  3. per pass over 32 ranks, the ranks' column counts (8 bits per column and rank: pixels of the 2 pad + 1 window rows)
 //     sit in shared memory as a 32 x region-width byte matrix and slide down the rows (the leaving and entering row's
 //     rank per column); on rows whose pixels read the pass's ranks, the window counts of the 64 tile columns are one
