@@ -108,6 +108,7 @@ def main() -> None:
     ap.add_argument("--budget", type=float, default=None, help="score budget of the skipped tiles (default: the network's)")
     ap.add_argument("--tolerance", type=float, default=0.025)
     ap.add_argument("--sweep", default=None, help="budget,tolerance pairs 'b:t,b:t,...' to evaluate instead of one setting")
+    ap.add_argument("--thresholds", default=None, help="thresholds 't,t,...' to evaluate instead of the network's")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
 
@@ -120,6 +121,18 @@ def main() -> None:
     net, meta = load_net(es_b200, args.net)
     t0 = time.time()
     budget = meta.get("skip_budget", 0.0) if args.budget is None else args.budget
+    if args.thresholds:
+        out = {"seed": args.seed, "frames": args.frames, "thresholds": []}
+        for t in (float(v) for v in args.thresholds.split(",")):
+            rows, timing = run(torch, es_b200, module, args.frames, args.seed, net, t, tolerance=args.tolerance, budget=budget)
+            out["thresholds"].append({"threshold": t, **summarize(rows, timing)})
+            print(json.dumps(out["thresholds"][-1]), flush=True)
+        net.close()
+        module.close()
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(json.dumps(out, indent=1))
+        return
     if args.sweep:
         out = {"threshold": meta["threshold"], "sweep": []}
         for item in args.sweep.split(","):
