@@ -10,7 +10,8 @@ lasting-texture figures, PSNR and color, and the per-frame reduction into per-se
   so consecutive steps do not hit L2), timed with CUDA events on the queueing stream; a step's done event also waits
   for the CAMBI streams.
 * ``e2e``: the same through the C ABI with the inputs in pinned host memory, copied host-to-device every step on a copy
-  stream (double-buffered) and the figures read back, inside the timed region.
+  stream (three input slots, each step's copy queued one step ahead) and the figures read back, inside the timed
+  region.
 * ``roofline``: the kernel with the most device time: its algorithmic bytes per launch (algorithmic_bytes) over its
   mean duration, against the measured HBM copy bandwidth. Durations come from a pass over the pool after the timed
   region with every kernel alone on the stream and bracketed by CUDA events (``kernels`` lists them all).
@@ -568,7 +569,11 @@ def main() -> None:
             for pic in [step.source] + step.encodes:
                 pics.append([torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).pin_memory() for a in (pic.y, pic.u, pic.v)])
             host_pool.append(pics)
-        slots = [[[torch.empty_like(t, device="cuda") for t in pic] for pic in host_pool[0]] for _ in range(2)]
+        # three input slots: step g + 1's copy is queued before step g - 1 is collected, so the copy stream never waits
+        # for the host (with two slots and the copy queued after the collect, the host's collect time left the copy
+        # engine idle for a fifth of each step)
+        depth = 3
+        slots = [[[torch.empty_like(t, device="cuda") for t in pic] for pic in host_pool[0]] for _ in range(depth)]
         views = [[es_b200.FrameView(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(), w * 2, w, 0, 2, 0, pic.depth)
                   for p, pic in zip(slot, [pool[0].source] + pool[0].encodes)] for slot in slots]
         h2d = sum(t.numel() * t.element_size() for pic in host_pool[0] for t in pic)
@@ -577,28 +582,36 @@ def main() -> None:
         fr2 = {"plain": PlainForm, "batched": BatchedForm, "learned": LearnedForm}[head]()
         acc2 = [es_b200.new_accum() for _ in range(n_enc)]
         copy_stream = torch.cuda.Stream()
-        copied = [torch.cuda.Event() for _ in range(2)]
-        free = [torch.cuda.Event() for _ in range(2)]
+        copied = [torch.cuda.Event() for _ in range(depth)]
+        free = [torch.cuda.Event() for _ in range(depth)]
 
-        def e2e_step(g, collect_prev):
-            s = g % 2
-            src = host_pool[g % len(host_pool)]
+        def copy_in(g):
+            s = g % depth
             with torch.cuda.stream(copy_stream):
-                copy_stream.wait_event(free[s])
-                for dst_pic, src_pic in zip(slots[s], src):
+                copy_stream.wait_event(free[s])  # the step that last read this slot is done
+                for dst_pic, src_pic in zip(slots[s], host_pool[g % len(host_pool)]):
                     for d, hsrc in zip(dst_pic, src_pic):
                         d.copy_(hsrc, non_blocking=True)
                 copied[s].record(copy_stream)
+
+        def e2e_step(g, g_first, g_end):
+            """Step g of the run g_first .. g_end - 1: its frames' copy (queued one step ahead), its launches, and the
+            collect of step g - 1."""
+            s = g % depth
+            if g == g_first:
+                copy_in(g)
+            if g + 1 < g_end:
+                copy_in(g + 1)
             stream.wait_event(copied[s])
             fr2.queue(g, views[s], stream.cuda_stream)
             free[s].record(stream)
-            if collect_prev:
+            if g > g_first:
                 fr2.collect(g - 1, acc2)
 
         with torch.cuda.stream(stream):
             warm = max(args.warmup, 28)
             for g in range(warm):
-                e2e_step(g, g > 0)
+                e2e_step(g, 0, warm)
             fr2.collect(warm - 1, acc2)
             barrier()
             torch.cuda.synchronize()
@@ -606,8 +619,8 @@ def main() -> None:
             t_start.record(stream)
             copy_stream.wait_event(t_start)
             g0 = warm
-            for k in range(args.steps):
-                e2e_step(g0 + k, k > 0)
+            for k in range(args.steps):  # exactly steps copies, steps launch sets and steps collects in the region
+                e2e_step(g0 + k, g0, g0 + args.steps)
             fr2.collect(g0 + args.steps - 1, acc2)
             t_end.record(stream)
             t_end.synchronize()
