@@ -515,6 +515,7 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kCT = 1024;  // threshold block
 constexpr int kCW = 256;   // windows per block
+constexpr int kThreshStage = 40960;  // oriented figures a threshold block stages in shared memory (160 KB)
 __host__ __device__ inline int collect_blocks_dev(int windows) { return (windows + kCW - 1) / kCW; }
 
 __device__ __forceinline__ uint16_t hist_bin(double pct)
@@ -523,27 +524,33 @@ __device__ __forceinline__ uint16_t hist_bin(double pct)
     return (uint16_t)llround(__ddiv_rn(__dadd_rn(c, 500.0), 0.05));
 }
 
-// The t-th smallest (0-based) of the non-negative floats v[i * stride] (their bit patterns order as the values).
-__device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, unsigned *hist)
+// The rank-th smallest (0-based) of the non-negative floats v[i * stride] (their bit patterns order as the values), by
+// three radix rounds of 11, 11 and 10 bits; each warp adds the lanes that share a digit with one atomic.
+__device__ unsigned select_kth(const float *v, int n, int stride, unsigned rank, unsigned *hist)
 {
     __shared__ unsigned s_prefix, s_mask, s_rem;
     __shared__ unsigned warp_tot[kCT / 32];
-    if (threadIdx.x == 0) { s_prefix = 0; s_mask = 0; s_rem = t; }
-    const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { s_prefix = 0; s_mask = 0; s_rem = rank; }
     for (int round = 0; round < 3; round++) {
-        const int shift = shifts[round], nb = 1 << widths[round];
-        for (int i = threadIdx.x; i < 2048; i += kCT) hist[i] = 0;
+        const int shift = round == 0 ? 21 : round == 1 ? 10 : 0, nb = round == 2 ? 1024 : 2048;
+        for (int i = tid; i < 2048; i += kCT) hist[i] = 0;
         __syncthreads();
         const unsigned prefix = s_prefix, mask = s_mask;
-        for (int i = threadIdx.x; i < n; i += kCT) {
-            const unsigned bits = __float_as_uint(v[(size_t)i * stride]);
-            if ((bits & mask) == prefix) atomicAdd(&hist[(bits >> shift) & (unsigned)(nb - 1)], 1u);
+        for (int i0 = tid - lane; i0 < n; i0 += kCT) {  // the same trip count for every lane of a warp
+            const int i = i0 + lane;
+            const unsigned bits = i < n ? __float_as_uint(v[(size_t)i * stride]) : 0u;
+            const bool in = i < n && (bits & mask) == prefix;
+            if (!__any_sync(0xffffffffu, in)) continue;  // after the first round most warps hold no candidate
+            const unsigned d = in ? (bits >> shift) & (unsigned)(nb - 1) : 0xFFFFFFFFu;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (in && lane == __ffs(peers) - 1) atomicAdd(&hist[d], (unsigned)__popc(peers));
         }
         __syncthreads();
         // the digit holding the rem-th smallest: thread t sums digits [t per, t per + per), a block scan places it
-        const int per = nb / kCT, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+        const int per = nb / kCT;
         unsigned local = 0;
-        for (int k = 0; k < per; k++) local += hist[t * per + k];
+        for (int k = 0; k < per; k++) local += hist[tid * per + k];
         unsigned incl = local;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -559,7 +566,7 @@ __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, un
         __syncthreads();
         if (excl <= rem && rem < incl) {
             unsigned below = excl;
-            int d = t * per;
+            int d = tid * per;
             while (below + hist[d] <= rem) below += hist[d++];
             s_rem = rem - below;
             s_prefix = prefix | ((unsigned)d << shift);
@@ -570,25 +577,62 @@ __device__ unsigned select_kth(const float *v, int n, int stride, unsigned t, un
     return s_prefix;
 }
 
-__global__ void __launch_bounds__(kCT) collect_threshold_kernel(const __grid_constant__ CollectBatch B)
+// The (rank + 1)-th smallest of the same floats, given bits a of the rank-th: a again when more than rank + 1 values
+// are at most a, otherwise the least value above a (one pass instead of three radix rounds).
+__device__ unsigned select_next(const float *v, int n, int stride, unsigned rank, unsigned a)
+{
+    __shared__ unsigned s_le, s_min;
+    if (threadIdx.x == 0) { s_le = 0; s_min = 0xFFFFFFFFu; }
+    __syncthreads();
+    unsigned le = 0, mn = 0xFFFFFFFFu;
+    for (int i = threadIdx.x; i < n; i += kCT) {
+        const unsigned bits = __float_as_uint(v[(size_t)i * stride]);
+        if (bits <= a) le++;
+        else mn = min(mn, bits);
+    }
+    le = __reduce_add_sync(0xffffffffu, le);
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&s_le, le);
+        atomicMin(&s_min, mn);
+    }
+    __syncthreads();
+    return s_le >= rank + 2 ? a : s_min;
+}
+
+// One block per source. With `staged` (every job has at most kThreshStage windows) the oriented figures, which sit
+// 8 floats apart in the figure array, are first gathered into dynamic shared memory, so the radix rounds and the
+// mask read them there.
+__global__ void __launch_bounds__(kCT) collect_threshold_kernel(const __grid_constant__ CollectBatch B, int staged)
 {
     __shared__ unsigned hist[2048];
+    extern __shared__ float stage[];
     const CollectJob &J = B.job[blockIdx.x];
     const float *st = J.stats[0];  // the source's oriented figures are the same in every encode's array
     const int n = J.windows;
+    const float *v = st + 6;
+    int stride = 8;
+    if (staged) {
+#pragma unroll 8
+        for (int i = threadIdx.x; i < n; i += kCT) stage[i] = __ldg(st + (size_t)i * 8 + 6);
+        __syncthreads();
+        v = stage;
+        stride = 1;
+    }
     // numpy's linear quantile at 0.8 of exact order statistics, in the reference's float / double arithmetic
     const double pos = 0.8 * (double)(n - 1);
     const unsigned lo = (unsigned)pos;
-    const float a = __uint_as_float(select_kth(st + 6, n, 8, lo, hist));
+    const unsigned a_bits = select_kth(v, n, stride, lo, hist);
+    const float a = __uint_as_float(a_bits);
     float q = a;
     if (lo + 1 < (unsigned)n) {
-        const float b = __uint_as_float(select_kth(st + 6, n, 8, lo + 1, hist));
+        const float b = __uint_as_float(select_next(v, n, stride, lo, a_bits));
         const float diff = __fsub_rn(b, a);
         q = __double2float_rn(__dadd_rn((double)a, __dmul_rn((double)diff, __dsub_rn(pos, (double)lo))));
     }
     if (threadIdx.x == 0) *J.threshold = q;
     for (int i = threadIdx.x; i < n; i += kCT) {
-        const float o = st[(size_t)i * 8 + 6];
+        const float o = v[(size_t)i * stride];
         J.mask[i] = o >= q && o > 0.0f;
     }
 }
@@ -663,15 +707,19 @@ __global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_const
     }
 }
 
-__global__ void collect_final_kernel(const __grid_constant__ CollectBatch B)
+// Warp k of an encode's block makes sum k: lane l adds the partials of blocks l, l + 32, ... in order, then a fixed
+// shuffle tree adds the 32 lane sums (the same order on every run).
+__global__ void __launch_bounds__(32 * kCollectSums) collect_final_kernel(const __grid_constant__ CollectBatch B)
 {
     int jb = 0;
     while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_enc) jb++;
     const CollectJob &J = B.job[jb];
-    const int e = blockIdx.x - J.first_enc, k = threadIdx.x, nblocks = collect_blocks_dev(J.windows);
-    if (k >= kCollectSums) return;
+    const int e = blockIdx.x - J.first_enc, k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nblocks = collect_blocks_dev(J.windows);
     double s = 0.0;
-    for (int b = 0; b < nblocks; b++) s += J.partials[((size_t)e * nblocks + b) * kCollectSums + k];
+    for (int b = lane; b < nblocks; b += 32) s += J.partials[((size_t)e * nblocks + b) * kCollectSums + k];
+    s = warp_sum(s);
+    if (lane != 0) return;
     FrameFigures *f = J.fig[e];
     if (k < 3) f->all_r[k] = s;
     else if (k < 6) f->all_d[k - 3] = s;
@@ -753,11 +801,17 @@ cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
         if (b.job[j].nenc <= 0 || b.job[j].windows <= 0) return cudaErrorInvalidValue;
     }
     if (encs == 0) return cudaSuccess;
+    int max_windows = 0;
+    for (int j = 0; j < b.njobs; j++) max_windows = max_windows > b.job[j].windows ? max_windows : b.job[j].windows;
+    const int staged = max_windows <= kThreshStage;
+    cudaError_t e = cudaFuncSetAttribute(collect_threshold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kThreshStage * (int)sizeof(float));
+    if (e != cudaSuccess) return e;
     {
         LaunchTimer t("frame_collect_threshold", s);
-        collect_threshold_kernel<<<b.njobs, kCT, 0, s>>>(b);
+        collect_threshold_kernel<<<b.njobs, kCT, staged ? (size_t)max_windows * sizeof(float) : 0, s>>>(b, staged);
     }
-    cudaError_t e = after_launch();
+    e = after_launch();
     if (e != cudaSuccess) return e;
     {
         LaunchTimer t("frame_collect_windows", s);
@@ -766,7 +820,7 @@ cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
     e = after_launch();
     if (e != cudaSuccess) return e;
     LaunchTimer t("frame_collect_final", s);
-    collect_final_kernel<<<encs, 32, 0, s>>>(b);
+    collect_final_kernel<<<encs, 32 * kCollectSums, 0, s>>>(b);
     return after_launch();
 }
 

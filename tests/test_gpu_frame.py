@@ -197,3 +197,49 @@ def test_frames_must_come_in_order_and_be_collected(cuda, module):
     with pytest.raises(es_b200.EsError):
         fr.collect(1, None, None)
     fr.close()
+
+
+def _striped_step(w, h, seed=11):
+    """A source whose right 70 % repeats one 16-pixel column profile (vertical stripes: the same oriented figure in
+    every window there, so the 0.8 quantile falls inside a run of equal values) beside faint grain; one blurred
+    encode."""
+    from scipy import ndimage
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    y = np.tile(rng.integers(200, 800, 16).astype(np.float32), (h, w // 16))
+    split = int(0.3 * (w // 16)) * 16
+    y[:, :split] = 500 + rng.normal(0, 2, (h, split))
+    src = np.clip(np.rint(y), 64, 940)
+    enc = np.clip(np.rint(ndimage.gaussian_filter(src, 1.0, mode="nearest")), 64, 940)
+    pic = lambda a: es_synth.Picture(a.astype(np.uint16), *(2 * [es_synth._chroma(a.astype(np.uint16))]), 10)
+    return es_synth.Step(pic(src), [pic(enc)])
+
+
+@pytest.mark.parametrize("w,h,kind", [(1920, 1088, "stripes"), (3840, 2160, "synth"), (4096, 2720, "synth"),
+                                      (4096, 2720, "stripes")])
+def test_structure_threshold_at_large_sizes(cuda, module, w, h, kind):
+    """The frame's structure threshold (the exact 0.8 quantile of the source's oriented figures) and mask against the
+    oracle's collect on the same window figures, with the figures staged in shared memory (up to 40960 windows) and
+    read in place (4096 x 2720: 43520 windows), on distinct figures and on a long run of equal ones."""
+    torch = cuda
+    step = es_synth.c2_step(0, w=w, h=h, n_encodes=1) if kind == "synth" else _striped_step(w, h)
+    fr = es_b200.Frame(module, w, h, 10, 1)
+    keep, views = es_b200.device_step(torch, step)
+    acc = [es_b200.new_accum()]
+    fr.queue(0, views[0], views[1:], torch.cuda.current_stream().cuda_stream)
+    res = fr.collect(0, acc, acc)
+    st, _ = fr.read_windows(0)
+    fr.close()
+    o = np.sort(st[:, 6])
+    lo = int(0.8 * (o.size - 1))
+    if kind == "stripes":  # the premise: the two order statistics that make the quantile are equal
+        assert o[lo] == o[lo + 1] and o[lo] > 0
+    want = oracle.Accum()
+    m = oracle.collect_frame(want, st)
+    assert res[0].structure_windows == int(m.sum())
+    for k in range(3):
+        assert np.array_equal(np.array(acc[0].amount[k].bins), want.amount[k].bins) and acc[0].amount[k].n == want.amount[k].n
+    for k in range(2):
+        assert np.array_equal(np.array(acc[0].matching[k].bins), want.matching[k].bins)
+    for name in ("st_r", "st_d", "sh_st_x"):
+        assert np.allclose(np.array(list(getattr(acc[0], name))), getattr(want, name), rtol=1e-12, atol=0), name
