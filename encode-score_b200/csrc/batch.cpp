@@ -72,7 +72,8 @@ struct es_batch {
     PinnedBuffer<UnpackView> h_views[2];
     // the CAMBI chain, the longer one, runs at the higher priority; the texture chain fills the SMs beside it
     Stream main{true}, side{false}, aux{true};  // aux: the proposal's lists beside the decimation
-    Event start, fork, join, done[2], fork_aux, join_aux;
+    Stream side2{false};                          // the structure threshold beside the lasting texture
+    Event start, fork, join, done[2], fork_aux, join_aux, fork_thr, join_thr;
     bool use_graphs = true;
     struct Step {
         cudaGraphExec_t exec;
@@ -464,7 +465,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
 }
 
 // The texture chain of step f (PSNR / color, window figures, lasting texture, reduction) for every source.
-void record_texture(es_batch &b, long f, cudaStream_t s)
+void record_texture(es_batch &b, long f, cudaStream_t s, cudaStream_t s2)
 {
     const int at = (int)(f % 2);
     const bool texture = f >= 2 * kRadius;
@@ -540,8 +541,21 @@ void record_texture(es_batch &b, long f, cudaStream_t s)
     }
     cuda_check(launch_pair_sums(pb, s), "batch squared errors and colors");
     cuda_check(launch_window_stats(wb, s), "batch window figures");
+    // the structure threshold needs only the window figures, so on a stream of its own it runs beside the lasting
+    // texture (one block, otherwise alone at the end of the chain)
+    const bool fork = cb.njobs && s2 != nullptr;
+    if (fork) {
+        cuda_check(cudaEventRecord(b.fork_thr.e, s), "event");
+        cuda_check(cudaStreamWaitEvent(s2, b.fork_thr.e, 0), "event");
+        cuda_check(launch_collect_threshold(cb, s2), "batch structure threshold");
+        cuda_check(cudaEventRecord(b.join_thr.e, s2), "event");
+    }
     cuda_check(launch_persist(qb, s), "batch lasting texture");
-    if (cb.njobs) cuda_check(launch_collect(cb, s), "batch collecting figures");
+    if (cb.njobs) {
+        if (fork) cuda_check(cudaStreamWaitEvent(s, b.join_thr.e, 0), "event");
+        else cuda_check(launch_collect_threshold(cb, s), "batch structure threshold");
+        cuda_check(launch_collect_sums(cb, s), "batch collecting figures");
+    }
     for (auto &sp : b.sources) {
         Source &S = *sp;
         cuda_check(cudaMemcpyAsync(S.h_sums[at].ptr, S.sums[at].ptr, S.sums[at].bytes(), cudaMemcpyDeviceToHost, s), "reading figures");
@@ -581,7 +595,7 @@ void record_step(es_batch &b, long f, uint32_t skip)
         cuda_check(cudaStreamWaitEvent(t, b.fork.e, 0), "event");
     }
     record_cambi(b, f, skip, s);
-    record_texture(b, f, t);
+    record_texture(b, f, t, split ? b.side2.s : nullptr);
     if (split) {
         cuda_check(cudaEventRecord(b.join.e, t), "event");
         cuda_check(cudaStreamWaitEvent(s, b.join.e, 0), "event");

@@ -262,6 +262,10 @@ struct CollectBatch {
 constexpr int kCollectSums = 20;  // 18 double sums and 2 counts per block
 int collect_blocks(int windows);
 cudaError_t launch_collect(CollectBatch &b, cudaStream_t s);
+// the same in two parts: the structure threshold and mask (needs the window figures only), then the windows' bins and
+// sums (needs the lasting figures too)
+cudaError_t launch_collect_threshold(CollectBatch &b, cudaStream_t s);
+cudaError_t launch_collect_sums(CollectBatch &b, cudaStream_t s);
 
 // ---- learned tile proposal -------------------------------------------------------------------------------------
 // A 4-layer network of valid 3 x 3 convolutions (2 -> 16 -> 16 -> 16 -> 1, ReLU after the first three) on 4 x 4

@@ -791,28 +791,39 @@ cudaError_t launch_pair_sums(PairSumsBatch &b, cudaStream_t s)
 
 int collect_blocks(int windows) { return collect_blocks_dev(windows); }
 
-cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
+// Grid rows of each job's encodes, and the most collect blocks of a job; an error for a job without encodes or windows.
+static cudaError_t collect_shape(CollectBatch &b, int &encs, int &nb, int &max_windows)
 {
-    int encs = 0, nb = 0;
+    encs = nb = max_windows = 0;
     for (int j = 0; j < b.njobs; j++) {
+        if (b.job[j].nenc <= 0 || b.job[j].windows <= 0) return cudaErrorInvalidValue;
         b.job[j].first_enc = encs;
         encs += b.job[j].nenc;
         nb = nb > collect_blocks(b.job[j].windows) ? nb : collect_blocks(b.job[j].windows);
-        if (b.job[j].nenc <= 0 || b.job[j].windows <= 0) return cudaErrorInvalidValue;
+        max_windows = max_windows > b.job[j].windows ? max_windows : b.job[j].windows;
     }
-    if (encs == 0) return cudaSuccess;
-    int max_windows = 0;
-    for (int j = 0; j < b.njobs; j++) max_windows = max_windows > b.job[j].windows ? max_windows : b.job[j].windows;
+    return cudaSuccess;
+}
+
+cudaError_t launch_collect_threshold(CollectBatch &b, cudaStream_t s)
+{
+    int encs, nb, max_windows;
+    cudaError_t e = collect_shape(b, encs, nb, max_windows);
+    if (e != cudaSuccess || encs == 0) return e;
     const int staged = max_windows <= kThreshStage;
-    cudaError_t e = cudaFuncSetAttribute(collect_threshold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kThreshStage * (int)sizeof(float));
+    e = cudaFuncSetAttribute(collect_threshold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kThreshStage * (int)sizeof(float));
     if (e != cudaSuccess) return e;
-    {
-        LaunchTimer t("frame_collect_threshold", s);
-        collect_threshold_kernel<<<b.njobs, kCT, staged ? (size_t)max_windows * sizeof(float) : 0, s>>>(b, staged);
-    }
-    e = after_launch();
-    if (e != cudaSuccess) return e;
+    LaunchTimer t("frame_collect_threshold", s);
+    collect_threshold_kernel<<<b.njobs, kCT, staged ? (size_t)max_windows * sizeof(float) : 0, s>>>(b, staged);
+    return after_launch();
+}
+
+cudaError_t launch_collect_sums(CollectBatch &b, cudaStream_t s)
+{
+    int encs, nb, max_windows;
+    cudaError_t e = collect_shape(b, encs, nb, max_windows);
+    if (e != cudaSuccess || encs == 0) return e;
     {
         LaunchTimer t("frame_collect_windows", s);
         collect_windows_kernel<<<dim3(nb, encs), kCW, 0, s>>>(b);
@@ -822,6 +833,12 @@ cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
     LaunchTimer t("frame_collect_final", s);
     collect_final_kernel<<<encs, 32 * kCollectSums, 0, s>>>(b);
     return after_launch();
+}
+
+cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
+{
+    const cudaError_t e = launch_collect_threshold(b, s);
+    return e != cudaSuccess ? e : launch_collect_sums(b, s);
 }
 
 const void *kernel_entry_unpack() { return (const void *)unpack_kernel; }
