@@ -149,3 +149,63 @@ def test_batch_rejects_bad_arguments(cuda, module):
     with pytest.raises(es_b200.EsError):
         b.collect(0)
     b.close()
+
+
+def test_host_frames_in_three_slots_equal_the_device_run(cuda, module, steps):
+    """Frames in pinned host memory, copied on a second stream into three device slots with frame f + 1's copy queued
+    before frame f - 1 is collected (the end-to-end pattern of bench.py and INTEGRATION.md), give the same results as
+    frames resident on the device: no copy overwrites a slot that a queued step still reads."""
+    from gpu_util import planar_view
+
+    torch = cuda
+    dev, dacc, _ = run_batch(cuda, module, steps)
+
+    def pinned(a):
+        a = np.ascontiguousarray(a)
+        return torch.from_numpy(a.view(np.int16) if a.dtype == np.uint16 else a).pin_memory()
+
+    pics = lambda f: [p for s in range(len(SOURCES)) for p in [steps[f][s].source] + list(steps[f][s].encodes)]
+    host = [[[pinned(a) for a in (p.y, p.u, p.v)] for p in pics(f)] for f in range(FRAMES)]
+    depths = [p.depth for p in pics(0)]
+    slots = [[[torch.empty_like(t, device="cuda") for t in pic] for pic in host[0]] for _ in range(3)]
+    views = [[planar_view(es_b200, *t, d) for t, d in zip(slot, depths)] for slot in slots]
+    stream, copy_stream = torch.cuda.Stream(), torch.cuda.Stream()
+    copied = [torch.cuda.Event() for _ in range(3)]
+    free = [torch.cuda.Event() for _ in range(3)]
+
+    def copy_in(f):
+        s = f % 3
+        with torch.cuda.stream(copy_stream):
+            copy_stream.wait_event(free[s])
+            for dst, src in zip(slots[s], host[f]):
+                for d, h in zip(dst, src):
+                    d.copy_(h, non_blocking=True)
+            copied[s].record(copy_stream)
+
+    b = es_b200.Batch(module, SOURCES)
+    accs = [es_b200.new_accum() for _ in range(b.n_encodes)]
+    results = {}
+
+    def collect(f):
+        r = b.collect(f, accs, accs)
+        results[f] = [(x.cambi, x.cambi_source, tuple(x.psnr), tuple(x.color_source), tuple(x.color_encode), x.texture,
+                       x.structure_windows, x.lasting_windows) for x in r]
+
+    with torch.cuda.stream(stream):
+        copy_in(0)
+        for f in range(FRAMES):
+            if f + 1 < FRAMES:
+                copy_in(f + 1)
+            stream.wait_event(copied[f % 3])
+            b.queue(f, views[f % 3], stream.cuda_stream)
+            free[f % 3].record(stream)
+            if f > 0:
+                collect(f - 1)
+        collect(FRAMES - 1)
+    b.close()
+    for f in range(FRAMES):
+        k = 0
+        for s, (w, h, pd, n) in enumerate(SOURCES):
+            assert results[f][k:k + n] == dev[s][0][f], (f, s)
+            k += n
+    assert [accum_bytes(x) for x in accs] == [accum_bytes(x) for x in dacc]
