@@ -267,6 +267,17 @@ cudaError_t launch_collect(CollectBatch &b, cudaStream_t s);
 cudaError_t launch_collect_threshold(CollectBatch &b, cudaStream_t s);
 cudaError_t launch_collect_sums(CollectBatch &b, cudaStream_t s);
 
+// ---- temporal alignment (src/kernels.cu:502-520, src/main.cpp:336-353) -------------------------------------------
+constexpr int kThumbW = 64, kThumbH = 36, kThumbPixels = kThumbW * kThumbH;
+constexpr int kThumbFrames = 64;  // frames of one thumbnail launch
+struct ThumbBatch {
+    FrameViewDev f[kThumbFrames];
+    int n, x0, y0, w, h;  // frames; the crop of every frame
+    float *out;           // [frame][kThumbH][kThumbW]
+};
+cudaError_t launch_thumbnails(const ThumbBatch &b, cudaStream_t s);
+cudaError_t launch_offset_totals(const float *ref, const float *probe, int n_probe, int lags, double *totals, cudaStream_t s);
+
 // ---- learned tile proposal -------------------------------------------------------------------------------------
 // A 4-layer network of valid 3 x 3 convolutions (2 -> 16 -> 16 -> 16 -> 1, ReLU after the first three) on 4 x 4
 // block features of scale 0 predicts log1p(mean positive c-value) of each 64 x 64 scale-0 tile. Parameters are one

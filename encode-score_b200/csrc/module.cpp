@@ -100,8 +100,12 @@ static const NamedKernel kKernels[] = {
 
 void check_device()
 {
+    // devices already found to be sm_100 with loadable kernels: reading all of a device's properties takes
+    // milliseconds, too long for entry points called per batch of frames
+    static std::atomic<uint64_t> verified{0};
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "finding the CUDA device");
+    if (dev >= 0 && dev < 64 && ((verified.load(std::memory_order_acquire) >> dev) & 1u)) return;
     cudaDeviceProp prop;
     cuda_check(cudaGetDeviceProperties(&prop, dev), "reading the device's properties");
     if (prop.major != 10 || prop.minor != 0)
@@ -109,6 +113,7 @@ void check_device()
                                        "; this library runs on sm_100 (B200) only");
     cudaFuncAttributes attr;
     cuda_check(cudaFuncGetAttributes(&attr, kernel_entry_cvalues()), "loading the kernels");
+    if (dev >= 0 && dev < 64) verified.fetch_or(uint64_t(1) << dev, std::memory_order_acq_rel);
 }
 
 // ---- CAMBI parameters ---------------------------------------------------------------------------------------------

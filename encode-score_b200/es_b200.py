@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # ES_B200_LIB selects another build of the library (another optimisation level, a profiling build)
 LIB_PATH = os.environ.get("ES_B200_LIB") or os.path.join(HERE, "libes_b200.so")
 
-ES_OK, ES_ERR_INVALID, ES_ERR_CUDA, ES_ERR_ALLOC, ES_ERR_STATE, ES_ERR_DEVICE = range(6)
+ES_OK, ES_ERR_INVALID, ES_ERR_CUDA, ES_ERR_ALLOC, ES_ERR_STATE, ES_ERR_DEVICE, ES_ERR_NO_MATCH = range(7)
+THUMB_W, THUMB_H = 64, 36
 HIST_BINS = 20001
 SCALES = 5
 
@@ -35,6 +36,7 @@ SYMBOLS = (
     "es_per_frame_json", "es_cambi_cache_open", "es_cambi_cache_find", "es_cambi_cache_add", "es_cambi_cache_file",
     "es_cambi_cache_close",
     "es_batch_graph_launches", "es_batch_destroy", "es_batch_set_proposal", "es_batch_proposal_stats",
+    "es_thumbnails", "es_offset_totals", "es_find_offset",
 )
 
 
@@ -185,6 +187,10 @@ def lib() -> ctypes.CDLL:
         L.es_batch_destroy.argtypes = [P]
         L.es_batch_set_proposal.argtypes = [P, P, ctypes.POINTER(ProposalOptions)]
         L.es_batch_proposal_stats.argtypes = [P, I, ctypes.POINTER(ProposalStats)]
+        D = ctypes.POINTER(ctypes.c_double)
+        L.es_thumbnails.argtypes = [ctypes.POINTER(FrameView), I, I, I, I, I, U64, P]
+        L.es_offset_totals.argtypes = [U64, I, U64, I, U64, P]
+        L.es_find_offset.argtypes = [U64, D, I, U64, D, I, P, D, D]
         _lib = L
     return _lib
 
@@ -575,3 +581,31 @@ class Batch:
         if self.handle:
             lib().es_batch_destroy(self.handle)
             self.handle = ctypes.c_void_p()
+
+
+# ---- temporal alignment (src/kernels.cu:502-520, src/main.cpp:301-353) ----------------------------------------------
+def thumbnails(views: list, x0: int, y0: int, w: int, h: int, out: int, stream: int = 0) -> None:
+    """64 x 36 luma thumbnails of the frames `views` cropped to w x h at (x0, y0), into the device floats at `out`
+    (2304 per frame, row by row)."""
+    arr = (FrameView * max(len(views), 1))(*views)
+    check(lib().es_thumbnails(arr, len(views), x0, y0, w, h, out, ctypes.c_void_p(stream)))
+
+
+def offset_totals(ref: int, n_ref: int, probe: int, n_probe: int, totals: int, stream: int = 0) -> None:
+    """Per lag, the double total of |ref[l + i][p] - probe[i][p]| over the probe's frames (device arrays)."""
+    check(lib().es_offset_totals(ref, n_ref, probe, n_probe, totals, ctypes.c_void_p(stream)))
+
+
+def find_offset(ref: int, ref_times, probe: int, probe_times, stream: int = 0) -> tuple:
+    """(offset, least mean difference) of the probe's thumbnails against the reference's (device arrays of
+    len(times) thumbnails each); raises EsError with status ES_ERR_NO_MATCH when they match at no lag."""
+    rt = (ctypes.c_double * len(ref_times))(*ref_times)
+    pt = (ctypes.c_double * len(probe_times))(*probe_times)
+    off, best = ctypes.c_double(), ctypes.c_double()
+    status = lib().es_find_offset(ref, rt, len(ref_times), probe, pt, len(probe_times), ctypes.c_void_p(stream),
+                                  ctypes.byref(off), ctypes.byref(best))
+    if status != ES_OK:
+        err = EsError(status, lib().es_last_error().decode(errors="replace"))
+        err.best_mean = best.value  # written for a failed match too
+        raise err
+    return off.value, best.value

@@ -12,6 +12,8 @@
  *   es_frame_*       the per-frame queue / collect of src/main.cpp:518-643 (which launches frame_planes,
  *                    window_stats, persist_stats, plane_sse and color_sums by name, src/main.cpp:229-234)
  *   es_accum_*, es_histogram_*   struct Histogram / Accum / score, src/stats.hpp:10-83
+ *   es_thumbnails, es_offset_totals, es_find_offset   the offset search between a source and its encodes:
+ *                    tiny_luma (src/kernels.cu:502-520), thumbnails() and find_offset() (src/main.cpp:301-353)
  */
 #ifndef ES_B200_H
 #define ES_B200_H
@@ -28,6 +30,7 @@ extern "C" {
 #define ES_ERR_ALLOC 3   /* device or pinned memory could not be allocated */
 #define ES_ERR_STATE 4   /* a call out of order, such as finish() without launch() */
 #define ES_ERR_DEVICE 5  /* no sm_100 device, or the kernels do not load on it */
+#define ES_ERR_NO_MATCH 6 /* es_find_offset: the probe matches the reference at no lag */
 
 /* The message of the calling thread's last failure ("" if none). The pointer stays valid until the thread's next
  * call into this library. */
@@ -335,6 +338,31 @@ int es_batch_proposal_stats(es_batch *b, int picture, es_proposal_stats *out);
 /* Diagnostics: how many steps were replayed from CUDA graphs. */
 uint64_t es_batch_graph_launches(const es_batch *b);
 void es_batch_destroy(es_batch *b);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Temporal alignment: the offset between a source and an encode that start at different points, found from 64 x 36
+ * luma thumbnails (src/kernels.cu:502-520, src/main.cpp:301-353).
+ * --------------------------------------------------------------------------------------------------------------- */
+#define ES_THUMB_W 64
+#define ES_THUMB_H 36
+/* Thumbnails of n frames in one launch: per frame, the box means of its luma cropped to w x h at (x0, y0), on a 10-bit
+ * scale (samples << (10 - depth)), into out[frame * 2304 + row * 64 + column] (device floats). Cell (tx, ty) covers
+ * columns x0 + tx w / 64 .. x0 + (tx + 1) w / 64 - 1 and rows alike; a cell with no pixel is NaN. Each cell's sum is
+ * an exact integer divided once, so the means equal tiny_luma's wherever a cell's sum is below 2^24 (cells up to
+ * 16,400 pixels: every picture up to 8K). views: host array of n views whose luma planes are in device memory. */
+int es_thumbnails(const es_frame_view *views, int n, int x0, int y0, int w, int h, uint64_t out, void *stream);
+/* For each lag l = 0 .. n_ref - n_probe: the sum over probe frames i and thumbnail pixels p, in that order, of
+ * |ref[l + i][p] - probe[i][p]|, each difference in float and the sum in double, as src/main.cpp:342-346 adds them.
+ * ref, probe: device thumbnails, 2304 floats per frame; totals: device doubles, one per lag. */
+int es_offset_totals(uint64_t ref, int n_ref, uint64_t probe, int n_probe, uint64_t totals, void *stream);
+/* find_offset (src/main.cpp:336-353): the offset to add to the probe's times so that its frames match the reference's,
+ * ref_times[lag] - probe_times[0] at the first lag of least mean thumbnail difference (total / (n_probe 2304)). Fewer
+ * than 24 probe frames, or more probe frames than reference frames, fail with ES_ERR_INVALID; a least mean difference
+ * above 16 (10-bit code values; matching pictures are well under 5) fails with ES_ERR_NO_MATCH. best_mean (may be
+ * NULL) receives the least mean in both cases. Thumbnails in device memory, times (seconds) in host memory; the call
+ * waits for `stream`. */
+int es_find_offset(uint64_t ref, const double *ref_times, int n_ref, uint64_t probe, const double *probe_times, int n_probe,
+                   void *stream, double *offset, double *best_mean);
 
 #ifdef __cplusplus
 }

@@ -6,7 +6,8 @@
 //  * the reference's CAMBI kernels run step by step with the launch shapes of src/cambi.cpp:88-135, keeping every
 //    scale's picture, mask and c-values for bit-exact comparison;
 //  * frame_planes, window_stats, persist_stats, plane_sse and color_sums with the launch shapes of
-//    src/main.cpp:502-566.
+//    src/main.cpp:502-566;
+//  * tiny_luma with the launch shape of src/main.cpp:321.
 // The four libvmaf luminance functions src/cambi.cpp declares (lines 7-15) are supplied here from the same published
 // model the product uses (BT.1886, 10-bit limited range, 300 / 0.01 cd/m2), so both sides share one parameter set.
 #include <cuda.h>
@@ -297,6 +298,20 @@ int ref_color_sums(void *kp, uint64_t u_, uint64_t v_, uint64_t n, int up, uint6
         void *args[] = {&u, &v, &nn, &up, &s};
         cu_check(cuLaunchKernel(k.get("color_sums"), 256, 1, 1, 256, 1, 1, 0, nullptr, args, nullptr), "color_sums");
         cu_check(cuCtxSynchronize(), "color_sums");
+    });
+}
+
+// tiny_luma with the launch shape of src/main.cpp:321 (64 x 36 blocks of 32 x 8 threads): one frame's thumbnail.
+int ref_tiny_luma(void *kp, const void *view, int x0, int y0, int w, int h, uint64_t out)
+{
+    return guarded([&] {
+        const Kernels &k = *(Kernels *)kp;
+        struct { const void *y, *u, *v; int ypitch, cpitch, semi, bytes, shift, depth; } f;
+        std::memcpy(&f, view, sizeof f);
+        CUdeviceptr o = out;
+        void *a[] = {&f, &x0, &y0, &w, &h, &o};
+        cu_check(cuLaunchKernel(k.get("tiny_luma"), 64, 36, 1, 32, 8, 1, 0, nullptr, a, nullptr), "tiny_luma");
+        cu_check(cuCtxSynchronize(), "tiny_luma");
     });
 }
 

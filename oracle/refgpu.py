@@ -30,6 +30,7 @@ class RefGpu:
         lib.ref_persist_stats.argtypes = [P, U64, U64, I, U64, I, I, U64]
         lib.ref_plane_sse.argtypes = [P, U64, U64, U64, U64]
         lib.ref_color_sums.argtypes = [P, U64, U64, U64, I, U64]
+        lib.ref_tiny_luma.argtypes = [P, P, I, I, I, I, U64]
         self._check(lib.ref_init())
         self.k = lib.ref_kernels()
         if not self.k:
@@ -72,6 +73,10 @@ class RefGpu:
 
     def color_sums(self, u, v, n, up, sums):
         self._check(self.lib.ref_color_sums(self.k, u, v, n, up, sums))
+
+    def tiny_luma(self, view, x0: int, y0: int, w: int, h: int, out: int) -> None:
+        """The reference's thumbnail of one frame (view: an es_frame_view-layout structure) into 2304 device floats."""
+        self._check(self.lib.ref_tiny_luma(self.k, ctypes.byref(view), x0, y0, w, h, out))
 
 
 _ref = None
