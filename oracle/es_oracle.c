@@ -509,3 +509,24 @@ void eso_color_sums(const uint16_t *u, const uint16_t *v, size_t n, int up, doub
     sums[1] = (double)sv;
     sums[2] = (double)ss * (1.0 / 1073741824.0);
 }
+
+double eso_find_offset_lag(const float *ref, int n_ref, const float *probe, int n_probe, int *lag)
+{
+    const size_t n = (size_t)n_probe;
+    double best = 1e30;
+    int found = 0;
+    for (int l = 0; l + n_probe <= n_ref; l++) {
+        double total = 0;
+        for (size_t i = 0; i < n && total < best * n * 2304; i++) {
+            const float *r = ref + ((size_t)l + i) * 2304, *q = probe + i * 2304;
+            for (int p = 0; p < 2304; p++) total += fabsf(r[p] - q[p]);
+        }
+        const double mean = total / (n * 2304.0);
+        if (mean < best) {
+            best = mean;
+            found = l;
+        }
+    }
+    *lag = found;
+    return best;
+}

@@ -89,6 +89,11 @@ uint64_t eso_plane_sse(const uint16_t *a, const uint16_t *b, size_t n);
 /* src/kernels.cu:470-484 color_sums: [sum U, sum V] exact on the 10-bit scale, and the sum of the color strength
  * sqrt(du^2 + dv^2), each term rounded to units of 2^-30 (the product's fixed-point definition). */
 void eso_color_sums(const uint16_t *u, const uint16_t *v, size_t n, int up, double sums[3]);
+/* src/main.cpp:339-348 find_offset's search, in its order of operations (float differences added in double, frame by
+ * frame and pixel by pixel, a lag abandoned once its partial total reaches the best so far): the lag of least mean
+ * difference of the n_probe thumbnails (2304 floats each) against n_ref reference thumbnails; returns that least mean
+ * and writes the lag. */
+double eso_find_offset_lag(const float *ref, int n_ref, const float *probe, int n_probe, int *lag);
 
 #ifdef __cplusplus
 }

@@ -70,6 +70,8 @@ def lib():
         _lib.eso_color_sums.argtypes = [P, P, ctypes.c_size_t, ctypes.c_int, P]
         _lib.eso_tvi_for_diff.argtypes = [ctypes.c_int, ctypes.c_double]
         _lib.eso_vlt_luma.argtypes = [ctypes.c_double]
+        _lib.eso_find_offset_lag.restype = ctypes.c_double
+        _lib.eso_find_offset_lag.argtypes = [P, ctypes.c_int, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     return _lib
 
 
@@ -408,3 +410,12 @@ def parts_json(a: Accum) -> dict:
                          "structure": [100.0 * a.sh_st_x[i] / a.sh_st_r[i] if a.sh_st_r[i] else float("nan") for i in range(2)],
                          "median": [a.matching[i].quantile(0.5) for i in range(2)], "worst_tenth": [a.matching[i].quantile(0.1) for i in range(2)]},
             "color_source": [a.color_r[i] / f for i in range(3)], "color_encode": [a.color_d[i] / f for i in range(3)]}
+
+
+def find_offset_lag(ref: np.ndarray, probe: np.ndarray) -> tuple[int, float]:
+    """``src/main.cpp:339-348`` in C (eso_find_offset_lag): (lag, least mean difference) of the probe's thumbnails."""
+    ref = np.ascontiguousarray(ref, np.float32)
+    probe = np.ascontiguousarray(probe, np.float32)
+    lag = ctypes.c_int()
+    best = lib().eso_find_offset_lag(_ptr(ref), ref.size // 2304, _ptr(probe), probe.size // 2304, ctypes.byref(lag))
+    return lag.value, best

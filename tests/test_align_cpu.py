@@ -69,3 +69,19 @@ def test_abi_checks_arguments_before_the_device():
     bad = (es_b200.FrameView * 1)(es_b200.FrameView(1, 1, 1, 128, 64, 0, 2, 0, 9))
     assert L.es_thumbnails(bad, 1, 0, 0, 64, 36, 1, None) == es_b200.ES_ERR_INVALID  # depth 9
     assert L.es_offset_totals(1, 10, 1, 11, 1, None) == es_b200.ES_ERR_INVALID  # more probe than reference frames
+
+
+def test_c_restatement_of_the_lag_search_equals_the_python_one():
+    import oracle
+
+    ref = moving(60, seed=4)
+    rng = np.random.default_rng(5)
+    for start, probe in ((21, ref[21:21 + 30] + rng.normal(0, 2, (30, 36, 64)).astype(np.float32)), (None, 1023 - ref[5:35])):
+        lag, best = oracle.find_offset_lag(ref, probe)
+        if start is None:
+            with pytest.raises(align.NoMatch) as e:
+                align.find_offset(ref, list(range(60)), probe, [0] * 30)
+            assert best == e.value.best > 16
+        else:
+            off, want_lag, want_best = align.find_offset(ref, list(range(60)), probe, [0] * 30)
+            assert lag == want_lag == start and best == want_best
