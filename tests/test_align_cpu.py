@@ -85,3 +85,18 @@ def test_c_restatement_of_the_lag_search_equals_the_python_one():
         else:
             off, want_lag, want_best = align.find_offset(ref, list(range(60)), probe, [0] * 30)
             assert lag == want_lag == start and best == want_best
+
+
+def test_ties_between_lags_keep_the_first():
+    """A reference whose pictures repeat with period 20: lags 7 and 27 give equal totals, bit for bit, and every
+    restatement keeps lag 7 (src/main.cpp:347 replaces the best only on a strictly smaller mean)."""
+    import oracle
+
+    base = moving(20, seed=8)
+    ref = np.concatenate([base, base, base])  # 60 frames, period 20
+    probe = ref[7:7 + 24] + np.random.default_rng(9).normal(0, 2, (24, 36, 64)).astype(np.float32)
+    totals = align.lag_totals(ref, probe)
+    assert totals[7] == totals[27] and int(np.argmin(totals)) == 7
+    off, lag, best = align.find_offset(ref, [k / 25.0 for k in range(60)], probe, [0.0] * 24)
+    assert lag == 7 and off == 7 / 25.0
+    assert oracle.find_offset_lag(ref, probe) == (7, best)

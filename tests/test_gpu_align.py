@@ -134,3 +134,14 @@ def test_find_offset_on_thumbnails_of_a_moving_sequence(cuda, module):
     with pytest.raises(align.NoMatch) as o:
         align.find_offset(host["src"], t_src, host["other"], t_enc)
     assert e.value.best_mean == o.value.best > 16
+
+
+def test_find_offset_keeps_the_first_of_tied_lags(cuda, module):
+    """Pictures that repeat with period 20 give lags 7 and 27 equal totals; the first is kept, as in the reference."""
+    base = moving(20, seed=8)
+    ref = np.concatenate([base, base, base])
+    probe = ref[7:7 + 24] + np.random.default_rng(9).normal(0, 2, (24, 36, 64)).astype(np.float32)
+    d_ref, d_probe = cuda.from_numpy(ref.ravel()).cuda(), cuda.from_numpy(probe.ravel().copy()).cuda()
+    off, best = es_b200.find_offset(d_ref.data_ptr(), [k / 25.0 for k in range(60)], d_probe.data_ptr(), [0.0] * 24)
+    want_off, want_lag, want_best = align.find_offset(ref, [k / 25.0 for k in range(60)], probe, [0.0] * 24)
+    assert want_lag == 7 and off == want_off and best == want_best
