@@ -52,6 +52,7 @@ struct Picture {
     int source = 0, encode = -1;  // encode -1: the source's own picture
     int w = 0, h = 0, depth = 10;
     int tile_rows[kScales] = {64, 64, 64, 64, 64};  // c-value tile rows per scale
+    float *cv_plane[kScales] = {};                   // optional: every computed c-value at its pixel (tests)
     es_cambi_params p{};
     int sw[kScales], sh[kScales];
     DeviceBuffer<uint16_t> words[kScales];
@@ -397,7 +398,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
             j.tiles_x = (j.w + kCvTX - 1) / kCvTX;
             j.first_tile = tiles;
             j.slot = i * kScales + sc;
-            j.plane = nullptr;
+            j.plane = pic.cv_plane[sc];
             j.tile_rows = (b.net && sc < 2) ? 64 : pic.tile_rows[sc];  // the proposal maps 64-row tiles of scales 0, 1
             tiles += j.tiles_x * ((j.h + j.tile_rows - 1) / j.tile_rows);
         }
@@ -800,6 +801,21 @@ int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5])
         if (b->last_collected < 0) throw Error(ES_ERR_STATE, "es_batch_scale_pooled: no frame collected");
         const double *sc = b->h_scores[b->last_collected % 2].ptr + (size_t)picture * (1 + kScales);
         for (int s = 0; s < kScales; s++) pooled[s] = sc[1 + s];
+    });
+}
+
+int es_batch_set_cvalue_planes(es_batch *b, int picture, float *const dev_planes[5])
+{
+    return guarded([&] {
+        require(b != nullptr, "es_batch_set_cvalue_planes: NULL batch");
+        require(picture >= 0 && picture < (int)b->pictures.size(), "es_batch_set_cvalue_planes: picture out of range");
+        if (b->queued[0] > b->last_collected || b->queued[1] > b->last_collected)
+            throw Error(ES_ERR_STATE, "es_batch_set_cvalue_planes: collect every queued step first");
+        cuda_check(cudaStreamSynchronize(b->main.s), "es_batch_set_cvalue_planes");
+        for (auto &g : b->graphs) cudaGraphExecDestroy(g.second.exec);  // captured steps hold the old addresses
+        b->graphs.clear();
+        Picture &pic = *b->pictures[picture];
+        for (int s = 0; s < kScales; s++) pic.cv_plane[s] = dev_planes ? dev_planes[s] : nullptr;
     });
 }
 

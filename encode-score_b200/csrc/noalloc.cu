@@ -7,12 +7,13 @@
 // in one file-scope device array of kScratchBytes (20 MiB), which every GPU that loads the library holds until the
 // process exits. The caller passes the input plane and a device double for the output.
 //
-// Host code cannot use the array's name as a device address (in host code it names a host-side stand-in), so the
-// first call on each device, with that device current, looks the address up with cudaGetSymbolAddress and fills the
-// reciprocal table; that first call should come before any stream capture. Every call shares the array: each call
-// clears what must start at zero, and calls whose work overlaps on the GPU race.
-#include <mutex>
-
+// Host code cannot use the array's name as a device address (in host code it names a host-side stand-in). A device
+// symbol's address belongs to a CUDA context, and a program may call from more than one context on a device (the
+// primary one, or one it made with cuCtxCreate), so every call looks the address up again with cudaGetSymbolAddress in
+// the context current on the calling thread, and every call rewrites the reciprocal table in its first kernel: no
+// address or table state is kept on the host. A context's first call may load the library's kernels into it, so make
+// it before any stream capture. Every call shares the array: each call clears what must start at zero, and calls whose
+// work overlaps on the GPU race.
 #include "es_internal.h"
 
 namespace es {
@@ -59,21 +60,23 @@ Carve carve(int w, int h)
     return c;
 }
 
-// 1/i as float for i < kLutEntries (entry 0 unused), the same correctly rounded values as reciprocal_table().
-__global__ void noalloc_lut_kernel(float *lut)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kLutEntries; i += gridDim.x * blockDim.x)
-        lut[i] = i ? __double2float_rn(__ddiv_rn(1.0, (double)i)) : 0.0f;
-}
-
 struct SlotSetup {
     float *list[kScales];
     unsigned long long n[kScales], k[kScales];
 };
 
-// Clears the five counter slots and points them at their lists (blockIdx.x = scale).
-__global__ void noalloc_slots_kernel(CvSlot *slots, const __grid_constant__ SlotSetup st)
+constexpr int kLutBlocks = 4;
+
+// Blocks 0 .. kScales - 1 clear the five counter slots and point them at their lists (blockIdx.x = scale); the other
+// kLutBlocks blocks write the reciprocal table lut[i] = 1/i as float for i < kLutEntries (entry 0 unused), the same
+// correctly rounded values as reciprocal_table().
+__global__ void noalloc_setup_kernel(CvSlot *slots, float *lut, const __grid_constant__ SlotSetup st)
 {
+    if (blockIdx.x >= kScales) {
+        for (int i = (blockIdx.x - kScales) * blockDim.x + threadIdx.x; i < kLutEntries; i += kLutBlocks * blockDim.x)
+            lut[i] = i ? __double2float_rn(__ddiv_rn(1.0, (double)i)) : 0.0f;
+        return;
+    }
     CvSlot &S = slots[blockIdx.x];
     for (int i = threadIdx.x; i < 2048; i += blockDim.x) S.hist[i] = 0;
     if (threadIdx.x == 0) {
@@ -87,27 +90,12 @@ __global__ void noalloc_slots_kernel(CvSlot *slots, const __grid_constant__ Slot
     }
 }
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-unsigned char *g_base[kMaxDevices] = {};
-
-// The array's device address on the current device, looked up (and the table filled) on the device's first call.
-unsigned char *scratch_on_current_device()
+// The array's device address in the CUDA context current on the calling thread.
+unsigned char *scratch_in_current_context()
 {
-    int dev = 0;
-    cuda_check(cudaGetDevice(&dev), "finding the CUDA device");
-    require(dev >= 0 && dev < kMaxDevices, "es_cambi_score_noalloc: device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_base[dev]) {
-        void *p = nullptr;
-        cuda_check(cudaGetSymbolAddress(&p, g_scratch), "finding the no-allocation scratch array");
-        unsigned char *base = (unsigned char *)p;
-        noalloc_lut_kernel<<<8, 256>>>((float *)(base + carve(2, 2).lut));
-        cuda_check(cudaGetLastError(), "filling the reciprocal table");
-        cuda_check(cudaDeviceSynchronize(), "filling the reciprocal table");
-        g_base[dev] = base;
-    }
-    return g_base[dev];
+    void *p = nullptr;
+    cuda_check(cudaGetSymbolAddress(&p, g_scratch), "finding the no-allocation scratch array");
+    return (unsigned char *)p;
 }
 
 }  // namespace
@@ -130,7 +118,7 @@ extern "C" int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int
         const es_cambi_params p = derive_params(w, h);
         require(p.pad <= kNoAllocMaxPad, "es_cambi_score_noalloc: window wider than 65");
         require(p.band_size > 0 && p.band_size <= kMaxBand, "es_cambi_score_noalloc: band out of range");
-        unsigned char *base = scratch_on_current_device();
+        unsigned char *base = scratch_in_current_context();
         cudaStream_t s = (cudaStream_t)stream;
         CvSlot *slots = (CvSlot *)(base + c.slots);
         double *rec = (double *)(base + c.score);
@@ -141,7 +129,7 @@ extern "C" int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int
             st.n[k] = (unsigned long long)c.sw[k] * c.sh[k];
             st.k[k] = topk_count(st.n[k], p.topk);
         }
-        noalloc_slots_kernel<<<kScales, 256, 0, s>>>(slots, st);
+        noalloc_setup_kernel<<<kScales + kLutBlocks, 256, 0, s>>>(slots, (float *)(base + c.lut), st);
         cuda_check(cudaGetLastError(), "clearing the counters");
 
         Prep0Batch pb{};

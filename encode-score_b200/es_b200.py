@@ -32,6 +32,7 @@ SYMBOLS = (
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
     "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
+    "es_batch_set_cvalue_planes",
     "es_windows_create", "es_windows_compute", "es_windows_figures", "es_windows_destroy",
     "es_per_frame_json", "es_cambi_cache_open", "es_cambi_cache_find", "es_cambi_cache_add", "es_cambi_cache_file",
     "es_cambi_cache_close",
@@ -182,6 +183,7 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.POINTER(Accum)), ctypes.POINTER(FrameResult)]
         L.es_batch_read_windows.argtypes = [P, I, I, P, P]
         L.es_batch_scale_pooled.argtypes = [P, I, ctypes.POINTER(ctypes.c_double)]
+        L.es_batch_set_cvalue_planes.argtypes = [P, I, ctypes.POINTER(P)]
         L.es_batch_graph_launches.argtypes = [P]
         L.es_batch_graph_launches.restype = U64
         L.es_batch_destroy.argtypes = [P]
@@ -561,6 +563,12 @@ class Batch:
         out = (ctypes.c_double * SCALES)()
         check(lib().es_batch_scale_pooled(self.handle, picture, out))
         return list(out)
+
+    def set_cvalue_planes(self, picture: int, ptrs: list | None) -> None:
+        """Later steps also write every computed c-value of `picture` into the zeroed device float planes `ptrs` (one
+        per scale); None switches it off."""
+        arr = (ctypes.c_void_p * SCALES)(*(ptrs or [None] * SCALES))
+        check(lib().es_batch_set_cvalue_planes(self.handle, picture, arr if ptrs else None))
 
     def set_proposal(self, net, threshold: float = 0.05, audit=(50, 200), tolerance: float = 0.025, budget: float = 0.0) -> None:
         """Switches the learned tile proposal on (net: ProposalNet) or off (net None); budget > 0 also skips, per

@@ -122,9 +122,11 @@ int es_cambi_scale_words(const es_cambi *c, int s, uint64_t *address);
  * library, which every GPU that loads the library holds until the process exits, so it takes pictures up to about
  * 1920 x 1080 (larger ones fail with ES_ERR_INVALID and the size they would need). `img` is a device plane of w x h
  * values at `depth` bits (8 or 10), `pitch` in pixels; the score is written to the device double `score`; all work is
- * queued on `stream` and the call returns without waiting. The first call on each device (with that device current)
- * looks up the array's address and fills a table, and should come before any stream capture. Every call shares the
- * array: calls whose work overlaps on the GPU race, so serialize them (one stream, or events). */
+ * queued on `stream` and the call returns without waiting. It runs in the CUDA context current on the calling thread
+ * (the primary context, or one made with cuCtxCreate): each call looks the array's address up in that context and
+ * rewrites its reciprocal table, so nothing is cached across contexts or device resets. A context's first call may
+ * load the library's kernels into it, so it should come before any stream capture. Every call shares the array: calls
+ * whose work overlaps on the GPU race, so serialize them (one stream, or events). */
 int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int depth, double *score, void *stream);
 
 /* ---------------------------------------------------------------------------------------------------------------
@@ -310,6 +312,10 @@ int es_batch_collect(es_batch *b, long f, const double *cached_source_cambi, es_
 int es_batch_read_windows(es_batch *b, int source, int encode, float *stats, float *persist);
 /* Introspection for tests: the pooled value of each scale of picture `picture` in the last collected step. */
 int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5]);
+/* Introspection for tests: as es_cambi_set_cvalue_planes for picture `picture` of later steps (dev_planes NULL
+ * switches it off). Steps already captured as CUDA graphs are dropped, so later ones capture the new setting. Every
+ * queued step must have been collected. */
+int es_batch_set_cvalue_planes(es_batch *b, int picture, float *const dev_planes[5]);
 /* The learned tile proposal (no counterpart in the reference): with a network, later steps compute c-values of
  * scales 0 and 1 only on tiles whose prediction (or, at scale 1, the prediction of a scale-0 tile it covers) reaches
  * `threshold`, plus a random audit sample (per mille of the other tiles, per scale); scales 2-4 always run. From the

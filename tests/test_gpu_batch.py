@@ -153,7 +153,7 @@ def test_batch_rejects_bad_arguments(cuda, module):
 
 def test_host_frames_in_three_slots_equal_the_device_run(cuda, module, steps):
     """Frames in pinned host memory, copied on a second stream into three device slots with frame f + 1's copy queued
-    before frame f - 1 is collected (the end-to-end pattern of bench.py and INTEGRATION.md), give the same results as
+    before frame f - 1 is collected (the end-to-end pattern of bench.py), give the same results as
     frames resident on the device: no copy overwrites a slot that a queued step still reads."""
     from gpu_util import planar_view
 
