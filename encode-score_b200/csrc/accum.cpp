@@ -147,4 +147,29 @@ double es_psnr(uint64_t sse, uint64_t n, int depth)
     return std::min(10.0 * std::log10(peak * peak / std::max(mse, 1e-16)), 6.0 * depth + 12);
 }
 
+size_t es_per_frame_json(const double *vmaf, const double *cambi, const double *cambi_source, const double *psnr_y, long n,
+                         char *buf, size_t size)
+{
+    // src/main.cpp:767-774: {"vmaf": [...], "cambi": [...], "cambi_source": [...], "psnr_y": [...]}, 6 digits (3 for
+    // PSNR), comma-separated without spaces; without VMAF figures, "vmaf": null
+    std::string out = "{\"vmaf\": ";
+    auto arr = [&](const double *v, int digits) {
+        std::string s = "[";
+        char tmp[64];
+        for (long i = 0; i < n; i++) {
+            std::snprintf(tmp, sizeof tmp, "%s%.*f", i ? "," : "", digits, v[i]);
+            s += tmp;
+        }
+        return s + "]";
+    };
+    out += vmaf ? arr(vmaf, 6) : std::string("null");
+    out += ", \"cambi\": " + arr(cambi, 6) + ", \"cambi_source\": " + arr(cambi_source, 6) + ", \"psnr_y\": " + arr(psnr_y, 3) + "}";
+    if (buf && size) {
+        const size_t k = std::min(size - 1, out.size());
+        std::memcpy(buf, out.data(), k);
+        buf[k] = '\0';
+    }
+    return out.size();
+}
+
 }  // extern "C"

@@ -1,19 +1,22 @@
-// es_cambi_cache: the source's CAMBI per frame kept on disk between runs, src/cache.hpp / src/cache.cpp in the same
-// file format and key, so a cache written by either implementation is read by the other.
+// es_cambi_cache: the source's CAMBI per frame, kept on disk between runs, so a later run against the same source
+// reads it instead of computing it again (the reference's CambiCache, src/cache.hpp:9-29, src/cache.cpp:13-88).
 //
-// The file is named by an FNV-1a hash of "cambi <version> <file size> <x0> <y0> <w> <h> <depth>" followed by the first
-// and the last mebibyte of the source file (a renamed or moved source keeps its scores), under
-// $XDG_CACHE_HOME/encode-score (else $HOME/.cache/encode-score). It holds 16-byte records {int64 pts; double score},
-// appended every 240 scores and on close; a partial record at the end (a run stopped in mid-write) is dropped on
-// open. A cache that cannot be opened behaves as an empty one that keeps nothing.
+// The on-disk format is shared with the reference, so a cache written by either program is read by the other:
+//  * directory: the caller's, else $XDG_CACHE_HOME/encode-score, else $HOME/.cache/encode-score;
+//  * file name: 16 lower-case hex digits of a 64-bit FNV-1a hash, then ".cambi". The hash runs over the key text
+//    "cambi <version> <source bytes> <x0> <y0> <w> <h> <depth>" (version 1), then the source's first min(size, 1 MiB)
+//    bytes, then the min(size, 1 MiB) bytes that start at max(size - 1 MiB, 0) (a small file is hashed twice);
+//  * content: records of 16 bytes, {int64 pts; double score} in host byte order, appended in batches of 240 and on
+//    close. A length that is not a whole number of records (a run stopped in mid-write) loses its partial last
+//    record when the cache is opened; a later record of the same pts wins over an earlier one.
+// A cache that cannot be opened (no directory, an unreadable source, a failed write) behaves as an empty one that keeps
+// nothing. Frames without a timestamp (INT64_MIN) are never looked up or stored.
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
-#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
-#include <cstring>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -24,42 +27,116 @@
 using namespace es;
 
 namespace {
-constexpr int kCacheVersion = 1;  // raised when the CAMBI computation changes its scores
-constexpr size_t kSample = 1 << 20, kFlush = 240;
-constexpr int64_t kNoPts = INT64_MIN;  // a frame without a presentation timestamp
 
-struct Record {
+constexpr int kFormatVersion = 1;             // raised when the CAMBI computation changes its scores
+constexpr off_t kSampleBytes = 1 << 20;       // bytes of the source hashed at its start and at its end
+constexpr size_t kRecordsPerWrite = 240;
+constexpr int64_t kNoTimestamp = INT64_MIN;
+
+struct ScoreRecord {
     int64_t pts;
     double score;
 };
-static_assert(sizeof(Record) == 16, "cache record layout");
+static_assert(sizeof(ScoreRecord) == 16, "the cache's records are 16 bytes");
 
-uint64_t fnv1a(uint64_t h, const void *data, size_t n)
+// 64-bit FNV-1a, fed in pieces.
+struct Fnv1a64 {
+    uint64_t state = 0xcbf29ce484222325ull;
+    void feed(const void *bytes, size_t n)
+    {
+        const unsigned char *p = static_cast<const unsigned char *>(bytes);
+        for (const unsigned char *end = p + n; p != end; ++p) state = (state ^ *p) * 0x100000001b3ull;
+    }
+};
+
+// Reads exactly n bytes at `at` unless the file ends first; returns the bytes read, or -1 on an error.
+ssize_t read_at(int fd, unsigned char *dst, size_t n, off_t at)
 {
-    for (size_t i = 0; i < n; i++) h = (h ^ ((const unsigned char *)data)[i]) * 0x100000001b3ull;
-    return h;
+    size_t got = 0;
+    while (got < n) {
+        const ssize_t r = pread(fd, dst + got, n - got, at + (off_t)got);
+        if (r < 0) return -1;
+        if (r == 0) break;
+        got += (size_t)r;
+    }
+    return (ssize_t)got;
 }
+
+// The cache file's name for a source, or "" when the source cannot be read.
+std::string cache_name(const char *source, int x0, int y0, int w, int h, int depth)
+{
+    const int fd = open(source, O_RDONLY);
+    if (fd < 0) return "";
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+        close(fd);
+        return "";
+    }
+    const off_t size = st.st_size;
+    // both samples in one buffer, hashed after the key text
+    const off_t head = size < kSampleBytes ? size : kSampleBytes;
+    const off_t tail_at = size > kSampleBytes ? size - kSampleBytes : 0;
+    std::vector<unsigned char> sample((size_t)(2 * head));
+    const ssize_t a = read_at(fd, sample.data(), (size_t)head, 0);
+    const ssize_t b = read_at(fd, sample.data() + head, (size_t)head, tail_at);
+    close(fd);
+    if (a < 0 || b < 0) return "";
+    const std::string key = "cambi " + std::to_string(kFormatVersion) + " " + std::to_string((long long)size) + " " +
+                            std::to_string(x0) + " " + std::to_string(y0) + " " + std::to_string(w) + " " +
+                            std::to_string(h) + " " + std::to_string(depth);
+    Fnv1a64 hash;
+    hash.feed(key.data(), key.size());
+    hash.feed(sample.data(), (size_t)a);
+    hash.feed(sample.data() + head, (size_t)b);
+    char hex[17];
+    std::snprintf(hex, sizeof hex, "%016llx", (unsigned long long)hash.state);
+    return std::string(hex) + ".cambi";
+}
+
+std::string default_directory()
+{
+    const char *xdg = std::getenv("XDG_CACHE_HOME");
+    if (xdg && *xdg) return xdg;
+    const char *home = std::getenv("HOME");
+    return home ? std::string(home) + "/.cache" : "";
+}
+
 }  // namespace
 
 struct es_cambi_cache {
-    std::string file;
-    std::unordered_map<int64_t, double> scores;
-    std::vector<Record> pending;
-    int fd = -1;
+    std::string path;                              // "" when there is no cache file
+    int fd = -1;                                   // open for appending while the cache stores
+    std::unordered_map<int64_t, double> known;     // every score read or added
+    std::vector<ScoreRecord> unwritten;
 
-    void flush()
+    // Reads the records of an opened file, dropping a partial last one. False when the file cannot be used.
+    bool load()
     {
-        if (fd >= 0 && !pending.empty() &&
-            write(fd, pending.data(), pending.size() * sizeof(Record)) != (ssize_t)(pending.size() * sizeof(Record))) {
-            close(fd);
-            fd = -1;
-        }
-        pending.clear();
+        struct stat st;
+        if (fstat(fd, &st) != 0) return false;
+        const off_t whole = st.st_size - st.st_size % (off_t)sizeof(ScoreRecord);
+        if (whole != st.st_size && ftruncate(fd, whole) != 0) return false;
+        std::vector<ScoreRecord> records((size_t)(whole / (off_t)sizeof(ScoreRecord)));
+        if (read_at(fd, reinterpret_cast<unsigned char *>(records.data()), (size_t)whole, 0) != (ssize_t)whole) return false;
+        for (const ScoreRecord &r : records) known[r.pts] = r.score;
+        return true;
+    }
+    void stop_storing()
+    {
+        if (fd >= 0) close(fd);
+        fd = -1;
+    }
+    void write_out()
+    {
+        if (unwritten.empty()) return;
+        const size_t bytes = unwritten.size() * sizeof(ScoreRecord);
+        if (fd >= 0 && write(fd, unwritten.data(), bytes) != (ssize_t)bytes) stop_storing();
+        unwritten.clear();
     }
     ~es_cambi_cache()
     {
-        flush();
-        if (fd >= 0) close(fd);
+        write_out();
+        stop_storing();
     }
 };
 
@@ -70,47 +147,24 @@ int es_cambi_cache_open(const char *path, int x0, int y0, int w, int h, int dept
     return guarded([&] {
         require(path != nullptr && out != nullptr, "es_cambi_cache_open: NULL argument");
         auto c = std::make_unique<es_cambi_cache>();
-        std::string d;
+        std::string where;
         if (dir) {
-            d = dir;
+            where = dir;
         } else {
-            const char *xdg = std::getenv("XDG_CACHE_HOME"), *home = std::getenv("HOME");
-            d = xdg && *xdg ? xdg : home ? std::string(home) + "/.cache" : "";
-            if (!d.empty()) {
-                mkdir(d.c_str(), 0755);
-                d += "/encode-score";
+            const std::string base = default_directory();
+            if (!base.empty()) {
+                mkdir(base.c_str(), 0755);
+                where = base + "/encode-score";
             }
         }
-        FILE *f = d.empty() ? nullptr : std::fopen(path, "rb");
-        if (f) {
-            mkdir(d.c_str(), 0755);
-            std::vector<unsigned char> buf(kSample);
-            std::fseek(f, 0, SEEK_END);
-            const long size = std::ftell(f);
-            char key[96];
-            const int len = std::snprintf(key, sizeof key, "cambi %d %ld %d %d %d %d %d", kCacheVersion, size, x0, y0, w, h, depth);
-            uint64_t hash = fnv1a(0xcbf29ce484222325ull, key, (size_t)len);
-            for (long at : {0L, std::max(size - (long)kSample, 0L)}) {
-                std::fseek(f, at, SEEK_SET);
-                hash = fnv1a(hash, buf.data(), std::fread(buf.data(), 1, kSample, f));
-            }
-            std::fclose(f);
-            char name[40];
-            std::snprintf(name, sizeof name, "/%016llx.cambi", (unsigned long long)hash);
-            c->file = d + name;
-            c->fd = open(c->file.c_str(), O_RDWR | O_CREAT | O_APPEND, 0644);
-            if (c->fd >= 0) {
-                struct stat st;
-                fstat(c->fd, &st);
-                const off_t whole = st.st_size / (off_t)sizeof(Record) * (off_t)sizeof(Record);
-                if (whole != st.st_size && ftruncate(c->fd, whole) != 0) {
-                    close(c->fd);
-                    c->fd = -1;
-                } else {
-                    std::vector<Record> records(whole / sizeof(Record));
-                    if (pread(c->fd, records.data(), whole, 0) == whole)
-                        for (const Record &r : records) c->scores[r.pts] = r.score;
-                }
+        const std::string name = where.empty() ? "" : cache_name(path, x0, y0, w, h, depth);
+        if (!name.empty()) {
+            mkdir(where.c_str(), 0755);
+            c->path = where + "/" + name;
+            c->fd = open(c->path.c_str(), O_RDWR | O_CREAT | O_APPEND, 0644);
+            if (c->fd >= 0 && !c->load()) {
+                c->known.clear();
+                c->stop_storing();
             }
         }
         *out = c.release();
@@ -119,9 +173,9 @@ int es_cambi_cache_open(const char *path, int x0, int y0, int w, int h, int dept
 
 int es_cambi_cache_find(const es_cambi_cache *c, int64_t pts, double *score)
 {
-    if (!c || pts == kNoPts) return 0;
-    const auto it = c->scores.find(pts);
-    if (it == c->scores.end()) return 0;
+    if (!c || pts == kNoTimestamp) return 0;
+    const auto it = c->known.find(pts);
+    if (it == c->known.end()) return 0;
     if (score) *score = it->second;
     return 1;
 }
@@ -130,40 +184,15 @@ int es_cambi_cache_add(es_cambi_cache *c, int64_t pts, double score)
 {
     return guarded([&] {
         require(c != nullptr, "es_cambi_cache_add: NULL cache");
-        if (c->fd < 0 || pts == kNoPts) return;
-        c->scores[pts] = score;
-        c->pending.push_back({pts, score});
-        if (c->pending.size() >= kFlush) c->flush();
+        if (c->fd < 0 || pts == kNoTimestamp) return;
+        c->known[pts] = score;
+        c->unwritten.push_back(ScoreRecord{pts, score});
+        if (c->unwritten.size() == kRecordsPerWrite) c->write_out();
     });
 }
 
-const char *es_cambi_cache_file(const es_cambi_cache *c) { return c ? c->file.c_str() : ""; }
+const char *es_cambi_cache_file(const es_cambi_cache *c) { return c ? c->path.c_str() : ""; }
 
 void es_cambi_cache_close(es_cambi_cache *c) { delete c; }
-
-size_t es_per_frame_json(const double *vmaf, const double *cambi, const double *cambi_source, const double *psnr_y, long n,
-                         char *buf, size_t size)
-{
-    // src/main.cpp:767-774: {"vmaf": [...], "cambi": [...], "cambi_source": [...], "psnr_y": [...]}, 6 digits (3 for
-    // PSNR), comma-separated without spaces; without VMAF figures, "vmaf": null
-    std::string out = "{\"vmaf\": ";
-    auto arr = [&](const double *v, int digits) {
-        std::string s = "[";
-        char tmp[64];
-        for (long i = 0; i < n; i++) {
-            std::snprintf(tmp, sizeof tmp, "%s%.*f", i ? "," : "", digits, v[i]);
-            s += tmp;
-        }
-        return s + "]";
-    };
-    out += vmaf ? arr(vmaf, 6) : std::string("null");
-    out += ", \"cambi\": " + arr(cambi, 6) + ", \"cambi_source\": " + arr(cambi_source, 6) + ", \"psnr_y\": " + arr(psnr_y, 3) + "}";
-    if (buf && size) {
-        const size_t k = std::min(size - 1, out.size());
-        std::memcpy(buf, out.data(), k);
-        buf[k] = '\0';
-    }
-    return out.size();
-}
 
 }  // extern "C"
