@@ -12,15 +12,21 @@ lasting-texture figures, PSNR and color, and the per-frame reduction into per-se
 * ``e2e``: the same through the C ABI with the inputs in pinned host memory, copied host-to-device every step on a copy
   stream (three input slots, each step's copy queued one step ahead) and the figures read back, inside the timed
   region.
-* ``roofline``: the kernel with the most device time: its algorithmic bytes per launch (algorithmic_bytes) over its
-  mean duration, against the measured HBM copy bandwidth. Durations come from a pass over the pool after the timed
-  region with every kernel alone on the stream and bracketed by CUDA events (``kernels`` lists them all).
-* ``cpu_baseline``: the CPU oracle (plain-C restatement of the reference) on the host cores, one frame step per
-  process, rank 0 at N = 1 only.
+* ``roofline``: the kernel with the most device time in a frame step: its algorithmic bytes per step (every launch
+  of it in the step; algorithmic_bytes) over its event-timed duration per step, against the measured HBM copy
+  bandwidth; ``step`` gives the same for the whole step (inputs read once, per-window outputs written once) over the
+  timed ms per step, and ``issue`` the kernel's instruction-issue roofline from a one-kernel ncu capture
+  (profiles/issue.json). Durations come from a pass over the pool after the timed region with every kernel alone on
+  the stream and bracketed by CUDA events (``kernels`` lists them all, each with its own HBM fraction).
+* ``cpu_baseline``: the CPU oracle (plain-C restatement of the reference) on the host cores, rank 0 at N = 1 only:
+  strips of a real frame step (13 distinct source frames for the lasting texture, host collect included), one strip
+  per process side by side for the all-core rate (median of 5 rounds) and one process alone for ``value_1_core``.
+* ``c3``: the uneven batch of 16 source / encode pairs per frame step, plain (16 es_frame) against batched (one
+  es_batch), as extra figures (``--workload c3`` makes it the headline instead).
 
 ``--impl reference`` times the reference's CPU path instead: the CPU oracle port over all host cores (the reference's
 own CPU implementation of this path is its numpy module plus libvmaf's CAMBI, neither of which exists on the GPU
-hosts), printing the same metric.
+hosts), printing the same metric and config.
 
 Multi-GPU: one process per GPU (torchrun), each scoring its own source; scaling is weak and the time is the max over
 ranks.
@@ -56,16 +62,15 @@ def scale_pixels(w: int, h: int) -> list[int]:
     return out
 
 
-def algorithmic_bytes(name: str, wl: dict, pics: int = 1) -> float | None:
-    """Bytes a launch of `name` must move at least: inputs read once, outputs written once (per launch). `pics` is the
-    number of pictures one CAMBI launch covers (1 in the plain form, every picture of the step in the batched one)."""
+def algorithmic_bytes(name: str, wl: dict) -> float | None:
+    """Bytes the launches of `name` in one frame step must move at least: inputs read once, outputs written once."""
     w, h, e = wl["w"], wl["h"], wl["n_enc"]
-    n, windows = w * h, (w // 16) * (h // 16)
+    n, windows, pics = w * h, (w // 16) * (h // 16), 1 + wl["n_enc"]
     sp = scale_pixels(w, h)
     table = {
-        "cambi_cvalues": 2.0 * sum(sp) * pics,               # the pictures' 5 scale planes (16-bit words)
-        "cambi_prep0": (2.0 * n + 2.0 * n) * pics,           # plane in, scale-0 words out
-        "cambi_decimate_mode": 4.0 * sum(sp[1:]) / 4 * pics, # mean over the 4 scale launches
+        "cambi_cvalues": 2.0 * sum(sp) * pics,              # every picture's 5 scale planes (16-bit words)
+        "cambi_prep0": (2.0 * n + 2.0 * n) * pics,          # plane in, scale-0 words out
+        "cambi_decimate_mode": 4.0 * sum(sp[1:]) * pics,    # scale s - 1's even rows in, scale s out
         "window_stats": 2.0 * n * (1 + e) + 32.0 * windows * e,
         "persist_stats": 2.0 * n * (2 + 4 + 2 + e) + 20.0 * windows * e,
         "pair_sums": 3.0 * n * (1 + e),
@@ -75,6 +80,14 @@ def algorithmic_bytes(name: str, wl: dict, pics: int = 1) -> float | None:
     return table.get(name)
 
 
+def step_algorithmic_bytes(wl: dict) -> float:
+    """A whole frame step's algorithmic bytes: every input picture read once (4:2:0, 2 bytes a sample at 10 bits, 1 at
+    8) plus the per-window outputs written once (8 window and 5 lasting floats per window and encode)."""
+    w, h, e = wl["w"], wl["h"], wl["n_enc"]
+    b = 2 if wl["pd"] == 10 else 1
+    return (1 + e) * 1.5 * w * h * b + e * (w // 16) * (h // 16) * 13 * 4
+
+
 def read_peaks() -> dict:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -82,6 +95,17 @@ def read_peaks() -> dict:
         return {"hbm_gbs": float(p["hbm_gbs"]), "source": "measured"}
     except (OSError, KeyError, ValueError):
         return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def read_issue(kernel: str, workload: str):
+    """The instruction-issue roofline of a kernel from a one-kernel ncu capture (profiles/issue.json): instructions
+    issued over (SMs x 4 schedulers x SM clock x duration), with the clock and duration of that capture."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "issue.json")) as f:
+            t = json.load(f)
+        return t.get(workload, {}).get(kernel)
+    except (OSError, ValueError):
+        return None
 
 
 def read_traffic(kernel: str, workload: str):
@@ -154,72 +178,133 @@ def make_pool(wl: dict, steps: int, source: int):
     return out
 
 
-_cpu_cache = {}
-STRIP_ROWS = 144  # rows of a 4K frame step per CPU sample (1/15 of the picture)
+STRIP_ROWS = 144   # rows of a frame step per CPU sample (1/15 of a 4K picture)
+CPU_FRAME = 12     # the frame step the CPU samples measure: its lasting texture reads source frames 0 .. 12
 
 
-def cpu_strip(args):
-    """A horizontal strip of one frame step through the CPU oracle (the reference's algorithm restated in C): CAMBI of
-    the source and each encode (window of the full picture), window figures, lasting-texture figures, PSNR squared
-    errors and color sums. Returns (frame pairs measured, as a fraction of whole pictures; seconds)."""
-    wl_name, f, row0, rows = args
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
+def _cpu_frames_dir() -> str:
+    import tempfile
+
+    return tempfile.mkdtemp(prefix="es_cpu_frames_")
+
+
+def cpu_make_frame(args):
+    """Worker: frame step f of the workload, saved as .npy planes under `d` (the source's luma of every frame; every
+    plane of the frames whose figures are measured)."""
+    import numpy as np
 
     import es_synth
 
+    wl_name, f, d = args
     wl = WORKLOADS[wl_name]
-    if (wl_name, f) not in _cpu_cache:
-        _cpu_cache.clear()
-        _cpu_cache[(wl_name, f)] = getattr(es_synth, wl["gen"])(f, w=wl["w"], h=wl["h"])
-    step = _cpu_cache[(wl_name, f)]
+    step = getattr(es_synth, wl["gen"])(f, w=wl["w"], h=wl["h"])
+    np.save(os.path.join(d, f"f{f}_p0_y.npy"), step.source.y)
+    if f in (CPU_FRAME, CPU_FRAME - 6):
+        for i, pic in enumerate([step.source] + list(step.encodes)):
+            for name in ("y", "u", "v"):
+                np.save(os.path.join(d, f"f{f}_p{i}_{name}.npy"), getattr(pic, name))
+    return f
+
+
+def cpu_strip(args):
+    """A horizontal strip of frame step CPU_FRAME through the CPU oracle (the reference's algorithm restated in C):
+    CAMBI of the source and of each encode (with the whole picture's window), window figures, lasting-texture figures
+    over 13 real source frames, PSNR squared errors and color sums, then the host collect of the window and lasting
+    figures into per-segment accumulators. Returns (frame pairs measured, as a fraction of whole pictures; seconds)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    wl_name, d, row0, rows = args
+    wl = WORKLOADS[wl_name]
+    f, n_enc, pd = CPU_FRAME, wl["n_enc"], wl["pd"]
     r0, r1 = row0, min(row0 + rows, wl["h"])
-    crop = lambda a, c=1: a[r0 // c:r1 // c]  # noqa: E731
-    t0 = time.perf_counter()
-    pd = wl["pd"]
+
+    def plane(frame, pic, name):
+        a = np.load(os.path.join(d, f"f{frame}_p{pic}_{name}.npy"), mmap_mode="r")
+        c = 1 if name == "y" else 2
+        return np.ascontiguousarray(a[r0 // c:r1 // c])
+
+    src = [plane(f, 0, n) for n in ("y", "u", "v")]
+    encs = [[plane(f, 1 + e, n) for n in ("y", "u", "v")] for e in range(n_enc)]
+    ring = [plane(k, 0, "y") for k in range(f - 12, f + 1)]
+    centre = [plane(f - 6, 1 + e, "y") for e in range(n_enc)]
     up = 10 - pd
     p = oracle.cambi_params(wl["w"], wl["h"])
-    src = crop(step.source.y)
-    oracle.cambi(src, pd, p)
-    ring = [src] * 13
-    for enc in step.encodes:
-        y = crop(enc.y)
+    acc = [oracle.Accum() for _ in range(n_enc)]
+    t0 = time.perf_counter()
+    oracle.cambi(src[0], pd, p)
+    oracle.color_sums(src[1], src[2], up)
+    for e in range(n_enc):
+        y, u, v = encs[e]
         oracle.cambi(y, pd, p)
-        oracle.window_stats(src, y, up)
-        oracle.persist_stats(ring, y, up)
-        for a, b in ((src, y), (crop(step.source.u, 2), crop(enc.u, 2)), (crop(step.source.v, 2), crop(enc.v, 2))):
+        _, st = oracle.window_stats(src[0], y, up)
+        _, ps = oracle.persist_stats(ring, centre[e], up)
+        for a, b in ((src[0], y), (src[1], u), (src[2], v)):
             oracle.plane_sse(a, b)
-        oracle.color_sums(crop(enc.u, 2), crop(enc.v, 2), up)
-    oracle.color_sums(crop(step.source.u, 2), crop(step.source.v, 2), up)
-    return len(step.encodes) * (r1 - r0) / wl["h"], time.perf_counter() - t0
+        oracle.color_sums(u, v, up)
+        mask = oracle.collect_frame(acc[e], st)
+        oracle.collect_lasting(acc[e], ps, mask)
+    return n_enc * (r1 - r0) / wl["h"], time.perf_counter() - t0
 
 
 class CpuSampler:
-    """A pool of spawned processes, one per host core, each timing strips of frame steps in parallel."""
+    """Spawned processes on the host cores timing strips of a real frame step (generated once by the same processes
+    and kept in a temporary directory): one strip per process and round, side by side, for the all-core rate, and
+    strips one at a time on one process for the 1-core rate."""
 
     def __init__(self, wl_name: str, processes: int):
         import multiprocessing as mp
 
         self.wl, self.n = wl_name, processes
         self.pool = mp.get_context("spawn").Pool(processes)
+        self.dir = _cpu_frames_dir()
+        self.pool.map(cpu_make_frame, [(wl_name, f, self.dir) for f in range(CPU_FRAME + 1)], chunksize=1)
+        self.strips = WORKLOADS[wl_name]["h"] // STRIP_ROWS
         self.round = 0
 
     def sample(self) -> tuple[float, str]:
-        h = WORKLOADS[self.wl]["h"]
-        # the strips of one frame step, in turn (each process makes the step once and keeps it, so later rounds time the
-        # oracle alone and the run's wall time stays short)
-        jobs = [(self.wl, 1000, ((self.round * self.n + i) % (h // STRIP_ROWS)) * STRIP_ROWS, STRIP_ROWS) for i in range(self.n)]
+        """All cores: one strip per process in parallel (the strips of the step in turn); frame pairs / slowest."""
+        jobs = [(self.wl, self.dir, ((self.round * self.n + i) % self.strips) * STRIP_ROWS, STRIP_ROWS) for i in range(self.n)]
         self.round += 1
         res = self.pool.map(cpu_strip, jobs, chunksize=1)
-        busy = max(r[1] for r in res)  # the processes run side by side; frame generation is not timed
+        busy = max(r[1] for r in res)
         pairs = sum(r[0] for r in res)
-        sample = (f"{self.n} strips of {STRIP_ROWS} rows ({pairs:.3f} frame pairs) of {WORKLOADS[self.wl]['desc']}, one strip per "
-                  f"process in parallel, {busy:.2f} s")
-        return pairs / busy, sample
+        return pairs / busy, f"{self.n} strips of {STRIP_ROWS} rows ({pairs:.3f} frame pairs) side by side, {busy:.2f} s"
+
+    def sample_one_core(self, strips: int = 3) -> float:
+        """One process, strips one after another: frame pairs / seconds."""
+        pairs = secs = 0.0
+        for i in range(strips):
+            fp, t = self.pool.apply(cpu_strip, ((self.wl, self.dir, (i % self.strips) * STRIP_ROWS, STRIP_ROWS),))
+            pairs += fp
+            secs += t
+        return pairs / secs
 
     def close(self):
+        import shutil
+
         self.pool.close()
         self.pool.join()
+        shutil.rmtree(self.dir, ignore_errors=True)
+
+
+def cpu_baseline_line(args, cores: int, rounds: int, warmup: int = 1) -> dict:
+    sampler = CpuSampler(args.workload, cores)
+    try:
+        for _ in range(warmup):
+            sampler.sample()
+        vals = [sampler.sample() for _ in range(rounds)]
+        one = sampler.sample_one_core()
+    finally:
+        sampler.close()
+    wl = WORKLOADS[args.workload]
+    value = statistics.median(v for v, _ in vals)
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "value_1_core": one, "rounds": [round(v, 4) for v, _ in vals],
+            "sample": (f"frame step {CPU_FRAME} of {wl['desc']} in strips of {STRIP_ROWS} rows: CAMBI of every picture, window and "
+                       "lasting-texture figures over 13 real source frames, PSNR, color and the host collect; median of "
+                       f"{rounds} rounds of {vals[-1][1]}; value_1_core: 3 strips one after another on one process")}
 
 
 def host_cores() -> int:
@@ -229,14 +314,18 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
+def run_config(wl: dict, world: int) -> dict:
+    """The workload's config, the same in both arms."""
+    return {"workload": wl["desc"], "frame_pairs_per_step": wl["n_enc"],
+            "l2": "inputs larger than L2: distinct frame steps of ~100 MB input cycled", "parallelism": f"replicas x{world}"}
+
+
 def reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     cores = host_cores()
     wl = WORKLOADS[args.workload]
-    cfg = {"workload": wl["desc"], "frame_pairs_per_step": wl["n_enc"],
-           "steps_sampled": f"each step: one {STRIP_ROWS}-row strip of a frame step per host core"}
     sampler = CpuSampler(args.workload, cores)
     for _ in range(args.warmup):
         sampler.sample()
@@ -250,15 +339,18 @@ def reference_arm(args, rank: int, world: int) -> None:
     value = statistics.median(values)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u16/int64", "data": "synthetic (seeded es_synth frames)", "config": cfg,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "vs_baseline": None, "dtype": "u16/int64", "data": "synthetic (seeded es_synth frames, no video decode)",
+            "config": run_config(wl, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": (f"each step: {sample} of frame step {CPU_FRAME} (CAMBI, window and lasting figures over "
+                                        "13 real source frames, PSNR, color, host collect)")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's CPU path for CAMBI is libvmaf and for texture its numpy module; neither runs on the GPU hosts, "
                     "so the plain-C oracle restating the reference's algorithm stands in, over all host cores"}
     print(json.dumps(line), flush=True)
 
 
-def run_c3(args, rank: int, world: int, local: int) -> None:
+def run_c3(args, rank: int, world: int, local: int, module=None, quiet: bool = False) -> dict | None:
     """The uneven batch: 16 source / encode pairs per frame step (6 x 1280x720 8-bit, 6 x 1920x800 10-bit cropped from
     1920x1080 frames with black bars, 4 x 3840x1600 10-bit; es_synth.c3_step), scored as 16 plain es_frame instances
     and as one es_batch (one launch per stage for all 32 pictures, graphs from frame 14, autotuned tiles). Device-
@@ -269,13 +361,18 @@ def run_c3(args, rank: int, world: int, local: int) -> None:
     import es_b200
     import es_synth
 
+    from concurrent.futures import ThreadPoolExecutor
+
     torch.cuda.set_device(local)
     srcs = es_synth.C3_SOURCES
+    with ThreadPoolExecutor(max_workers=min(16, host_cores())) as ex:
+        made = {(f, i): ex.submit(es_synth.c3_step, f, i, w, h, d) for f in range(2) for i, (w, h, d) in enumerate(srcs)}
+        made = {k: v.result() for k, v in made.items()}
     pool = []
     for f in range(2):
         step = []
         for i, (w, h, d) in enumerate(srcs):
-            st = es_synth.c3_step(f, i, w, h, d)
+            st = made[(f, i)]
             fw, fh = es_synth.C3_BARS.get((w, h), (w, h))
             y0 = ((fh - h) // 2) & ~1
             pics = []
@@ -290,7 +387,9 @@ def run_c3(args, rank: int, world: int, local: int) -> None:
             step.append(pics)
         pool.append(step)
     torch.cuda.synchronize()
-    module = es_b200.Module()
+    own_module = module is None
+    if own_module:
+        module = es_b200.Module()
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     pairs = len(srcs) * args.steps
@@ -347,7 +446,8 @@ def run_c3(args, rank: int, world: int, local: int) -> None:
     ms_b, l_b = timed(q_batch, c_batch)
     graphs = batch.graph_launches()
     batch.close()
-    module.close()
+    if own_module:
+        module.close()
     if rank == 0:
         line = {"metric": "frame-pairs/s, 16 uneven source/encode pairs per frame step", "value": pairs / (ms_b / 1000.0),
                 "unit": "frame-pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b / args.steps,
@@ -359,7 +459,10 @@ def run_c3(args, rank: int, world: int, local: int) -> None:
                 "forms": {"plain": {"value": pairs / (ms_plain / 1000.0), "ms_per_step": ms_plain / args.steps, "gpu_launches": int(l_plain)},
                           "batched": {"value": pairs / (ms_b / 1000.0), "ms_per_step": ms_b / args.steps, "gpu_launches": int(l_b),
                                       "graph_steps": int(graphs)}}}
-        print(json.dumps(line), flush=True)
+        if not quiet:
+            print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 def main() -> None:
@@ -373,6 +476,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--only-head", action="store_true", help="time only the headline form (for profiling runs)")
+    ap.add_argument("--no-graphs", action="store_true", help="batched forms launch every kernel (for profiling runs)")
+    ap.add_argument("--no-c3", action="store_true", help="skip the 16-pair uneven batch figures")
     ap.add_argument("--budget", type=float, default=None, help="learned form: score budget of skipped tiles (default: the network's)")
     ap.add_argument("--tolerance", type=float, default=None, help="learned form: audit tolerance (default: the network's)")
     args = ap.parse_args()
@@ -446,7 +551,7 @@ def main() -> None:
         name = "batched (es_batch: one launch per stage for all pictures, steps replayed from CUDA graphs)"
 
         def __init__(self):
-            self.b = es_b200.Batch(module, [(w, h, pd, n_enc)])
+            self.b = es_b200.Batch(module, [(w, h, pd, n_enc)], use_graphs=not args.no_graphs)
 
         def queue(self, f, pics, sh):
             self.b.queue(f, pics, sh)
@@ -630,42 +735,52 @@ def main() -> None:
         fr2.close()
 
     # ---- roofline of the dominant kernel ------------------------------------------------------------------------
+    peaks = read_peaks()
     total_kernel_ms = sum(v[0] for v in times.values()) or 1.0
     top = max(times, key=lambda k: times[k][0]) if times else None
     roofline = None
-    peaks = read_peaks()
     if top:
-        per_launch_ms = times[top][0] / times[top][1]
-        alg = algorithmic_bytes(top, wl, pics=(1 + n_enc) if head != "plain" else 1)
-        achieved = alg / (per_launch_ms / 1000.0) / 1e9 if alg else None
+        # per step: all launches of the kernel in one frame step (with the proposal the c-value kernel runs twice, the
+        # second launch over the fallback tiles only), so bytes per step over the kernel's time per step
+        ms_step = times[top][0] / kernel_steps
+        launches_step = times[top][1] / kernel_steps
+        alg = algorithmic_bytes(top, wl)
+        achieved = alg / (ms_step / 1000.0) / 1e9 if alg else None
+        step_bytes = step_algorithmic_bytes(wl)
         roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": read_traffic(top, f"{args.workload}:{head}"),
-                    "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "peak_source": peaks["source"]}
-    kernels = {k: {"ms_per_step": v[0] / kernel_steps, "launches_per_step": v[1] / kernel_steps, "share": v[0] / total_kernel_ms}
-               for k, v in sorted(times.items(), key=lambda kv: -kv[1][0])}
+                    "algorithmic_bytes_per_step": alg, "ms_per_step": ms_step, "launches_per_step": launches_step,
+                    "peak_source": peaks["source"],
+                    "step": {"algorithmic_bytes": step_bytes, "ms_per_step": ms / args.steps,
+                             "achieved": step_bytes / (ms / args.steps / 1000.0) / 1e9,
+                             "frac": step_bytes / (ms / args.steps / 1000.0) / 1e9 / peaks["hbm_gbs"]},
+                    "issue": read_issue(top, f"{args.workload}:{head}")}
+    kernels = {}
+    for k, v in sorted(times.items(), key=lambda kv: -kv[1][0]):
+        kms = v[0] / kernel_steps
+        kb = algorithmic_bytes(k, wl)
+        kernels[k] = {"ms_per_step": kms, "launches_per_step": v[1] / kernel_steps, "share": v[0] / total_kernel_ms,
+                      "algorithmic_bytes_per_step": kb, "hbm_frac": kb / (kms / 1000.0) / 1e9 / peaks["hbm_gbs"] if kb else None}
 
     # ---- CPU baseline (rank 0, one GPU) -------------------------------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", "1")
-        cores = host_cores()
-        sampler = CpuSampler(args.workload, cores)
-        sampler.sample()  # generation and imports, untimed
-        vals = [sampler.sample() for _ in range(3)]
-        sampler.close()
-        cpu = {"value": statistics.median(v for v, _ in vals), "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "3 rounds of " + vals[-1][1]}
+        cpu = cpu_baseline_line(args, host_cores(), rounds=5)
+
+    # ---- the uneven batch (16 pairs per step): plain vs batched, as extra figures -------------------------------
+    c3 = None
+    if args.workload == "c2" and not args.no_c3 and not args.only_head:
+        c3 = run_c3(args, rank, world, local, module=module, quiet=True)
 
     module.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "u16/int64", "data": "synthetic (seeded es_synth frames, no video decode)",
-                "config": {"workload": wl["desc"], "frame_pairs_per_step": n_enc, "pool_steps": args.pool,
-                           "l2": "inputs larger than L2: 6 distinct steps of ~100 MB input each cycled",
-                           "form": forms[head]["form"], "parallelism": f"replicas x{world}"},
+                "config": run_config(wl, world), "form": forms[head]["form"], "pool_steps": args.pool,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
-                "forms": forms, "kernels": kernels}
+                "forms": forms, "kernels": kernels, "c3": c3}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -1,12 +1,14 @@
 #!/usr/bin/env python3
-"""The c-value tile autotuner: picks, per picture size, the rows of the c-value kernel's tiles at each of CAMBI's five
-scales (64, 32 or 16; tiles are 64 pixels wide), and writes the table es_b200.Batch reads (autotune.json).
+"""The c-value tile autotuner: picks, per picture size, the shape of the c-value kernel's tiles at each of CAMBI's five
+scales -- 64 or 128 columns (blocks of 256 or 512 threads) by 64, 32 or 16 rows -- and writes the table es_b200.Batch
+reads (autotune.json).
 
-Taller tiles stage proportionally less window margin (rows + 2 pad region rows per tile), shorter tiles balance the
-few tiles of the small scales over more blocks; which wins depends on the picture size and window. For each size the
-tuner scores a source and an encode of synthetic content (es_synth: the c2 recipe at 10 bits, c3's at 8), timing the
-c-value launch alone with CUDA events (es_kernel_timing) over a few steps, and runs a coordinate descent: starting
-from 64 rows everywhere, each scale in turn tries 32 and 16 and keeps the fastest when it gains more than 2%.
+Wider and taller tiles stage proportionally less window margin ((columns + 2 pad) x (rows + 2 pad) region pixels per
+tile), smaller tiles balance the few tiles of the small scales over more blocks; which wins depends on the picture size
+and window. For each size the tuner scores a source and an encode of synthetic content (es_synth: the c2 recipe at 10
+bits, c3's at 8), timing the c-value launches alone with CUDA events (es_kernel_timing) over a few steps, and runs a
+coordinate descent: starting from the library's default shapes, each scale in turn tries every shape and keeps the
+fastest when it gains more than 2%.
 """
 
 from __future__ import annotations
@@ -39,7 +41,7 @@ def main() -> None:
     torch.cuda.set_device(0)
     module = es_b200.Module()
     classes = CLASSES if not args.classes else [tuple(int(v) for v in c.split("x")) for c in args.classes.split(",")]
-    table = {"device": torch.cuda.get_device_name(0), "method": "coordinate descent over scales, 2% gain to switch",
+    table = {"device": torch.cuda.get_device_name(0), "method": "coordinate descent over scales and tile shapes, 2% gain to switch",
              "classes": {}}
     stream = torch.cuda.current_stream().cuda_stream
     for (w, h, depth) in classes:
@@ -49,8 +51,8 @@ def main() -> None:
             steps.append(st)
         dev = [es_b200.device_step(torch, st) for st in steps]
 
-        def time_rows(rows):
-            b = es_b200.Batch(module, [(w, h, depth, 1)], use_graphs=False, tuning={(w, h): rows})
+        def time_shape(rows, cols):
+            b = es_b200.Batch(module, [(w, h, depth, 1)], use_graphs=False, tuning={(w, h): {"rows": rows, "cols": cols}})
             acc = [es_b200.new_accum()]
             f = 0
             for _ in range(2):
@@ -70,21 +72,24 @@ def main() -> None:
             return times["cambi_cvalues"][0] / args.steps
 
         t0 = time.time()
-        best = [64] * 5
-        best_ms = time_rows(best)
+        rows, cols = [64] * 5, [128, 128, 64, 64, 64]  # the library's defaults
+        best_ms = time_shape(rows, cols)
         base_ms = best_ms
-        tried = [[list(best), best_ms]]
+        tried = [[list(rows), list(cols), best_ms]]
         for s in range(5):
-            for r in (32, 16):
-                cand = list(best)
-                cand[s] = r
-                ms = time_rows(cand)
-                tried.append([cand, ms])
-                if ms < best_ms * 0.98:
-                    best, best_ms = cand, ms
-        table["classes"][f"{w}x{h}"] = {"depth": depth, "cv_tile_rows": best, "cvalues_ms": best_ms, "cvalues_ms_all_64": base_ms,
-                                        "tried": tried, "seconds": time.time() - t0}
-        print(f"{w}x{h}@{depth}: {best} {best_ms:.3f} ms (all 64: {base_ms:.3f} ms)", flush=True)
+            for c in (128, 64):
+                for r in (64, 32, 16):
+                    if (r, c) == (rows[s], cols[s]):
+                        continue
+                    cr, cc = list(rows), list(cols)
+                    cr[s], cc[s] = r, c
+                    ms = time_shape(cr, cc)
+                    tried.append([cr, cc, ms])
+                    if ms < best_ms * 0.98:
+                        rows, cols, best_ms = cr, cc, ms
+        table["classes"][f"{w}x{h}"] = {"depth": depth, "cv_tile_rows": rows, "cv_tile_cols": cols, "cvalues_ms": best_ms,
+                                        "cvalues_ms_defaults": base_ms, "tried": tried, "seconds": time.time() - t0}
+        print(f"{w}x{h}@{depth}: rows {rows} cols {cols} {best_ms:.3f} ms (defaults: {base_ms:.3f} ms)", flush=True)
     with open(args.out, "w") as fh:
         json.dump(table, fh, indent=1)
     module.close()

@@ -52,6 +52,7 @@ struct Picture {
     int source = 0, encode = -1;  // encode -1: the source's own picture
     int w = 0, h = 0, depth = 10;
     int tile_rows[kScales] = {64, 64, 64, 64, 64};  // c-value tile rows per scale
+    int tile_cols[kScales] = {64, 64, 64, 64, 64};  // c-value tile columns per scale
     float *cv_plane[kScales] = {};                   // optional: every computed c-value at its pixel (tests)
     es_cambi_params p{};
     int sw[kScales], sh[kScales];
@@ -395,7 +396,8 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
             j.w = pic.sw[sc];
             j.h = pic.sh[sc];
             j.pad = pic.p.pad;
-            j.tiles_x = (j.w + kCvTX - 1) / kCvTX;
+            j.tile_cols = b.net ? kCvTX : pic.tile_cols[sc];  // the proposal maps 64-column tiles
+            j.tiles_x = (j.w + j.tile_cols - 1) / j.tile_cols;
             j.first_tile = tiles;
             j.slot = i * kScales + sc;
             j.plane = pic.cv_plane[sc];
@@ -656,7 +658,7 @@ int es_batch_create(const es_module *m, int n_sources, const es_batch_source *so
 {
     return guarded([&] {
         require(m != nullptr && sources != nullptr && out != nullptr, "es_batch_create: NULL argument");
-        require(n_sources >= 1 && n_sources <= kMaxSources, "es_batch_create: 1 to 16 sources");
+        require(n_sources >= 1 && n_sources <= kMaxSources, "es_batch_create: 1 to 32 sources");
         int pictures = 0;
         for (int i = 0; i < n_sources; i++) {
             const es_batch_source &d = sources[i];
@@ -666,7 +668,7 @@ int es_batch_create(const es_module *m, int n_sources, const es_batch_source *so
             require(d.n_encodes >= 1 && d.n_encodes <= kMaxEncodes, "es_batch_create: 1 to 16 encodes per source");
             pictures += 1 + d.n_encodes;
         }
-        require(pictures <= kMaxBatchPictures, "es_batch_create: at most 32 pictures (sources and encodes) per batch");
+        require(pictures <= kMaxBatchPictures, "es_batch_create: at most 64 pictures (sources and encodes) per batch");
         check_device();
         auto b = std::make_unique<es_batch>();
         if (options) b->use_graphs = options->use_graphs != 0;
@@ -687,6 +689,9 @@ int es_batch_create(const es_module *m, int n_sources, const es_batch_source *so
                     const int r = sources[i].cv_tile_rows[sc];
                     require(r == 0 || r == 16 || r == 32 || r == 64, "es_batch_create: c-value tile rows must be 0, 16, 32 or 64");
                     pic->tile_rows[sc] = r ? r : 64;
+                    const int c = sources[i].cv_tile_cols[sc];
+                    require(c == 0 || c == 64 || c == 128, "es_batch_create: c-value tile columns must be 0, 64 or 128");
+                    pic->tile_cols[sc] = c ? c : cv_default_tile_cols(sc);
                 }
                 b->pictures.push_back(std::move(pic));
             }
@@ -790,6 +795,18 @@ int es_batch_read_windows(es_batch *b, int source, int encode, float *stats, flo
             require(b->last_collected >= 2 * kRadius, "es_batch_read_windows: no lasting texture before frame 12");
             cuda_check(cudaMemcpy(persist, S.persist[at].ptr + (size_t)encode * win * kPersist, win * kPersist * 4, cudaMemcpyDeviceToHost), "reading");
         }
+    });
+}
+
+int es_batch_luma(const es_batch *b, int picture, long f, uint64_t *address)
+{
+    return guarded([&] {
+        require(b != nullptr && address != nullptr, "es_batch_luma: NULL argument");
+        require(picture >= 0 && picture < (int)b->pictures.size(), "es_batch_luma: picture out of range");
+        const long ring = b->pictures[picture]->encode < 0 ? kRing : kEncRing;
+        if (f < 0 || f >= b->next || f + ring < b->next)
+            throw Error(ES_ERR_STATE, "es_batch_luma: frame " + std::to_string(f) + " is not in the ring");
+        *address = (uint64_t)luma_of(*b, picture, f);
     });
 }
 

@@ -120,7 +120,8 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
         j.w = c->sw[sc];
         j.h = c->sh[sc];
         j.pad = p.pad;
-        j.tiles_x = (j.w + kCvTX - 1) / kCvTX;
+        j.tile_cols = c->tile_mass ? kCvTX : cv_default_tile_cols(sc);  // per-tile masses are counted on 64 x 64 tiles
+        j.tiles_x = (j.w + j.tile_cols - 1) / j.tile_cols;
         j.first_tile = tiles;
         j.slot = sc;
         j.plane = c->planes[sc];

@@ -44,8 +44,7 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
     __shared__ __align__(16) uint16_t pre8[kP0R - 1][kP0C];
     __shared__ uint32_t flatbits[kP0F][3];
     __shared__ uint32_t needbits[32];
-    int j = 0;
-    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_tile) j++;
+    const int j = find_job(b.njobs, (int)blockIdx.x, [&](int k) { return b.job[k].first_tile; });
     const Prep0Job &J = b.job[j];
     const int t = blockIdx.x - J.first_tile, w = J.w, h = J.h, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -199,8 +198,7 @@ constexpr int kDTW = 64, kDTH = 16;
 __global__ void __launch_bounds__(256) decimate_mode_kernel(const __grid_constant__ DecBatch b)
 {
     __shared__ uint16_t d[kDTH + 2][kDTW + 2];
-    int j = 0;
-    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
+    const int j = find_job(b.njobs, (int)blockIdx.x, [&](int k) { return b.job[k].first_block; });
     const DecJob &J = b.job[j];
     const int w = J.w, h = J.h, tiles_x = (w + kDTW - 1) / kDTW, t = blockIdx.x - J.first_block;
     const int x0 = (t % tiles_x) * kDTW, y0 = (t / tiles_x) * kDTH;

@@ -27,42 +27,42 @@ namespace es {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kCvChunk = kCvThreads / kCvTX;  // rows whose c-values are computed together
+constexpr int kCvChunk = 4;                   // rows whose c-values are computed together (threads = 4 x tile width)
 constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
-constexpr int kWarps = kCvThreads / 32;
 constexpr unsigned kNoRank = 0xFFu;           // rank plane: no relevant code
 constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks can hold
 
-__host__ __device__ constexpr int cv_rw(int pad) { return kCvTX + 2 * pad; }
+// Tiles are TX columns wide (64 or 128); a block has 4 TX threads.
+__host__ __device__ constexpr int cv_rw(int tx, int pad) { return tx + 2 * pad; }
 // the staged region starts at the multiple of 8 at or left of x0 - pad; its row stride is a whole number of vectors
-__host__ __device__ constexpr int cv_stride(int pad) { return (cv_rw(pad) + 7 + 7) & ~7; }
-__host__ __device__ constexpr int cv_cs(int pad) { return (cv_rw(pad) + 127) & ~127; }  // rank plane row
+__host__ __device__ constexpr int cv_stride(int tx, int pad) { return (cv_rw(tx, pad) + 7 + 7) & ~7; }
+__host__ __device__ constexpr int cv_cs(int tx, int pad) { return (cv_rw(tx, pad) + 127) & ~127; }  // rank plane row
 // k-steps of 32 region columns, and the row of the column counts (bytes; 16 more than the k-steps, so the 8 rows an
 // ldmatrix phase reads fall on different banks)
-__host__ __device__ constexpr int cv_nk(int pad) { return (cv_rw(pad) + 31) >> 5; }
-__host__ __device__ constexpr int cv_cstr(int pad) { return 32 * cv_nk(pad) + 16; }
-constexpr int kCvMaxK = cv_nk(kMaxPad);
-constexpr int kCvWS = kCvTX + 2;  // window-count row (u16): an odd number of words, so ranks fall on different banks
+__host__ __device__ constexpr int cv_nk(int tx, int pad) { return (cv_rw(tx, pad) + 31) >> 5; }
+__host__ __device__ constexpr int cv_cstr(int tx, int pad) { return 32 * cv_nk(tx, pad) + 16; }
+// k-steps one warp's window reaches (its 8 output columns and 2 pad more), at most
+constexpr int kCvMaxK = (8 + 2 * kMaxPad + 31) / 32 + 1;
+__host__ __device__ constexpr int cv_ws(int tx) { return tx + 2; }  // window-count row (u16): an odd number of words
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 // Shared memory: the rank plane, the per-code and per-rank tables and the pass buffers. (The band codes are read from
 // global memory twice, once for the code tables and once for the rank plane, instead of being staged: the smaller
 // footprint lets 4 blocks share an SM.)
 struct CvLayout {
-    size_t rplane, rank, rcode, nbr, relneed, wcount, cols, list, total;
+    size_t rplane, rank, nbr, relneed, wcount, cols, list, total;
 };
-__host__ __device__ inline CvLayout cv_layout(int pad)
+__host__ __device__ inline CvLayout cv_layout(int tx, int pad)
 {
     const size_t rh = (size_t)kCvTY + 2 * pad;
     CvLayout l;
     // the rank plane, window counts and column counts first: until the plane is built they hold the region's band
     // codes (16 bits each) when those fit
     l.rplane = 0;
-    l.wcount = align16(l.rplane + rh * cv_cs(pad));
-    l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * kCvWS * 2);
-    l.rank = align16(l.cols + (size_t)kCvBins * cv_cstr(pad));
-    l.rcode = align16(l.rank + (size_t)kMaxBand * 2);
-    l.nbr = align16(l.rcode + (size_t)kMaxBand * 2);
+    l.wcount = align16(l.rplane + rh * cv_cs(tx, pad));
+    l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * cv_ws(tx) * 2);
+    l.rank = align16(l.cols + (size_t)kCvBins * cv_cstr(tx, pad));
+    l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
     l.list = align16(l.relneed + (size_t)kMaxBand * 2);
     l.total = align16(l.list + (size_t)kListCap * 4);
@@ -85,8 +85,11 @@ __device__ __forceinline__ void mma_u8(int (&d)[4], uint32_t a0, uint32_t a1, ui
                  : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-__global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_constant__ CvBatch b)
+template <int TX>
+__global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_constant__ CvBatch b)
 {
+    constexpr int kCvThreads = 4 * TX, kWarps = kCvThreads / 32, kCvWS = cv_ws(TX);
+    constexpr int kQuads = TX / 4;  // 4-pixel groups of a tile row
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t occ[32], srv[32], rel[32], needbits[32];
     __shared__ uint16_t relpre[33];
@@ -99,34 +102,32 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
     __shared__ unsigned next_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const Band &bd = b.band;
-    // the codes whose c-value is needed (some d has value <= tvi[d] and value + d + 1 > vlt): warp w, words w + 8 k
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int code = (warp + 8 * k) * 32 + lane;
+    // the codes whose c-value is needed (some d has value <= tvi[d] and value + d + 1 > vlt): warp w, words w + kWarps k
+    for (int word = warp; word < 32; word += kWarps) {
+        const int code = word * 32 + lane;
         const unsigned m = __ballot_sync(kFull, code < bd.band_size && needs_cvalue(code, bd));
-        if (lane == 0) needbits[warp + 8 * k] = m;
+        if (lane == 0) needbits[word] = m;
     }
     __syncthreads();
     auto needed = [&](unsigned code) { return (needbits[code >> 5] >> (code & 31)) & 1u; };
 
   // one tile, gt its global number; all threads return together
   auto tile_body = [&](const int gt) {
-    int j = 0;
-    while (j + 1 < b.njobs && gt >= b.job[j + 1].first_tile) j++;
+    const int j = find_job(b.njobs, gt, [&](int k) { return b.job[k].first_tile; });
     const CvJob &J = b.job[j];
     if (b.run && !b.run[J.run_index]) return;
     const int tile = gt - J.first_tile;
     const int th = J.tile_rows ? J.tile_rows : kCvTY;  // shorter tiles use the same buffers, like a picture's last row
-    const int x0 = (tile % J.tiles_x) * kCvTX, y0 = (tile / J.tiles_x) * th;
+    const int x0 = (tile % J.tiles_x) * TX, y0 = (tile / J.tiles_x) * th;
     const int w = J.w, h = J.h, P = J.pad;
-    const int rows = min(th, h - y0), cols = min(kCvTX, w - x0);
+    const int rows = min(th, h - y0), cols = min(TX, w - x0);
     const bool vec = (w & 7) == 0 && (((uintptr_t)J.word) & 15) == 0;  // rows of 16-byte vectors
 
     // 1. does any pixel of the tile need a c-value?
     bool any = false;
-    if (vec && cols == kCvTX) {
-        for (int i = tid; i < kCvTY * (kCvTX / 8); i += kCvThreads) {
-            const int r = i >> 3, v = i & 7;
+    if (vec && cols == TX) {
+        for (int i = tid; i < kCvTY * (TX / 8); i += kCvThreads) {
+            const int r = i / (TX / 8), v = i % (TX / 8);
             if (r >= rows) continue;
             const uint4 q = __ldg((const uint4 *)(J.word + (size_t)(y0 + r) * w + x0) + v);
             auto test = [&](unsigned word) {
@@ -139,8 +140,8 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             test(q.w);
         }
     } else {
-        for (int i = tid; i < kCvTX * kCvTY; i += kCvThreads) {
-            const int r = i >> 6, c = i & (kCvTX - 1);
+        for (int i = tid; i < TX * kCvTY; i += kCvThreads) {
+            const int r = i / TX, c = i % TX;
             if (r < rows && c < cols) {
                 const uint16_t code = code_of(J.word[(size_t)(y0 + r) * w + x0 + c], bd);
                 any |= code != kNone && needed(code);
@@ -152,12 +153,11 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         return;
     }
 
-    const int RW = cv_rw(P), RH = rows + 2 * P, CS = cv_cs(P), S = cv_stride(P);
+    const int RW = cv_rw(TX, P), RH = rows + 2 * P, CS = cv_cs(TX, P), S = cv_stride(TX, P);
     const int xs = ((x0 - P) >> 3) << 3, ox = (x0 - P) - xs;  // region start (aligned) and the offset of x0 - P in it
-    const CvLayout L = cv_layout(P);
+    const CvLayout L = cv_layout(TX, P);
     uint8_t *rplane = smem + L.rplane;                   // [RH][CS]: rank (- offset) of pixel (x0 - P + j, y0 - P + r)
     uint16_t *rank = (uint16_t *)(smem + L.rank);        // code -> rank
-    uint16_t *rcode = (uint16_t *)(smem + L.rcode);      // rank -> code
     uint32_t *nbr = (uint32_t *)(smem + L.nbr);          // rank -> neighbour rank offsets
     uint16_t *relneed = (uint16_t *)(smem + L.relneed);  // rank -> ranks read (bit 4: itself); 0: not served
     float *blist = (float *)(smem + L.list);
@@ -243,13 +243,14 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         rank[c] = (word & bit) ? (uint16_t)(relpre[c >> 5] + __popc(word & (bit - 1u))) : kNone;
     }
     __syncthreads();
-    // per rank: its code; for a served code the rank offsets (+4) of its neighbours u-4 .. u-1, u+1 .. u+4 (15 = none)
-    // and the mask of the ranks rank-4 .. rank+4 its c-value reads (bit 4 is its own)
+    // per rank of a served code: the rank offsets (+4) of the neighbours u-4 .. u-1, u+1 .. u+4 its c-value
+    // reads (15 = none: not in the region, or at a distance d + 1 whose diff CAMBI's thresholds switch off for this
+    // code, which gives the same c-value as a neighbour with no pixels) and the mask of the ranks rank-4 .. rank+4 read
+    // (bit 4 is its own)
     bool any_served = false;
     for (int c = tid; c < bd.band_size; c += kCvThreads) {
         const int rc = rank[c];
         if (rc == kNone) continue;
-        rcode[rc] = (uint16_t)c;
         if (!(srv[c >> 5] & (1u << (c & 31)))) {
             relneed[rc] = 0;
             continue;
@@ -262,9 +263,9 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             const int q = c + (i < 4 ? i - 4 : i - 3);
             const int d = i < 4 ? 3 - i : i - 4;  // distance d + 1
             unsigned nib = 15u;
-            if (q >= 0 && q < bd.band_size && rank[q] != kNone) {
+            if (q >= 0 && q < bd.band_size && rank[q] != kNone && ((dists >> d) & 1u)) {
                 nib = (unsigned)((int)rank[q] - rc + 4);
-                if ((dists >> d) & 1u) mask |= 1u << nib;
+                mask |= 1u << nib;
             }
             packed |= nib << (4 * i);
         }
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
     // m tiles), over the k-steps of 32 region columns its window reaches.
     uint8_t *colc = smem + L.cols;                       // [rank][CSTR]: column counts of the pass's ranks
     uint16_t *wc16 = (uint16_t *)(smem + L.wcount);      // [chunk row][rank][kCvWS]: window counts
-    const int NK = cv_nk(P), CSTR = cv_cstr(P);
+    const int NK = cv_nk(TX, P), CSTR = cv_cstr(TX, P);
     const int g = lane >> 2, t = lane & 3;
     const int ks_lo = (8 * warp) >> 5, ks_hi = min(NK - 1, (8 * warp + 7 + 2 * P) >> 5);
     uint32_t bfrag[kCvMaxK][2];  // this lane's B fragments: rows (region columns) 32 (ks_lo + kk) + 16 r + 4 t + i,
@@ -375,10 +376,10 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
         if (tid < kCvTY) rowneed[tid] = 0;
         for (int i = tid; i < kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
         __syncthreads();
-        // the pass ranks each row's pixels read: first the served pass ranks present in each row (16 lanes per row, 4
-        // pixels per lane from two aligned words of the rank plane), then, per row, the ranks those read
-        for (int i = tid; i < kCvTY * (kCvTX / 4); i += kCvThreads) {
-            const int r = i >> 4, q = i & 15;
+        // the pass ranks each row's pixels read: first the served pass ranks present in each row (TX / 4 lanes per
+        // row, 4 pixels per lane from two aligned words of the rank plane), then, per row, the ranks those read
+        for (int i = tid; i < kCvTY * kQuads; i += kCvThreads) {
+            const int r = i / kQuads, q = i % kQuads;
             uint32_t bits = 0;
             if (r < rows) {
                 const int at = (r + P) * CS + P + 4 * q;  // tile columns 4 q .. 4 q + 3
@@ -392,8 +393,8 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
                 }
             }
 #pragma unroll
-            for (int o = 8; o; o >>= 1) bits |= __shfl_xor_sync(kFull, bits, o);
-            if ((lane & 15) == 0 && r < kCvTY) rowneed[r] = bits;
+            for (int o = kQuads / 2; o; o >>= 1) bits |= __shfl_xor_sync(kFull, bits, o);
+            if ((lane & (kQuads - 1)) == 0 && r < kCvTY) rowneed[r] = bits;
         }
         __syncthreads();
         if (tid < rows) {
@@ -462,7 +463,7 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
             default: window_counts_n(std::integral_constant<int, 6>{}, i, need); break;
             }
         };
-        const int ci = tid >> 6, cc = tid & (kCvTX - 1);  // this thread's pixel in a chunk
+        const int ci = tid / TX, cc = tid % TX;  // this thread's pixel in a chunk
         for (int r0 = 0; r0 < rows; r0 += kCvChunk) {
             const int n_rows = min(kCvChunk, rows - r0);
             bool chunk_any = false;
@@ -499,15 +500,15 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
                         const int base = k - 4;
                         const uint16_t *wc = wc16 + (size_t)ci * kCvBins * kCvWS + cc;
                         auto count = [&](int kk) -> unsigned { return wc[kk * kCvWS]; };
-                        const int value = rcode[rk] + bd.band_base + kDiffs;
                         const unsigned p0 = count(k);
+                        // a diff with no neighbour (pm = 0) gives 0, which never raises c
 #pragma unroll
                         for (int d = 0; d < kDiffs; d++) {
-                            if (value <= bd.tvi[d] && value + d + 1 > bd.vlt) {
-                                const unsigned o1 = (nb >> (4 * (4 + d))) & 15u, o2 = (nb >> (4 * (3 - d))) & 15u;
-                                const unsigned p1 = o1 != 15u ? count(base + (int)o1) : 0u;
-                                const unsigned p2 = o2 != 15u ? count(base + (int)o2) : 0u;
-                                const unsigned pm = p1 > p2 ? p1 : p2;
+                            const unsigned o1 = (nb >> (4 * (4 + d))) & 15u, o2 = (nb >> (4 * (3 - d))) & 15u;
+                            const unsigned p1 = o1 != 15u ? count(base + (int)o1) : 0u;
+                            const unsigned p2 = o2 != 15u ? count(base + (int)o2) : 0u;
+                            const unsigned pm = p1 > p2 ? p1 : p2;
+                            if (pm) {
                                 const float val = __fmul_rn(__uint2float_rn((unsigned)bd.weight[d] * p0 * pm), __ldg(b.lut + p0 + pm));
                                 if (val > c) c = val;
                             }
@@ -580,20 +581,54 @@ __global__ void __launch_bounds__(kCvThreads, 4) cvalues_kernel(const __grid_con
 
 }  // namespace
 
-size_t cvalues_smem_bytes(int max_pad) { return cv_layout(max_pad).total; }
+size_t cvalues_smem_bytes(int max_pad, int tile_cols) { return cv_layout(tile_cols == 128 ? 128 : 64, max_pad).total; }
+
+namespace {
+template <int TX>
+cudaError_t launch_cvalues_tx(const CvBatch &b, cudaStream_t s)
+{
+    const size_t smem = cvalues_smem_bytes(b.max_pad, TX);
+    cudaError_t e = cudaFuncSetAttribute(cvalues_kernel<TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    LaunchTimer t("cambi_cvalues", s);
+    const int list_blocks = kCvListBlocks * 64 / TX;  // the same threads per SM for either width
+    const int grid = b.tiles ? (b.total_tiles < list_blocks ? b.total_tiles : list_blocks) : b.total_tiles;
+    cvalues_kernel<TX><<<grid, 4 * TX, smem, s>>>(b);
+    return after_launch();
+}
+
+int tile_cols_of(const CvJob &j) { return j.tile_cols == 128 ? 128 : 64; }
+}  // namespace
 
 cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s)
 {
     if (b.total_tiles <= 0) return cudaSuccess;
-    const size_t smem = cvalues_smem_bytes(b.max_pad);
-    cudaError_t e = cudaFuncSetAttribute(cvalues_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    LaunchTimer t("cambi_cvalues", s);
-    const int grid = b.tiles ? (b.total_tiles < kCvListBlocks ? b.total_tiles : kCvListBlocks) : b.total_tiles;
-    cvalues_kernel<<<grid, kCvThreads, smem, s>>>(b);
-    return after_launch();
+    bool has64 = false, has128 = false;
+    for (int j = 0; j < b.njobs; j++) (tile_cols_of(b.job[j]) == 128 ? has128 : has64) = true;
+    if (!(has64 && has128)) return has128 ? launch_cvalues_tx<128>(b, s) : launch_cvalues_tx<64>(b, s);
+    // tiles of both widths: one launch per width, each over its own jobs (a tile list or per-tile masses name tiles
+    // of one numbering, so they need one width)
+    if (b.tiles || b.tile_mass) return cudaErrorInvalidValue;
+    for (int width : {128, 64}) {
+        CvBatch sub = b;
+        sub.njobs = 0;
+        int tiles = 0;
+        for (int j = 0; j < b.njobs; j++) {
+            if (tile_cols_of(b.job[j]) != width) continue;
+            CvJob job = b.job[j];
+            const int th = job.tile_rows ? job.tile_rows : kCvTY;
+            job.first_tile = tiles;
+            tiles += job.tiles_x * ((job.h + th - 1) / th);
+            sub.job[sub.njobs++] = job;
+        }
+        sub.total_tiles = tiles;
+        if (tiles == 0) continue;
+        const cudaError_t e = width == 128 ? launch_cvalues_tx<128>(sub, s) : launch_cvalues_tx<64>(sub, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
-const void *kernel_entry_cvalues() { return (const void *)cvalues_kernel; }
+const void *kernel_entry_cvalues() { return (const void *)cvalues_kernel<64>; }
 
 }  // namespace es

@@ -43,8 +43,24 @@ constexpr uint16_t kMaskBit = 0x8000;  // a scale's plane holds value | mask << 
 constexpr int kMaxBand = 1024;         // codes of a 10-bit pipeline
 constexpr int kMaxPad = 64;            // window 129
 constexpr int kMaxPictures = 64;       // pictures in one batched launch
-constexpr int kMaxJobs = 160;          // pictures x scales in one c-value launch
+constexpr int kMaxJobs = kMaxPictures * 5;  // pictures x scales in one c-value launch
 constexpr int kWin = 16;               // detail window side (src/kernels.cu:331)
+
+#ifdef __CUDACC__
+// The job whose range of blocks or tiles holds t: the last job j with first(j) <= t, by binary search over a job
+// table whose first blocks do not decrease (a job without blocks shares its first with the next).
+template <typename First>
+__device__ __forceinline__ int find_job(int njobs, int t, First first)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t >= first(mid)) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+#endif
 
 // CAMBI's band parameters (src/kernels.cu:65-69 CambiParams without the per-scale size).
 struct Band {
@@ -110,6 +126,7 @@ struct CvJob {
     float *plane;   // optional: every computed c-value at its pixel
     int run_index;  // the entry of CvBatch::run that gates this job (with a run table)
     int tile_rows;  // rows of this job's tiles: 64 (0 means 64), 32 or 16; tiles are numbered row by row
+    int tile_cols;  // columns of this job's tiles: 64 (0 means 64) or 128 (tiles_x counts tiles of this width)
 };
 struct CvBatch {
     CvJob job[kMaxJobs];
@@ -130,7 +147,10 @@ struct CvBatch {
 // Blocks of a tile-list launch.
 constexpr int kCvListBlocks = 148 * 4;
 constexpr int kCvTX = 64, kCvTY = 64, kCvThreads = 256, kCvBins = 32;
-size_t cvalues_smem_bytes(int max_pad);
+size_t cvalues_smem_bytes(int max_pad, int tile_cols);
+// The c-value tile width of a scale when nothing else asks for one: 128 columns where pictures are wide (scales 0 and
+// 1: the staged margins cost less per output pixel), 64 below (more, shorter-lived tiles for the small scales).
+inline int cv_default_tile_cols(int scale) { return scale < 2 ? 128 : 64; }
 cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s);
 
 // ---- top-k pooling and score -------------------------------------------------------------------------------------
@@ -182,6 +202,20 @@ struct UnpackBatch {
 };
 cudaError_t launch_unpack(const UnpackBatch &b, cudaStream_t s);
 
+// ---- the VMAF picture feed (src/kernels.cu:537-545) -------------------------------------------------------------
+struct PictureJob {
+    const uint16_t *src;  // w x h values, rows of w
+    void *dst;            // rows of `pitch` bytes, `bytes` (1 or 2) per sample
+    int w, h, pitch, bytes;
+    int first_block;      // set by the launcher
+};
+constexpr int kPictureMaxJobs = kMaxPictures;
+struct PictureBatch {
+    PictureJob job[kPictureMaxJobs];
+    int njobs;
+};
+cudaError_t launch_to_pictures(PictureBatch &b, cudaStream_t s);
+
 // ---- detail window statistics ------------------------------------------------------------------------------------
 constexpr int kMaxEncodes = 16;
 struct WindowJob {
@@ -192,7 +226,7 @@ struct WindowJob {
     int first_block;                    // set by the launcher
 };
 // Per-source work of a frame step for up to kMaxSources sources in one launch.
-constexpr int kMaxSources = 16;
+constexpr int kMaxSources = 32;
 struct WindowBatch {
     WindowJob job[kMaxSources];
     int njobs;

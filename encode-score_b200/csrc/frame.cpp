@@ -425,6 +425,35 @@ int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist
     });
 }
 
+int es_frame_luma(const es_frame *fr, int p, long f, uint64_t *address)
+{
+    return guarded([&] {
+        require(fr != nullptr && address != nullptr, "es_frame_luma: NULL argument");
+        require(p >= 0 && p <= fr->nenc, "es_frame_luma: picture out of range");
+        const long ring = p == 0 ? kRing : kEncRing;
+        if (f < 0 || f >= fr->next || f + ring < fr->next)
+            throw Error(ES_ERR_STATE, "es_frame_luma: frame " + std::to_string(f) + " is not in the ring");
+        *address = (uint64_t)(p == 0 ? fr->src_plane(f) : fr->enc_plane(p - 1, f));
+    });
+}
+
+int es_to_pictures(const es_picture_copy *copies, int n, void *stream)
+{
+    return guarded([&] {
+        require(copies != nullptr && n >= 1 && n <= kPictureMaxJobs, "es_to_pictures: 1 to 64 copies");
+        PictureBatch pb{};
+        for (int i = 0; i < n; i++) {
+            const es_picture_copy &c = copies[i];
+            require(c.src != 0 && c.dst != 0, "es_to_pictures: NULL plane or picture");
+            require(c.w > 0 && c.h > 0, "es_to_pictures: empty plane");
+            require(c.bytes == 1 || c.bytes == 2, "es_to_pictures: samples must be 1 or 2 bytes");
+            require(c.pitch >= c.w * c.bytes, "es_to_pictures: pitch is smaller than a row");
+            pb.job[pb.njobs++] = PictureJob{(const uint16_t *)c.src, (void *)c.dst, c.w, c.h, c.pitch, c.bytes, 0};
+        }
+        cuda_check(launch_to_pictures(pb, (cudaStream_t)stream), "copying pictures");
+    });
+}
+
 void es_frame_destroy(es_frame *fr)
 {
     if (!fr) return;

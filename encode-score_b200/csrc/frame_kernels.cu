@@ -28,8 +28,7 @@ __device__ __forceinline__ unsigned sample_at(const void *plane, int pitch, int 
 // (semi-planar, shifted samples such as P010, odd alignments) one sample at a time.
 __global__ void __launch_bounds__(256) unpack_kernel(const __grid_constant__ UnpackBatch b)
 {
-    int j = 0;
-    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
+    const int j = find_job(b.njobs, (int)blockIdx.x, [&](int k) { return b.job[k].first_block; });
     const UnpackJob &J = b.job[j];
     const FrameViewDev f = b.views ? b.views[j].f : J.f;
     const int x0 = b.views ? b.views[j].x0 : J.x0, y0 = b.views ? b.views[j].y0 : J.y0;
@@ -839,6 +838,70 @@ cudaError_t launch_collect(CollectBatch &b, cudaStream_t s)
 {
     const cudaError_t e = launch_collect_threshold(b, s);
     return e != cudaSuccess ? e : launch_collect_sums(b, s);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// The VMAF picture feed: src/kernels.cu:537-545 (to_picture), one launch for every plane of a step. A thread moves 8
+// samples of a row: one 16-byte load of the 16-bit values, and one 8-byte (8-bit picture) or 16-byte store where the
+// destination row allows, else sample by sample. An 8-bit picture keeps the low byte of each value, as the reference.
+// ---------------------------------------------------------------------------------------------------------------
+namespace {
+constexpr int kPicThreads = 256;
+
+__global__ void __launch_bounds__(kPicThreads) to_pictures_kernel(const __grid_constant__ PictureBatch b)
+{
+    const int j = find_job(b.njobs, (int)blockIdx.x, [&](int k) { return b.job[k].first_block; });
+    const PictureJob &J = b.job[j];
+    const int groups = (J.w + 7) / 8;  // 8-sample groups per row
+    const long long i = (long long)(blockIdx.x - J.first_block) * kPicThreads + threadIdx.x;
+    if (i >= (long long)groups * J.h) return;
+    const int y = (int)(i / groups), x = (int)(i - (long long)y * groups) * 8;
+    const uint16_t *src = J.src + (size_t)y * J.w + x;
+    char *row = (char *)J.dst + (size_t)y * J.pitch;
+    const bool src_vec = (J.w & 7) == 0 && (((uintptr_t)J.src) & 15) == 0;
+    if (src_vec && x + 8 <= J.w) {
+        const uint4 q = __ldg((const uint4 *)src);
+        if (J.bytes == 1) {
+            uint8_t *d = (uint8_t *)row + x;
+            const uint2 v = make_uint2(__byte_perm(q.x, q.y, 0x6420), __byte_perm(q.z, q.w, 0x6420));
+            if ((((uintptr_t)d) & 7) == 0) {
+                *(uint2 *)d = v;
+            } else {
+                for (int k = 0; k < 4; k++) d[k] = (uint8_t)(v.x >> (8 * k));
+                for (int k = 0; k < 4; k++) d[4 + k] = (uint8_t)(v.y >> (8 * k));
+            }
+        } else {
+            uint16_t *d = (uint16_t *)row + x;
+            if ((((uintptr_t)d) & 15) == 0) {
+                *(uint4 *)d = q;
+            } else {
+                const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+                for (int k = 0; k < 8; k++) d[k] = (uint16_t)(w4[k >> 1] >> (16 * (k & 1)));
+            }
+        }
+        return;
+    }
+    for (int k = 0; k < 8 && x + k < J.w; k++) {
+        const uint16_t v = src[k];
+        if (J.bytes == 1) ((uint8_t *)row)[x + k] = (uint8_t)v;
+        else ((uint16_t *)row)[x + k] = v;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_to_pictures(PictureBatch &b, cudaStream_t s)
+{
+    int blocks = 0;
+    for (int j = 0; j < b.njobs; j++) {
+        PictureJob &J = b.job[j];
+        J.first_block = blocks;
+        blocks += (int)(((long long)((J.w + 7) / 8) * J.h + kPicThreads - 1) / kPicThreads);
+    }
+    if (blocks <= 0) return cudaSuccess;
+    LaunchTimer t("to_pictures", s);
+    to_pictures_kernel<<<blocks, kPicThreads, 0, s>>>(b);
+    return after_launch();
 }
 
 const void *kernel_entry_unpack() { return (const void *)unpack_kernel; }

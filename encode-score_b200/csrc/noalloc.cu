@@ -154,7 +154,8 @@ extern "C" int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int
             j.w = c.sw[k];
             j.h = c.sh[k];
             j.pad = p.pad;
-            j.tiles_x = (j.w + kCvTX - 1) / kCvTX;
+            j.tile_cols = cv_default_tile_cols(k);
+            j.tiles_x = (j.w + j.tile_cols - 1) / j.tile_cols;
             j.first_tile = tiles;
             j.slot = k;
             j.plane = nullptr;

@@ -103,8 +103,7 @@ __global__ void __launch_bounds__(256) feature_map_kernel(const __grid_constant_
         }
     }
     __syncthreads();
-    int j = 0;
-    while (j + 1 < b.njobs && (int)blockIdx.x >= b.job[j + 1].first_block) j++;
+    const int j = find_job(b.njobs, (int)blockIdx.x, [&](int k) { return b.job[k].first_block; });
     const PredJob &J = b.job[j];
     const int fw = (J.w + 3) / 4, fh = (J.h + 3) / 4;
     const int i = (blockIdx.x - J.first_block) * 256 + threadIdx.x;
@@ -434,8 +433,7 @@ __global__ void __launch_bounds__(kPT, 5) predict_kernel(const __grid_constant__
             if (tid == 0) b.pred[gt] = -INFINITY;
             continue;
         }
-        int j = 0;
-        while (j + 1 < b.njobs && gt >= b.job[j + 1].first_tile) j++;
+        const int j = find_job(b.njobs, gt, [&](int k) { return b.job[k].first_tile; });
         const PredJob &J = b.job[j];
         const int tile = gt - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
         // the 24 x 24 feature window: map pixels 16 tx - 4 .. 16 tx + 19 (a tile is 16 map pixels; 0 outside the map)
@@ -480,8 +478,7 @@ __global__ void __launch_bounds__(256) propose_kernel(const __grid_constant__ Pr
 {
     const unsigned long long frame = *b.frame;
     for (int gt = blockIdx.x * 256 + threadIdx.x; gt < b.total_tiles; gt += gridDim.x * 256) {
-        int j = 0;
-        while (j + 1 < b.njobs && gt >= b.job[j + 1].first_tile) j++;
+        const int j = find_job(b.njobs, gt, [&](int k) { return b.job[k].first_tile; });
         const ProposeJob &J = b.job[j];
         const int tile = gt - J.first_tile, tx = tile % J.tiles_x, ty = tile / J.tiles_x;
         uint8_t kind = kTileRun;

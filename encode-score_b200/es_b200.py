@@ -32,7 +32,7 @@ SYMBOLS = (
     "es_histogram_add", "es_histogram_quantile", "es_accum_init", "es_accum_merge", "es_accum_score", "es_accum_json",
     "es_psnr", "es_frame_create", "es_frame_queue", "es_frame_collect", "es_frame_read_windows", "es_frame_destroy",
     "es_batch_create", "es_batch_queue", "es_batch_collect", "es_batch_read_windows", "es_batch_scale_pooled",
-    "es_batch_set_cvalue_planes",
+    "es_batch_set_cvalue_planes", "es_batch_luma", "es_frame_luma", "es_to_pictures",
     "es_windows_create", "es_windows_compute", "es_windows_figures", "es_windows_destroy",
     "es_per_frame_json", "es_cambi_cache_open", "es_cambi_cache_find", "es_cambi_cache_add", "es_cambi_cache_file",
     "es_cambi_cache_close",
@@ -95,7 +95,18 @@ _lib = None
 
 class BatchSource(ctypes.Structure):
     _fields_ = [("w", ctypes.c_int), ("h", ctypes.c_int), ("pd", ctypes.c_int), ("n_encodes", ctypes.c_int),
-                ("cv_tile_rows", ctypes.c_int * 5)]
+                ("cv_tile_rows", ctypes.c_int * 5), ("cv_tile_cols", ctypes.c_int * 5)]
+
+
+class PictureCopy(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_uint64), ("dst", ctypes.c_uint64), ("w", ctypes.c_int), ("h", ctypes.c_int),
+                ("pitch", ctypes.c_int), ("bytes", ctypes.c_int)]
+
+
+def to_pictures(copies: list, stream: int = 0) -> None:
+    """es_to_pictures: copies [(src, dst, w, h, pitch, bytes), ...] planes into pictures, one launch."""
+    arr = (PictureCopy * len(copies))(*[PictureCopy(*c) for c in copies])
+    check(lib().es_to_pictures(arr, len(copies), ctypes.c_void_p(stream)))
 
 
 class ProposalOptions(ctypes.Structure):
@@ -184,6 +195,9 @@ def lib() -> ctypes.CDLL:
         L.es_batch_read_windows.argtypes = [P, I, I, P, P]
         L.es_batch_scale_pooled.argtypes = [P, I, ctypes.POINTER(ctypes.c_double)]
         L.es_batch_set_cvalue_planes.argtypes = [P, I, ctypes.POINTER(P)]
+        L.es_batch_luma.argtypes = [P, I, ctypes.c_long, ctypes.POINTER(U64)]
+        L.es_frame_luma.argtypes = [P, I, ctypes.c_long, ctypes.POINTER(U64)]
+        L.es_to_pictures.argtypes = [ctypes.POINTER(PictureCopy), I, P]
         L.es_batch_graph_launches.argtypes = [P]
         L.es_batch_graph_launches.restype = U64
         L.es_batch_destroy.argtypes = [P]
@@ -471,6 +485,12 @@ class Frame:
         check(lib().es_frame_collect(self.handle, f, cached, fa, ca, out))
         return list(out)
 
+    def luma(self, p: int, f: int) -> int:
+        """Device address of picture p's unpacked luma of frame f (0: the source, 1 + e: encode e)."""
+        out = ctypes.c_uint64()
+        check(lib().es_frame_luma(self.handle, p, f, ctypes.byref(out)))
+        return out.value
+
     def read_windows(self, encode: int, persist: bool = False):
         import numpy as np
         windows = (self.w // 16) * (self.h // 16)
@@ -502,7 +522,8 @@ AUTOTUNE_PATH = os.path.join(HERE, "autotune.json")
 
 
 def autotune_table(path: str = AUTOTUNE_PATH) -> dict:
-    """{(w, h): c-value tile rows per scale} from the autotuner's table (empty when there is none)."""
+    """{(w, h): {"rows": c-value tile rows per scale, "cols": tile columns per scale}} from the autotuner's table
+    (empty when there is none; columns 0 where the table has none, the library's default)."""
     import json
     try:
         with open(path) as f:
@@ -512,15 +533,25 @@ def autotune_table(path: str = AUTOTUNE_PATH) -> dict:
     out = {}
     for key, entry in t.get("classes", {}).items():
         w, h = (int(v) for v in key.split("x"))
-        out[(w, h)] = list(entry["cv_tile_rows"])
+        out[(w, h)] = {"rows": list(entry["cv_tile_rows"]), "cols": list(entry.get("cv_tile_cols", [0] * 5))}
     return out
+
+
+def _tile_shape(entry) -> tuple:
+    """(rows, cols) per scale from a tuning entry: a list of rows, or a dict with "rows" and optionally "cols"."""
+    if entry is None:
+        return [64] * 5, [0] * 5
+    if isinstance(entry, dict):
+        return list(entry.get("rows", [64] * 5)), list(entry.get("cols", [0] * 5))
+    return list(entry), [0] * 5
 
 
 class Batch:
     """Batched frame steps of several sources (es_batch_*): one launch per stage for all pictures, CUDA graphs from
     frame 14 on. ``sources`` is a list of (w, h, pd, n_encodes); pictures and encodes are numbered source by source.
-    ``tuning``: None for the autotuned c-value tile rows of autotune.json (by picture size; 64 where absent), False
-    for 64 everywhere, or a dict {(w, h): [rows per scale]}."""
+    ``tuning``: None for the autotuned c-value tile shapes of autotune.json (by picture size; the library's defaults
+    where absent), False for the defaults everywhere, or a dict {(w, h): rows per scale, or {"rows": [...], "cols":
+    [...]}} (cols 0: the library's default width)."""
 
     def __init__(self, module: Module, sources: list, use_graphs: bool = True, tuning=None):
         self.handle = ctypes.c_void_p()
@@ -528,9 +559,11 @@ class Batch:
         self.n_pictures = sum(1 + s[3] for s in self.sources)
         self.n_encodes = sum(s[3] for s in self.sources)
         table = autotune_table() if tuning is None else (tuning or {})
-        self.tile_rows = [list(table.get((s[0], s[1]), [64] * 5)) for s in self.sources]
-        arr = (BatchSource * len(self.sources))(*[BatchSource(*s, (ctypes.c_int * 5)(*r))
-                                                  for s, r in zip(self.sources, self.tile_rows)])
+        shapes = [_tile_shape(table.get((s[0], s[1]))) for s in self.sources]
+        self.tile_rows = [r for r, _ in shapes]
+        self.tile_cols = [c for _, c in shapes]
+        arr = (BatchSource * len(self.sources))(*[BatchSource(*s, (ctypes.c_int * 5)(*r), (ctypes.c_int * 5)(*c))
+                                                  for s, (r, c) in zip(self.sources, shapes)])
         opt = BatchOptions(int(use_graphs))
         check(lib().es_batch_create(module.handle, len(self.sources), arr, ctypes.byref(opt), ctypes.byref(self.handle)))
 
@@ -558,6 +591,11 @@ class Batch:
         ps = np.zeros((windows, 5), np.float32) if persist else None
         check(lib().es_batch_read_windows(self.handle, source, encode, st.ctypes.data, ps.ctypes.data if persist else None))
         return st, ps
+
+    def luma(self, picture: int, f: int) -> int:
+        out = ctypes.c_uint64()
+        check(lib().es_batch_luma(self.handle, picture, f, ctypes.byref(out)))
+        return out.value
 
     def scale_pooled(self, picture: int) -> list:
         out = (ctypes.c_double * SCALES)()

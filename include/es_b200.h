@@ -233,6 +233,26 @@ int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es
  * src/kernels.cu:434); either pointer may be NULL. */
 int es_frame_read_windows(es_frame *fr, int encode, float *stats, float *persist);
 void es_frame_destroy(es_frame *fr);
+/* The device address of picture p's unpacked luma plane of frame f (p = 0: the source, 1 + e: encode e; w x h 16-bit
+ * values at the pipeline depth, rows of w), as es_frame_queue left it: valid from that queue call until frame f + 14
+ * (the source) or f + 7 (an encode) is queued. It is the plane src/main.cpp:506-512 hands to libvmaf (see
+ * es_to_pictures). */
+int es_frame_luma(const es_frame *fr, int p, long f, uint64_t *address);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * The VMAF picture feed: to_picture (src/kernels.cu:537-545) as src/main.cpp:506-512 uses it, copying each unpacked
+ * luma plane into libvmaf's preallocated CUDA picture (data[0], stride[0]). libvmaf itself is not part of this
+ * library; a caller that links it passes the picture's device address and row pitch.
+ * --------------------------------------------------------------------------------------------------------------- */
+typedef struct {
+    uint64_t src;   /* device plane: w x h 16-bit values, rows of w */
+    uint64_t dst;   /* device picture: rows of `pitch` bytes */
+    int w, h;
+    int pitch;      /* bytes per picture row, at least w * bytes */
+    int bytes;      /* 1 (an 8-bit pipeline: the low byte of each value, as the reference) or 2 */
+} es_picture_copy;
+/* Copies n planes (1 to 64) in one launch queued on `stream`. */
+int es_to_pictures(const es_picture_copy *copies, int n, void *stream);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Texture window energies on larger windows, in three arithmetics (the precision study; no counterpart in the
@@ -279,8 +299,8 @@ void es_proposal_net_destroy(es_proposal_net *net);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Batched frame steps: no counterpart in the reference, which scores one source per process with one launch per
- * kernel and picture (src/main.cpp:518-643). A batch holds up to 16 sources, each with its own encodes, picture size
- * and pipeline depth (at most 32 pictures in all), and scores a frame step of all of them with one launch per stage;
+ * kernel and picture (src/main.cpp:518-643). A batch holds up to 32 sources, each with its own encodes, picture size
+ * and pipeline depth (at most 64 pictures in all), and scores a frame step of all of them with one launch per stage;
  * CAMBI runs beside the texture figures, and from frame 14 on a step is replayed from a CUDA graph per ring phase.
  * queue / collect keep es_frame_queue / es_frame_collect's contract (double-buffered by f % 2, frames in order).
  * --------------------------------------------------------------------------------------------------------------- */
@@ -291,6 +311,8 @@ typedef struct {
     int n_encodes; /* 1 to 16 */
     int cv_tile_rows[5]; /* rows of the c-value tiles per scale: 64, 32 or 16 (0 = 64); an autotuner's choice. With
                           * the learned proposal on, scales 0 and 1 use 64. */
+    int cv_tile_cols[5]; /* columns of the c-value tiles per scale: 64 or 128 (0 = 128 at scales 0 and 1, 64 below);
+                          * an autotuner's choice. With the learned proposal on, every scale uses 64. */
 } es_batch_source;
 typedef struct {
     int use_graphs; /* replay steps from CUDA graphs once the rings are full (frame 14 on) */
@@ -310,6 +332,8 @@ int es_batch_collect(es_batch *b, long f, const double *cached_source_cambi, es_
                      es_accum *const *centre_acc, es_frame_result *out);
 /* Introspection for tests: as es_frame_read_windows for encode `encode` of source `source`. */
 int es_batch_read_windows(es_batch *b, int source, int encode, float *stats, float *persist);
+/* As es_frame_luma for picture `picture` of the batch (numbered source by source: the source, then its encodes). */
+int es_batch_luma(const es_batch *b, int picture, long f, uint64_t *address);
 /* Introspection for tests: the pooled value of each scale of picture `picture` in the last collected step. */
 int es_batch_scale_pooled(es_batch *b, int picture, double pooled[5]);
 /* Introspection for tests: as es_cambi_set_cvalue_planes for picture `picture` of later steps (dev_planes NULL

@@ -7,7 +7,8 @@
 //    scale's picture, mask and c-values for bit-exact comparison;
 //  * frame_planes, window_stats, persist_stats, plane_sse and color_sums with the launch shapes of
 //    src/main.cpp:502-566;
-//  * tiny_luma with the launch shape of src/main.cpp:321.
+//  * tiny_luma with the launch shape of src/main.cpp:321;
+//  * to_picture with the launch shape of src/main.cpp:511.
 // The four libvmaf luminance functions src/cambi.cpp declares (lines 7-15) are supplied here from the same published
 // model the product uses (BT.1886, 10-bit limited range, 300 / 0.01 cd/m2), so both sides share one parameter set.
 #include <cuda.h>
@@ -312,6 +313,18 @@ int ref_tiny_luma(void *kp, const void *view, int x0, int y0, int w, int h, uint
         void *a[] = {&f, &x0, &y0, &w, &h, &o};
         cu_check(cuLaunchKernel(k.get("tiny_luma"), 64, 36, 1, 32, 8, 1, 0, nullptr, a, nullptr), "tiny_luma");
         cu_check(cuCtxSynchronize(), "tiny_luma");
+    });
+}
+
+// to_picture with the launch shape of src/main.cpp:511 (Kernels::launch over w x h): one plane into one picture.
+int ref_to_picture(void *kp, uint64_t src, int w, int h, uint64_t dst, int pitch, int bytes)
+{
+    return guarded([&] {
+        const Kernels &k = *(Kernels *)kp;
+        CUdeviceptr s = src, d = dst;
+        void *a[] = {&s, &w, &h, &d, &pitch, &bytes};
+        Kernels::launch(k.get("to_picture"), w, h, a, nullptr);
+        cu_check(cuCtxSynchronize(), "to_picture");
     });
 }
 

@@ -31,6 +31,7 @@ class RefGpu:
         lib.ref_plane_sse.argtypes = [P, U64, U64, U64, U64]
         lib.ref_color_sums.argtypes = [P, U64, U64, U64, I, U64]
         lib.ref_tiny_luma.argtypes = [P, P, I, I, I, I, U64]
+        lib.ref_to_picture.argtypes = [P, U64, I, I, U64, I, I]
         self._check(lib.ref_init())
         self.k = lib.ref_kernels()
         if not self.k:
@@ -77,6 +78,10 @@ class RefGpu:
     def tiny_luma(self, view, x0: int, y0: int, w: int, h: int, out: int) -> None:
         """The reference's thumbnail of one frame (view: an es_frame_view-layout structure) into 2304 device floats."""
         self._check(self.lib.ref_tiny_luma(self.k, ctypes.byref(view), x0, y0, w, h, out))
+
+    def to_picture(self, src: int, w: int, h: int, dst: int, pitch: int, bytes_: int) -> None:
+        """The reference's VMAF picture feed of one plane."""
+        self._check(self.lib.ref_to_picture(self.k, src, w, h, dst, pitch, bytes_))
 
 
 _ref = None

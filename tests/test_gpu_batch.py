@@ -127,6 +127,17 @@ def test_short_cvalue_tiles_equal_the_plain_step(cuda, module, steps):
     compare(plain, pacc, batch, bacc)
 
 
+@pytest.mark.parametrize("cols", [[64] * 5, [128] * 5, [64, 128, 64, 128, 128]])
+def test_cvalue_tile_widths_equal_the_plain_step(cuda, module, steps, cols):
+    """c-value tiles 64 or 128 columns wide, at any scale and with any rows, give the same results as the plain step
+    (whose CAMBI uses the library's default widths)."""
+    plain, pacc = run_plain(cuda, module, steps)
+    rows = ([64, 32, 16, 64, 32], [32, 64, 64, 16, 16], [16, 16, 32, 64, 64])
+    tuning = {(w, h): {"rows": r, "cols": cols} for (w, h, _, _), r in zip(SOURCES, rows)}
+    batch, bacc, _ = run_batch(cuda, module, steps, tuning=tuning)
+    compare(plain, pacc, batch, bacc)
+
+
 def test_batch_skipped_source_cambi_uses_the_cached_value(cuda, module, steps):
     rng = np.random.default_rng(5)
     flags = [[bool(rng.integers(0, 2)) for _ in SOURCES] for _ in range(FRAMES)]

@@ -133,7 +133,8 @@ def test_c2_4k10_three_encodes_batched_equals_the_oracle(cuda, module, c2_steps)
     with _pool() as pool:
         orc = OracleSequence(c2_steps, 10, pool)
     b = es_b200.Batch(module, [(w, h, 10, n_enc)])
-    assert b.tile_rows[0] == es_b200.autotune_table().get((w, h), [64] * 5), "the autotuned tile rows of 4K are in use"
+    tuned = es_b200.autotune_table().get((w, h), {"rows": [64] * 5, "cols": [0] * 5})
+    assert b.tile_rows[0] == tuned["rows"] and b.tile_cols[0] == tuned["cols"], "the autotuned tile shapes of 4K are in use"
     planes = [[torch.zeros(shape, dtype=torch.float32, device="cuda") for shape in _scale_shapes(w, h)] for _ in range(1 + n_enc)]
     for p in range(1 + n_enc):
         b.set_cvalue_planes(p, [t.data_ptr() for t in planes[p]])
