@@ -478,6 +478,9 @@ def main() -> None:
     ap.add_argument("--only-head", action="store_true", help="time only the headline form (for profiling runs)")
     ap.add_argument("--no-graphs", action="store_true", help="batched forms launch every kernel (for profiling runs)")
     ap.add_argument("--no-c3", action="store_true", help="skip the 16-pair uneven batch figures")
+    ap.add_argument("--profile", type=int, default=0, metavar="N",
+                    help="profiling run: N untimed frame steps of the headline form, every kernel its own launch, then exit")
+    ap.add_argument("--form", choices=["plain", "batched", "learned"], default=None, help="the form --profile runs")
     ap.add_argument("--budget", type=float, default=None, help="learned form: score budget of skipped tiles (default: the network's)")
     ap.add_argument("--tolerance", type=float, default=None, help="learned form: audit tolerance (default: the network's)")
     args = ap.parse_args()
@@ -614,6 +617,25 @@ def main() -> None:
             launches = es_b200.launch_count() - launches0
             clk = clocks.stop()
         return max_over_ranks(start.elapsed_time(end)), launches, clk, f
+
+    if args.profile:
+        # a short run for a profiler: no timing, no graphs (each kernel is its own launch), two distinct steps
+        args.no_graphs = True
+        have = os.path.exists(os.path.join(ROOT, "encode-score_b200", "proposal_net.npy"))
+        which = args.form or ("learned" if have else "batched")
+        form = {"plain": PlainForm, "batched": BatchedForm, "learned": LearnedForm}[which]()
+        acc = [es_b200.new_accum() for _ in range(n_enc)]
+        with torch.cuda.stream(stream):
+            res = []
+            for f in range(args.profile):
+                p = dev_pool[f % len(dev_pool)]
+                form.queue(f, [x[1] for x in p], stream.cuda_stream)
+                res = form.collect(f, acc) or res
+        torch.cuda.synchronize()
+        form.close()
+        module.close()
+        print(f"profile run: {args.profile} frame steps of the {which} form", flush=True)
+        return
 
     pairs = args.steps * n_enc * world
     forms = {}

@@ -378,6 +378,9 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
         j.depth = pic.depth;
         j.mask_index = pic.p.mask_index;
         j.word = pic.words[0].ptr;
+        j.word1 = pic.words[1].ptr;
+        j.w1 = pic.sw[1];
+        j.h1 = pic.sh[1];
         if (b.net) {
             j.feat = b.feat.ptr + b.feat_at[i];
             j.need = b.need.ptr + pred_tiles;
@@ -385,7 +388,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
         }
     }
     pb.band = band;
-    cuda_check(launch_prep0(pb, s), "batch scale 0");
+    cuda_check(launch_prep0(pb, s), "batch scales 0 and 1");
     CvBatch cb{};
     int tiles = 0;
     for (int i : run) {
@@ -424,7 +427,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
     }
     const int nslots = (int)b.pictures.size() * kScales;
     cuda_check(launch_slots_reset(b.slots.ptr, nslots, b.slot_n.ptr, b.slot_k.ptr, s), "batch reset");
-    for (int sc = 1; sc < kScales; sc++) {
+    for (int sc = 2; sc < kScales; sc++) {
         DecBatch db{};
         int blocks = 0;
         for (int i : run) {

@@ -89,15 +89,15 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
     pj.depth = c->depth;
     pj.mask_index = p.mask_index;
     pj.word = c->words[0].ptr;
-    pj.tiles_x = (c->w + 63) / 64;
-    pj.first_tile = 0;
-    pb.total_tiles = pj.tiles_x * ((c->h + 31) / 32);
-    cuda_check(launch_prep0(pb, caller), "cambi scale 0");
+    pj.word1 = c->words[1].ptr;
+    pj.w1 = c->sw[1];
+    pj.h1 = c->sh[1];
+    cuda_check(launch_prep0(pb, caller), "cambi scales 0 and 1");
     cuda_check(cudaEventRecord(c->copied.e, caller), "cambi event");
     cudaStream_t s = serial_streams() ? caller : c->stream.s;
     cuda_check(cudaStreamWaitEvent(s, c->copied.e, 0), "cambi event");
     cuda_check(launch_slots_reset(c->slots.ptr, kScales, c->slot_n.ptr, c->slot_k.ptr, s), "cambi reset");
-    for (int sc = 1; sc < kScales; sc++) {
+    for (int sc = 2; sc < kScales; sc++) {
         DecBatch db{};
         db.njobs = 1;
         DecJob &dj = db.job[0];

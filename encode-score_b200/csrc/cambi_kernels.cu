@@ -27,29 +27,46 @@ __device__ __forceinline__ uint16_t mode3(uint16_t a, uint16_t b, uint16_t c)
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Scale 0: src/kernels.cu:524-535 (from8), 14-40 (mask), 488-500 (mode), in one pass over a 64 x 64 tile.
-// The plane is staged with its margins (8-byte loads for tiles inside the picture); an 8-bit plane is turned into
-// 10-bit anti-dithered values, a 10-bit one is used as staged. A warp per row packs the flat pixels into bit words by
-// ballot; each thread then walks 16 rows of one column, counting the 7 flat bits around each pixel with a funnel shift
-// and a popcount, summing 7 rows as it goes, and applying the separable mode filter from running row modes.
-// Staged region: columns x0-4 .. x0+71 (index x - (x0-4)), rows y0-3 .. y0+68 (index y - (y0-3)).
+// Scales 0 and 1: src/kernels.cu:524-535 (from8), 14-40 (mask), 488-500 (mode), 43-53 (decimation), in one pass over a
+// 64 x 64 tile of scale 0 and the 32 x 32 tile of scale 1 beneath it.
+//
+// The plane is staged with its margins (16-byte loads for tiles inside the picture; an 8-bit plane becomes 10-bit
+// anti-dithered values in a second buffer). A warp per staged row packs the flat pixels into bit words by ballot. Each
+// warp then walks 8 rows of the tile, a lane taking two neighbouring columns as the two halves of 32-bit words: the 7
+// flat bits around each column come from one funnel shift and two popcounts and are summed over 7 rows as they go, and
+// the 3 x 3 mode filter runs on both columns at once with 16-bit SIMD compares and minima. The scale-0 words at even
+// positions, with a ring of them one step outside the tile (made on their own), then give the tile's scale-1 words
+// (decimation and mode filter of the decimated values) without another read of scale 0.
+// Staged region: columns x0-8 .. x0+71 (index x - (x0-8)), rows y0-5 .. y0+69 (index y - (y0-5)).
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int kP0T = 64;                    // output tile side
-constexpr int kP0C = kP0T + 12, kP0R = kP0T + 8;  // staged columns (76) and rows (72)
-constexpr int kP0F = kP0T + 6;              // flat pixels per side: x0-3 .. x0+66, y0-3 .. y0+66
+constexpr int kP0T = 64;                 // scale-0 tile side
+constexpr int kP0C = 80, kP0R = 75;      // staged columns and rows
+constexpr int kP0X = 8, kP0Y = 5;        // staged index of x0, y0
+constexpr int kP0FR = 73, kP0FX = 5;     // flat rows y0-5 .. y0+67; bit i of a row is column x0-5+i
+constexpr int kP0D = 34;                 // scale-0 words (x0-2+2X, y0-2+2Y), X, Y in 0 .. 33
 
-__global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ Prep0Batch b)
+// The mode of three values per 16-bit half (the smallest when all three differ), values below 2^15.
+__device__ __forceinline__ uint32_t mode3x2(uint32_t a, uint32_t b, uint32_t c)
 {
-    __shared__ __align__(16) uint16_t raw[kP0R][kP0C];
-    __shared__ __align__(16) uint16_t pre8[kP0R - 1][kP0C];
-    __shared__ uint32_t flatbits[kP0F][3];
+    const uint32_t eab = __vcmpeq2(a, b), eac = __vcmpeq2(a, c), ebc = __vcmpeq2(b, c);
+    const uint32_t mn = __vminu2(a, __vminu2(b, c));
+    const uint32_t bc = (b & ebc) | (mn & ~ebc);
+    const uint32_t e = eab | eac;
+    return (a & e) | (bc & ~e);
+}
+
+__global__ void __launch_bounds__(256, 4) prep0_kernel(const __grid_constant__ Prep0Batch b)
+{
+    __shared__ __align__(16) uint16_t buf[2][kP0R][kP0C];  // [0]: the staged plane; [1]: 8-bit planes at 10 bits
+    __shared__ uint32_t flatbits[kP0FR][4];                // 3 words of bits and a zero word
+    __shared__ uint16_t dw[kP0D][kP0D];                    // scale-0 words at even positions, for scale 1
     __shared__ uint32_t needbits[32];
     const int j = find_job(b.njobs, (int)blockIdx.x, [&](int k) { return b.job[k].first_tile; });
     const Prep0Job &J = b.job[j];
     const int t = blockIdx.x - J.first_tile, w = J.w, h = J.h, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int x0 = (t % J.tiles_x) * kP0T, y0 = (t / J.tiles_x) * kP0T;
-    const int xs = x0 - 4, ys = y0 - 3;
+    const int xs = x0 - kP0X, ys = y0 - kP0Y;
     if (J.feat && b.need_span < 0) {  // the codes that need c-values when they are no single range: bit c of word
                                       // c / 32 (warp w makes words w, w + 8, ...)
 #pragma unroll
@@ -59,131 +76,206 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
             if (lane == 0) needbits[warp + 8 * k] = m;
         }
     }
-    const bool inside = xs >= 0 && xs + kP0C <= w && ys >= 0 && ys + kP0R <= h && (J.pitch & 3) == 0 && (((uintptr_t)J.img) & 7) == 0;
+    if (tid < kP0FR) flatbits[tid][3] = 0;
+    const bool inside = xs >= 0 && xs + kP0C <= w && ys >= 0 && ys + kP0R <= h && (J.pitch & 7) == 0 && (((uintptr_t)J.img) & 15) == 0;
     if (inside) {
-        for (int i = tid; i < kP0R * (kP0C / 4); i += 256) {
-            const int r = i / (kP0C / 4), q = i - r * (kP0C / 4);
-            *(uint2 *)&raw[r][4 * q] = __ldg((const uint2 *)(J.img + (size_t)(ys + r) * J.pitch + xs) + q);
+        for (int i = tid; i < kP0R * (kP0C / 8); i += 256) {
+            const int r = i / (kP0C / 8), q = i - r * (kP0C / 8);
+            *(uint4 *)&buf[0][r][8 * q] = __ldg((const uint4 *)(J.img + (size_t)(ys + r) * J.pitch + xs) + q);
         }
     } else {
         for (int i = tid; i < kP0R * kP0C; i += 256) {
             const int r = i / kP0C, c = i - r * kP0C, x = xs + c, y = ys + r;
-            raw[r][c] = (x >= 0 && x < w && y >= 0 && y < h) ? J.img[(size_t)y * J.pitch + x] : (uint16_t)0;
+            buf[0][r][c] = (x >= 0 && x < w && y >= 0 && y < h) ? J.img[(size_t)y * J.pitch + x] : (uint16_t)0;
         }
     }
     __syncthreads();
-    // preprocessed values of x0-4 .. x0+71, y0-3 .. y0+67: an 8-bit plane at 10 bits, the mean of the 2 x 2 block to
+    // preprocessed values of x0-5 .. x0+68, y0-5 .. y0+68: an 8-bit plane at 10 bits, the mean of the 2 x 2 block to
     // the lower right (pairs on the last row and column); a 10-bit plane as staged (0 outside the picture)
-    if (J.depth == 8) {
-        for (int i = tid; i < (kP0R - 1) * (kP0C - 1); i += 256) {
-            const int r = i / (kP0C - 1), c = i - r * (kP0C - 1), x = xs + c, y = ys + r;
+    const int sel = J.depth == 8 ? 1 : 0;
+    if (sel) {
+        for (int i = tid; i < 74 * 74; i += 256) {
+            const int r = i / 74, c = 3 + (i - r * 74), x = xs + c, y = ys + r;
             unsigned v = 0;
             if (x >= 0 && x < w && y >= 0 && y < h) {
-                const unsigned a = (unsigned)raw[r][c] << 2;
+                const unsigned a = (unsigned)buf[0][r][c] << 2;
                 if (x < w - 1 && y < h - 1)
-                    v = (a + ((unsigned)raw[r][c + 1] << 2) + ((unsigned)raw[r + 1][c] << 2) + ((unsigned)raw[r + 1][c + 1] << 2)) >> 2;
-                else if (y < h - 1) v = (a + ((unsigned)raw[r + 1][c] << 2)) >> 1;
-                else if (x < w - 1) v = (a + ((unsigned)raw[r][c + 1] << 2)) >> 1;
+                    v = (a + ((unsigned)buf[0][r][c + 1] << 2) + ((unsigned)buf[0][r + 1][c] << 2) + ((unsigned)buf[0][r + 1][c + 1] << 2)) >> 2;
+                else if (y < h - 1) v = (a + ((unsigned)buf[0][r + 1][c] << 2)) >> 1;
+                else if (x < w - 1) v = (a + ((unsigned)buf[0][r][c + 1] << 2)) >> 1;
                 else v = a;
             }
-            pre8[r][c] = (uint16_t)v;
-        }
-        __syncthreads();
-        // back into the staged plane, so every later read names one shared array (32-bit shared addressing)
-        for (int i = tid; i < (kP0R - 1) * (kP0C - 1); i += 256) {
-            const int r = i / (kP0C - 1), c = i - r * (kP0C - 1);
-            raw[r][c] = pre8[r][c];
+            buf[1][r][c] = (uint16_t)v;
         }
         __syncthreads();
     }
-    auto &pre = raw;
     // flat: equal to the right and lower neighbours (the last column / row count as equal); nothing outside
-    const bool interior = x0 >= 3 && x0 + kP0T + 3 < w && y0 >= 3 && y0 + kP0T + 3 < h;
-    for (int q = warp; q < kP0F; q += 8) {
-        const int y = ys + q;
-        uint32_t words[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const int c = lane + 32 * k, x = x0 - 3 + c;  // staged column c + 1
+    {
+        const bool interior = x0 >= 5 && x0 + kP0T + 4 < w && y0 >= 5 && y0 + kP0T + 4 < h;
+        for (int task = warp; task < kP0FR * 3; task += 8) {
+            const int q = task / 3, k = task - q * 3;
+            const int i = 32 * k + lane, c = i + (kP0X - kP0FX), x = x0 - kP0FX + i, y = ys + q;
             bool f = false;
-            if (c < kP0F) {
-                const uint16_t v = pre[q][c + 1];
-                if (interior) f = v == pre[q][c + 2] && v == pre[q + 1][c + 1];
+            if (i < kP0FR) {
+                const uint16_t v = buf[sel][q][c];
+                if (interior) f = v == buf[sel][q][c + 1] && v == buf[sel][q + 1][c];
                 else if (x >= 0 && x < w && y >= 0 && y < h)
-                    f = (x == w - 1 || v == pre[q][c + 2]) && (y == h - 1 || v == pre[q + 1][c + 1]);
+                    f = (x == w - 1 || v == buf[sel][q][c + 1]) && (y == h - 1 || v == buf[sel][q + 1][c]);
             }
-            words[k] = __ballot_sync(0xffffffffu, f);
+            const uint32_t word = __ballot_sync(0xffffffffu, f);
+            if (lane == 0) flatbits[q][k] = word;
         }
-        if (lane < 3) flatbits[q][lane] = lane == 0 ? words[0] : lane == 1 ? words[1] : words[2];
     }
     __syncthreads();
-    const int c = tid & (kP0T - 1), g = tid >> 6, x = x0 + c;
-    const bool feat = J.feat != nullptr;  // the same for the whole block
-    if (x >= w && !feat) return;
-    // flat count of the 7 columns around x in flat row 16 g + q (bit c of a row is column x - 3), and the horizontal
-    // mode of picture row y0 + 16 g - 1 + k (staged row 16 g + 2 + k), each made once as the window moves down and
-    // kept only while the window holds it, so few registers stay live and 5 blocks share an SM
-    const int kw = c >> 5, sh = c & 31;
-    auto h7 = [&](int q) { return __popc(__funnelshift_r(flatbits[16 * g + q][kw], flatbits[16 * g + q][kw + 1], sh) & 0x7Fu); };
-    const bool edge_x = x == 0 || x == w - 1;
-    auto hmode = [&](int k) -> uint16_t {
-        const uint16_t *row = pre[16 * g + 2 + k];
-        return edge_x ? row[c + 4] : mode3(row[c + 3], row[c + 4], row[c + 5]);
+
+    // the walk: warp g makes rows y0 + 8 g .. + 7, lane l columns x0 + 2 l and + 1
+    const int x = x0 + 2 * lane, g = warp;
+    const int kw = (2 * lane + 2) >> 5, sh = (2 * lane + 2) & 31;  // flat bit of column x - 3
+    auto h7 = [&](int q) -> uint32_t {  // flat counts of the 7 columns around x and x + 1 in flat row q, as halves
+        const uint32_t bits = __funnelshift_r(flatbits[q][kw], flatbits[q][kw + 1], sh);
+        return (uint32_t)__popc(bits & 0x7Fu) | ((uint32_t)__popc((bits >> 1) & 0x7Fu) << 16);
     };
-    int cnt = 0, hv[22];  // hv[q] = h7(q), each kept for the 7 rows of the window it enters
+    // columns x and x + 1 at a picture edge keep their own value in the horizontal mode
+    const uint32_t edge = ((x == 0 || x == w - 1) ? 0x0000FFFFu : 0u) | ((x + 1 == w - 1) ? 0xFFFF0000u : 0u);
+    const int c = x - xs;  // staged column of x (even)
+    auto pair = [&](int r, int cc) -> uint32_t { return *(const uint32_t *)&buf[sel][r][cc]; };
+    auto hmode = [&](int y) -> uint32_t {  // horizontal modes of x and x + 1 in picture row y
+        const int r = y - ys;
+        const uint32_t l2 = pair(r, c - 2), m2 = pair(r, c), r2 = pair(r, c + 2);
+        const uint32_t left = __byte_perm(l2, m2, 0x5432), right = __byte_perm(m2, r2, 0x5432);
+        return (m2 & edge) | (mode3x2(left, m2, right) & ~edge);
+    };
+    const bool feat = J.feat != nullptr;  // the same for the whole block
+    const uint32_t idx2 = (uint32_t)J.mask_index * 0x10001u;
+    const bool vec_store = (w & 1) == 0 && (((uintptr_t)J.word) & 3) == 0;
+    const bool need_range = b.need_span >= 0;
+    const uint32_t lo2 = (uint32_t)b.need_lo * 0x10001u, span2 = (uint32_t)(b.need_span < 0 ? 0 : b.need_span) * 0x10001u;
+    const int yb = y0 + 8 * g;
+    uint32_t hv[14];  // h7 of flat rows yb-3 .. yb+10 (flat row index y - (y0-5))
+    uint32_t cnt = 0;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
-        hv[q] = h7(q);
+        hv[q] = h7(yb - 3 - ys + q);
         cnt += hv[q];
     }
-    uint16_t m0 = hmode(0), m1 = hmode(1);
-    // features of the 4 x 4 blocks (the proposal's block_features): value sum, masked and counted pixels of this
-    // column's 4 rows, then summed over the block's 4 columns (lanes c .. c + 3 of one warp)
-    unsigned fpack = 0;  // value sum (bits 0-15, at most 16 x 1023), masked pixels (16-20), counted pixels (24-28)
+    uint32_t m0 = hmode(yb - 1), m1 = hmode(yb);
+    uint32_t fsum = 0, fmask = 0, fn = 0;  // features of this lane's two columns over the current 4 rows
     bool need = false;
-    const bool need_range = b.need_span >= 0;
-    const unsigned need_lo = (unsigned)b.need_lo, need_span = (unsigned)b.need_span;
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        hv[i + 6] = h7(i + 6);
+    for (int i = 0; i < 8; i++) {
+        const int y = yb + i;
+        hv[i + 6] = h7(y + 3 - ys);
         cnt += hv[i + 6];
-        const uint16_t m2 = hmode(i + 2);
-        const int y = y0 + 16 * g + i;
-        if (y < h && x < w) {
-            const uint16_t v = (y == 0 || y == h - 1) ? pre[16 * g + 3 + i][c + 4] : mode3(m0, m1, m2);
-            const uint16_t word = (uint16_t)(v | (cnt > J.mask_index ? kMaskBit : 0));
-            J.word[(size_t)y * w + x] = word;
+        const uint32_t m2 = hmode(y + 1);
+        uint32_t v2 = mode3x2(m0, m1, m2);
+        if (y == 0 || y == h - 1) v2 = pair(y - ys, c);
+        const uint32_t mk = __vcmpgtu2(cnt, idx2) & 0x80008000u;
+        const uint32_t word2 = v2 | mk;
+        if (y < h) {
+            if (vec_store && x + 1 < w) {
+                *(uint32_t *)(J.word + (size_t)y * w + x) = word2;
+            } else {
+                if (x < w) J.word[(size_t)y * w + x] = (uint16_t)word2;
+                if (x + 1 < w) J.word[(size_t)y * w + x + 1] = (uint16_t)(word2 >> 16);
+            }
+            if ((i & 1) == 0 && x < w) dw[4 * g + i / 2 + 1][lane + 1] = (uint16_t)word2;
             if (feat) {
-                fpack += (unsigned)v | ((unsigned)(word >> 15) << 16) | (1u << 24);
+                const uint32_t ok = (x + 1 < w) ? 0xFFFFFFFFu : (x < w ? 0x0000FFFFu : 0u);
+                const uint32_t vk = v2 & ok, mm = (mk >> 15) & ok & 0x10001u;
+                fsum += (vk & 0xFFFFu) + (vk >> 16);
+                fmask += (mm & 1u) + (mm >> 16);
+                fn += (ok & 1u) + (ok >> 31);
+                uint32_t hit;
                 if (need_range) {
-                    need |= (word >> 15) && (unsigned)v - need_lo <= need_span;
+                    hit = __vcmpleu2(__vsub2(v2, lo2), span2) & __vcmpne2(mk, 0u) & ok;
                 } else {
-                    const uint16_t code = code_of(word, b.band);
-                    need |= code != kNone && ((needbits[code >> 5] >> (code & 31)) & 1u);
+                    hit = 0;
+                    for (int k = 0; k < 2; k++) {
+                        const uint16_t code = code_of((uint16_t)(word2 >> (16 * k)), b.band);
+                        if (((ok >> (16 * k)) & 1u) && code != kNone && ((needbits[code >> 5] >> (code & 31)) & 1u)) hit = 1;
+                    }
                 }
+                need |= hit != 0;
             }
         }
         cnt -= hv[i];
         m0 = m1;
         m1 = m2;
         if (feat && (i & 3) == 3) {
-            fpack += __shfl_xor_sync(0xffffffffu, fpack, 1);
-            fpack += __shfl_xor_sync(0xffffffffu, fpack, 2);
-            const int fw = (w + 3) / 4, fh = (h + 3) / 4, u = x >> 2, v4 = (y0 + 16 * g + i - 3) >> 2;
-            if ((c & 3) == 0 && u < fw && v4 < fh) {
-                const unsigned fsum = fpack & 0xFFFFu, fmask = (fpack >> 16) & 0xFFu, fn = fpack >> 24;
+            // the 4 x 4 block of columns x - 2 l % 4 .. + 3: this lane's pair and its neighbour's
+            fsum += __shfl_xor_sync(0xffffffffu, fsum, 1);
+            fmask += __shfl_xor_sync(0xffffffffu, fmask, 1);
+            fn += __shfl_xor_sync(0xffffffffu, fn, 1);
+            const int fw = (w + 3) / 4, fh = (h + 3) / 4, u = x >> 2, v4 = (y - 3) >> 2;
+            if ((lane & 1) == 0 && u < fw && v4 < fh) {
                 // (sum / n - 512) / 256 rounded once to float; for a whole block (n = 16) every step is exact in
                 // float, so the double path is needed only at the picture's edges
                 const float f0 = fn == 16 ? __fmul_rn(__fsub_rn(__fmul_rn((float)fsum, 0.0625f), 512.0f), 0.00390625f)
                                           : fn ? (float)(((double)fsum / (double)fn - 512.0) / 256.0) : 0.0f;
                 J.feat[(size_t)v4 * fw + u] = make_float2(f0, __fmul_rn((float)fmask, 0.0625f));
             }
-            fpack = 0;
+            fsum = fmask = fn = 0;
         }
     }
     if (feat) {
         need = __syncthreads_or(need);
         if (tid == 0) J.need[t] = need ? 1u : 0u;
+    }
+    if (!J.word1) return;  // the same for the whole block
+
+    // the ring of scale-0 words one step outside the tile that scale 1 reads: rows y0-2 and y0+64 (X = 0 .. 33), then
+    // columns x0-2 and x0+64 (Y = 1 .. 32)
+    if (tid < 2 * kP0D + 2 * (kP0D - 2)) {
+        int X, Y;
+        if (tid < 2 * kP0D) {
+            X = tid % kP0D;
+            Y = tid < kP0D ? 0 : kP0D - 1;
+        } else {
+            Y = 1 + (tid - 2 * kP0D) % (kP0D - 2);
+            X = tid - 2 * kP0D < kP0D - 2 ? 0 : kP0D - 1;
+        }
+        const int px = x0 - 2 + 2 * X, py = y0 - 2 + 2 * Y;
+        if (px >= 0 && px < w && py >= 0 && py < h) {
+            const int bi = px - (x0 - kP0FX) - 3, bw = bi >> 5, bs = bi & 31;
+            int n = 0;
+#pragma unroll
+            for (int dy = -3; dy <= 3; dy++)
+                n += __popc(__funnelshift_r(flatbits[py + dy - ys][bw], flatbits[py + dy - ys][bw + 1], bs) & 0x7Fu);
+            const int pc = px - xs;
+            auto hm1 = [&](int yy) -> uint16_t {
+                const uint16_t *row = buf[sel][yy - ys];
+                return (px == 0 || px == w - 1) ? row[pc] : (uint16_t)(mode3x2(row[pc - 1], row[pc], row[pc + 1]) & 0xFFFFu);
+            };
+            const uint16_t v = (py == 0 || py == h - 1) ? buf[sel][py - ys][pc]
+                                                        : (uint16_t)(mode3x2(hm1(py - 1), hm1(py), hm1(py + 1)) & 0xFFFFu);
+            dw[Y][X] = (uint16_t)(v | (n > J.mask_index ? kMaskBit : 0));
+        }
+    }
+    __syncthreads();
+    // scale 1: the decimated words dw, mode-filtered (rows and columns at the picture's edges keep their value); thread
+    // (cx, q) makes column cx of rows 4 q .. 4 q + 3 of the 32 x 32 tile
+    {
+        const int w1 = J.w1, h1 = J.h1, X0 = x0 >> 1, Y0 = y0 >> 1;
+        const int cx = tid & 31, q = tid >> 5, X1 = X0 + cx;
+        if (X1 < w1) {
+            const int X = cx + 1;
+            const bool edge1 = X1 == 0 || X1 == w1 - 1;
+            auto val = [&](int Y, int XX) -> uint32_t { return dw[Y][XX] & 0x7FFFu; };
+            uint32_t hm[6];  // rows Y0 + 4 q - 1 .. + 4 (dw rows 4 q .. 4 q + 5)
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const int Y = 4 * q + k, Yp = Y0 + Y - 1;
+                hm[k] = (Yp < 0 || Yp >= h1) ? 0u : edge1 ? val(Y, X) : (mode3x2(val(Y, X - 1), val(Y, X), val(Y, X + 1)) & 0xFFFFu);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int Y1 = Y0 + 4 * q + i;
+                if (Y1 >= h1) break;
+                const uint16_t word = dw[4 * q + i + 1][X];
+                const uint32_t v = (Y1 == 0 || Y1 == h1 - 1) ? (uint32_t)(word & 0x7FFFu) : (mode3x2(hm[i], hm[i + 1], hm[i + 2]) & 0xFFFFu);
+                J.word1[(size_t)Y1 * w1 + X1] = (uint16_t)(v | (word & kMaskBit));
+            }
+        }
     }
 }
 

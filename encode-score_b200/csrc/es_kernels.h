@@ -69,7 +69,7 @@ struct Band {
     int weight[kDiffs];
 };
 
-// ---- scale 0: preprocessing, zero-derivative mask and mode filter of one plane -------------------------------------
+// ---- scales 0 and 1: preprocessing, zero-derivative mask and mode filter of one plane, then its first decimation --
 struct Prep0Job {
     const uint16_t *img;  // input plane, `pitch` pixels per row
     int pitch, w, h, depth, mask_index;
@@ -79,6 +79,9 @@ struct Prep0Job {
     // as the proposal's feature kernel makes it, and per 64 x 64 tile whether a pixel needs a c-value (0 or 1)
     float2 *feat;
     unsigned *need;
+    // optional: scale 1 (w1 x h1 = the halved size, rounded up) made in the same pass; nullptr: scale 0 only
+    uint16_t *word1;
+    int w1, h1;
 };
 constexpr int kPrep0MaxJobs = kMaxPictures;
 struct Prep0Batch {

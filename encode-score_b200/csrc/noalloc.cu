@@ -134,10 +134,19 @@ extern "C" int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int
 
         Prep0Batch pb{};
         pb.njobs = 1;
-        pb.job[0] = Prep0Job{(const uint16_t *)img, pitch, w, h, depth, p.mask_index, (uint16_t *)(base + c.words[0]), (w + 63) / 64, 0};
-        pb.total_tiles = pb.job[0].tiles_x * ((h + 31) / 32);
-        cuda_check(launch_prep0(pb, s), "cambi scale 0");
-        for (int k = 1; k < kScales; k++) {
+        Prep0Job &pj = pb.job[0];
+        pj.img = (const uint16_t *)img;
+        pj.pitch = pitch;
+        pj.w = w;
+        pj.h = h;
+        pj.depth = depth;
+        pj.mask_index = p.mask_index;
+        pj.word = (uint16_t *)(base + c.words[0]);
+        pj.word1 = (uint16_t *)(base + c.words[1]);
+        pj.w1 = c.sw[1];
+        pj.h1 = c.sh[1];
+        cuda_check(launch_prep0(pb, s), "cambi scales 0 and 1");
+        for (int k = 2; k < kScales; k++) {
             DecBatch db{};
             db.njobs = 1;
             db.job[0] = DecJob{(const uint16_t *)(base + c.words[k - 1]), c.sw[k - 1], c.sh[k - 1], (uint16_t *)(base + c.words[k]),
