@@ -451,10 +451,7 @@ void record_cambi(es_batch &b, long f, uint32_t skip, cudaStream_t s)
         if (split) cuda_check(cudaStreamWaitEvent(s, b.join_aux.e, 0), "event");
         record_proposal_cvalues(b, cb, ab, s);
     }
-    static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
-    for (int round = 0; round < 3; round++)
-        cuda_check(launch_select_round(b.slots.ptr, nslots, shifts[round], widths[round], s), "batch top-k");
-    cuda_check(launch_sum_above(b.slots.ptr, nslots, s), "batch top-k");
+    cuda_check(launch_topk(b.slots.ptr, nslots, s), "batch top-k");
     ScoreBatch sb{};
     for (int i : run) {
         ScoreJob &j = sb.job[sb.njobs++];

@@ -144,11 +144,7 @@ void queue_cambi(es_cambi *c, uint64_t img, int pitch, cudaStream_t caller)
         static_assert(sizeof(CvSlot) % 8 == 0, "slot layout");
     }
     cuda_check(launch_cvalues(cb, s), "cambi c-values");
-    for (int round = 0; round < 3; round++) {
-        static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
-        cuda_check(launch_select_round(c->slots.ptr, kScales, shifts[round], widths[round], s), "cambi top-k");
-    }
-    cuda_check(launch_sum_above(c->slots.ptr, kScales, s), "cambi top-k");
+    cuda_check(launch_topk(c->slots.ptr, kScales, s), "cambi top-k");
     ScoreBatch sb{};
     sb.njobs = 1;
     sb.job[0].first_slot = 0;

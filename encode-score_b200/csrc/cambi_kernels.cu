@@ -9,8 +9,9 @@
 //    reads one 16-bit word per pixel;
 //  * decimate_mode_kernel builds scales 1-4 the same way from the previous scale's words;
 //  * the c-values themselves are in cvalues_kernels.cu;
-//  * select_round_kernel / select_pick_kernel / sum_above_kernel find the exact k-th largest value on the device when
-//    more than k values are positive (no host round trips), and score_kernel pools and weights the scales.
+//  * select_hist_kernel / select_pick_kernel find the exact k-th largest value, and the sum above it, on the device
+//    when more than k values are positive (no host round trips; the first radix digit is counted by the c-value
+//    kernel), and score_kernel pools and weights the scales.
 #include "cambi_codes.h"
 #include "es_kernels.h"
 
@@ -336,6 +337,7 @@ __global__ void slots_reset_kernel(CvSlot *slots, int nslots, const unsigned lon
     if (s >= nslots) return;
     CvSlot &S = slots[s];
     for (int i = threadIdx.x; i < 2048; i += blockDim.x) S.hist[i] = 0;
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) S.dsum[i] = 0;
     if (threadIdx.x == 0) {
         S.sum_fx = S.count = S.list_n = 0;
         S.n = n[s];
@@ -346,35 +348,55 @@ __global__ void slots_reset_kernel(CvSlot *slots, int nslots, const unsigned lon
     }
 }
 
-// One radix round over every slot whose positive count exceeds k; block b takes the b-th share of each such slot's list.
-// One block of kSelThreads per SM: each block merges one shared histogram per slot into the slot's, so fewer, larger
-// blocks mean fewer global atomics for the same reads.
+// A positive c-value in units of 2^-24 (exact: c-values are multiples of 2^-24).
+__device__ __forceinline__ unsigned long long fx_of(unsigned bits) { return __float2ull_rn(__fmul_rn(__uint_as_float(bits), 16777216.0f)); }
+
+// One radix round over every slot whose positive count exceeds k (the first round's counts come from the c-value
+// kernel); block b takes the b-th share of each such slot's list. One block of kSelThreads per SM: each block merges
+// one shared histogram per slot into the slot's, so fewer, larger blocks mean fewer global atomics for the same reads.
+// The last round (last = 1) also sums, per digit, the values that match the prefix (they are equal when their digits
+// are), and the values whose prefix is greater than the selected one (all of them lie above the k-th value).
 constexpr int kSelThreads = 1024, kSelBlocks = 148;
 
-__global__ void __launch_bounds__(kSelThreads) select_hist_kernel(CvSlot *slots, int nslots, int shift, int width)
+__global__ void __launch_bounds__(kSelThreads) select_hist_kernel(CvSlot *slots, int nslots, int shift, int width, int last)
 {
     __shared__ unsigned hist[2048];
+    __shared__ unsigned long long dsum[1024];
     const int nb = 1 << width;
     for (int sl = 0; sl < nslots; sl++) {
         CvSlot &S = slots[sl];
         if (S.count <= S.k) continue;  // the same for the whole block
-        for (int i = threadIdx.x; i < nb; i += kSelThreads) hist[i] = 0;
+        for (int i = threadIdx.x; i < nb; i += kSelThreads) {
+            hist[i] = 0;
+            if (last) dsum[i] = 0;
+        }
         __syncthreads();
         const unsigned *v = (const unsigned *)S.list;
         const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * kSelThreads;
         const unsigned mask = S.mask, prefix = S.prefix;
+        unsigned long long above_fx = 0, above_n = 0;
         // neighbouring c-values of the list are often equal (they come from the same tile), so each thread adds runs
         // of equal digits at once; 4 values per 16-byte load
-        unsigned last = 0, run = 0;
+        unsigned lastd = 0, run = 0;
+        auto flush_run = [&]() {
+            atomicAdd(&hist[lastd], run);
+            if (last) atomicAdd(&dsum[lastd], (unsigned long long)run * fx_of(prefix | lastd));
+        };
         auto add = [&](unsigned bits) {
-            if ((bits & mask) != prefix) return;
+            if ((bits & mask) != prefix) {
+                if (last && (bits & mask) > prefix) {
+                    above_fx += fx_of(bits);
+                    above_n++;
+                }
+                return;
+            }
             const unsigned d = (bits >> shift) & (unsigned)(nb - 1);
-            if (run && d == last) {
+            if (run && d == lastd) {
                 run++;
                 return;
             }
-            if (run) atomicAdd(&hist[last], run);
-            last = d;
+            if (run) flush_run();
+            lastd = d;
             run = 1;
         };
         // four 16-byte loads in flight per thread, then the rest one by one
@@ -399,20 +421,37 @@ __global__ void __launch_bounds__(kSelThreads) select_hist_kernel(CvSlot *slots,
             add(q.w);
         }
         for (unsigned long long i = n4 * 4 + (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n; i += stride) add(v[i]);
-        if (run) atomicAdd(&hist[last], run);
+        if (run) flush_run();
+        if (last) {
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                above_fx += __shfl_down_sync(0xffffffffu, above_fx, o);
+                above_n += __shfl_down_sync(0xffffffffu, above_n, o);
+            }
+            if ((threadIdx.x & 31) == 0 && above_n) {
+                atomicAdd(&S.above_fx, above_fx);
+                atomicAdd(&S.above_n, above_n);
+            }
+        }
         __syncthreads();
-        for (int i = threadIdx.x; i < nb; i += kSelThreads)
+        for (int i = threadIdx.x; i < nb; i += kSelThreads) {
             if (hist[i]) atomicAdd(&S.hist[i], hist[i]);
+            if (last && dsum[i]) atomicAdd(&S.dsum[i], dsum[i]);
+        }
         __syncthreads();
     }
 }
 
-__global__ void __launch_bounds__(256) select_pick_kernel(CvSlot *slots, int shift, int width)
+// Picks the digit of the k-th largest value from a round's counts; the last round then adds the values of the greater
+// digits to the sum and count above it.
+__global__ void __launch_bounds__(256) select_pick_kernel(CvSlot *slots, int shift, int width, int last)
 {
     CvSlot &S = slots[blockIdx.x];
     if (S.count <= S.k) return;
     __shared__ unsigned long long part[256];
+    __shared__ int picked;
     const int nb = 1 << width, per = nb / 256, t = threadIdx.x;
+    if (t == 0) picked = 0;
     // thread t holds the digits nb - (t + 1) per .. nb - t per - 1, counted from the top
     const int top = nb - t * per - 1;
     unsigned long long mine = 0;
@@ -434,57 +473,39 @@ __global__ void __launch_bounds__(256) select_pick_kernel(CvSlot *slots, int shi
         S.remaining = remaining - above;
         S.prefix |= (unsigned)digit << shift;
         S.mask |= (unsigned)(nb - 1) << shift;
+        picked = digit;
     }
     __syncthreads();
-    for (int i = t; i < nb; i += 256) S.hist[i] = 0;
-}
-
-__global__ void __launch_bounds__(kSelThreads) sum_above_kernel(CvSlot *slots, int nslots)
-{
-    for (int sl = 0; sl < nslots; sl++) {
-        CvSlot &S = slots[sl];
-        if (S.count <= S.k) continue;
-        const float threshold = __uint_as_float(S.prefix);
-        const unsigned long long n = S.list_n, n4 = n / 4, stride = (unsigned long long)gridDim.x * kSelThreads;
-        unsigned long long s = 0, c = 0;
-        auto add = [&](float v) {
-            if (v > threshold) {
-                s += __float2ull_rn(__fmul_rn(v, 16777216.0f));
-                c++;
-            }
-        };
-        // four 16-byte loads in flight per thread, then the rest one by one
-        unsigned long long i = (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x;
-        for (; i + 3 * stride < n4; i += 4 * stride) {
-            float4 q[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) q[u] = __ldg((const float4 *)S.list + i + u * stride);
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                add(q[u].x);
-                add(q[u].y);
-                add(q[u].z);
-                add(q[u].w);
-            }
+    if (last) {
+        // the values of the digits above the picked one: their sums and counts, added to those of greater prefixes
+        const int D = picked;
+        unsigned long long fx = 0, cnt = 0;
+        for (int d = D + 1 + t; d < nb; d += 256) {
+            fx += S.dsum[d];
+            cnt += S.hist[d];
         }
-        for (; i < n4; i += stride) {
-            const float4 q = __ldg((const float4 *)S.list + i);
-            add(q.x);
-            add(q.y);
-            add(q.z);
-            add(q.w);
+        part[t] = fx;
+        __syncthreads();
+        for (int o = 128; o; o >>= 1) {
+            if (t < o) part[t] += part[t + o];
+            __syncthreads();
         }
-        for (unsigned long long i = n4 * 4 + (unsigned long long)blockIdx.x * kSelThreads + threadIdx.x; i < n; i += stride) add(S.list[i]);
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            s += __shfl_down_sync(0xffffffffu, s, o);
-            c += __shfl_down_sync(0xffffffffu, c, o);
+        const unsigned long long fx_all = part[0];
+        __syncthreads();
+        part[t] = cnt;
+        __syncthreads();
+        for (int o = 128; o; o >>= 1) {
+            if (t < o) part[t] += part[t + o];
+            __syncthreads();
         }
-        if ((threadIdx.x & 31) == 0 && c) {
-            atomicAdd(&S.above_fx, s);
-            atomicAdd(&S.above_n, c);
+        if (t == 0) {
+            S.above_fx += fx_all;
+            S.above_n += part[0];
         }
+        __syncthreads();
+        for (int i = t; i < nb; i += 256) S.dsum[i] = 0;
     }
+    for (int i = t; i < nb; i += 256) S.hist[i] = 0;
 }
 
 __global__ void score_kernel(const __grid_constant__ ScoreBatch b)
@@ -565,26 +586,26 @@ cudaError_t launch_slots_reset(CvSlot *slots, int nslots, const unsigned long lo
     return after_launch();
 }
 
-cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width, cudaStream_t s)
+cudaError_t launch_topk(CvSlot *slots, int nslots, cudaStream_t s)
 {
     if (nslots <= 0) return cudaSuccess;
-    {
-        LaunchTimer t("cambi_select_hist", s);
-        select_hist_kernel<<<kSelBlocks, kSelThreads, 0, s>>>(slots, nslots, shift, width);
+    static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+    for (int round = 0; round < 3; round++) {
+        const int last = round == 2;
+        if (round > 0) {  // the first round's counts were made by the c-value kernel
+            LaunchTimer t("cambi_select_hist", s);
+            select_hist_kernel<<<kSelBlocks, kSelThreads, 0, s>>>(slots, nslots, shifts[round], widths[round], last);
+        }
+        cudaError_t e = round > 0 ? after_launch() : cudaSuccess;
+        if (e != cudaSuccess) return e;
+        {
+            LaunchTimer t("cambi_select_pick", s);
+            select_pick_kernel<<<nslots, 256, 0, s>>>(slots, shifts[round], widths[round], last);
+        }
+        e = after_launch();
+        if (e != cudaSuccess) return e;
     }
-    cudaError_t e = after_launch();
-    if (e != cudaSuccess) return e;
-    LaunchTimer t("cambi_select_pick", s);
-    select_pick_kernel<<<nslots, 256, 0, s>>>(slots, shift, width);
-    return after_launch();
-}
-
-cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s)
-{
-    if (nslots <= 0) return cudaSuccess;
-    LaunchTimer t("cambi_sum_above", s);
-    sum_above_kernel<<<kSelBlocks, kSelThreads, 0, s>>>(slots, nslots);
-    return after_launch();
+    return cudaSuccess;
 }
 
 cudaError_t launch_score(const ScoreBatch &b, cudaStream_t s)

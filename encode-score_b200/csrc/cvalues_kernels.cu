@@ -85,6 +85,15 @@ __device__ __forceinline__ void mma_u8(int (&d)[4], uint32_t a0, uint32_t a1, ui
                  : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// The band codes of the two words of x (value | mask << 15 per 16-bit half): value - band_base where masked and in the
+// band, kNone (0xFFFF) otherwise, per half.
+__device__ __forceinline__ uint32_t codes2(uint32_t x, uint32_t base2, uint32_t size2)
+{
+    const uint32_t u = __vsub2(x & 0x7FFF7FFFu, base2);  // wraps below the band
+    const uint32_t in = __vcmpltu2(u, size2) & __vcmpne2(x & 0x80008000u, 0u);
+    return u | ~in;
+}
+
 template <int TX>
 __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_constant__ CvBatch b)
 {
@@ -98,6 +107,7 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
     __shared__ unsigned long long list_base;
     __shared__ unsigned long long red_sum[kWarps];
     __shared__ unsigned red_cnt[kWarps];
+    __shared__ unsigned hist1[kCvDigits];  // the tile's positive c-values by their first radix digit
 
     __shared__ unsigned next_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -125,14 +135,22 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
 
     // 1. does any pixel of the tile need a c-value?
     bool any = false;
+    const uint32_t base2 = (uint32_t)bd.band_base * 0x10001u, size2 = (uint32_t)bd.band_size * 0x10001u;
     if (vec && cols == TX) {
+        const bool range = b.need_span >= 0;
+        const uint32_t lo2 = (uint32_t)b.need_lo * 0x10001u, span2 = (uint32_t)(range ? b.need_span : 0) * 0x10001u;
         for (int i = tid; i < kCvTY * (TX / 8); i += kCvThreads) {
             const int r = i / (TX / 8), v = i % (TX / 8);
             if (r >= rows) continue;
             const uint4 q = __ldg((const uint4 *)(J.word + (size_t)(y0 + r) * w + x0) + v);
-            auto test = [&](unsigned word) {
-                const uint16_t c0 = code_of(word & 0xFFFFu, bd), c1 = code_of(word >> 16, bd);
-                any |= (c0 != kNone && needed(c0)) || (c1 != kNone && needed(c1));
+            auto test = [&](uint32_t word) {
+                if (range) {  // masked values in the one range of needed values, both halves at once
+                    any |= (__vcmpleu2(__vsub2(word & 0x7FFF7FFFu, lo2), span2) & __vcmpne2(word & 0x80008000u, 0u)) != 0;
+                } else {
+                    const uint32_t c2 = codes2(word, base2, size2);
+                    const uint16_t c0 = (uint16_t)c2, c1 = (uint16_t)(c2 >> 16);
+                    any |= (c0 != kNone && needed(c0)) || (c1 != kNone && needed(c1));
+                }
             };
             test(q.x);
             test(q.y);
@@ -162,49 +180,49 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
     uint16_t *relneed = (uint16_t *)(smem + L.relneed);  // rank -> ranks read (bit 4: itself); 0: not served
     float *blist = (float *)(smem + L.list);
     if (tid < 32) occ[tid] = srv[tid] = 0;
+    if (tid < kCvDigits) hist1[tid] = 0;
     if (tid == 0) list_n = 0;
     __syncthreads();
 
-    // the band codes of region row r, pixels xs + 8 v .. + 7 (16-byte loads where the row allows)
-    auto load8 = [&](int r, int v, uint16_t (&cs)[8]) {
+    // the band codes of region row r, pixels xs + 8 v .. + 7, packed in pairs (16-byte loads where the row allows)
+    auto load8 = [&](int r, int v) -> uint4 {
         const int y = y0 - P + r, xv = xs + 8 * v;
         if (vec && y >= 0 && y < h && xv >= 0 && xv + 8 <= w) {
             const uint4 q = __ldg((const uint4 *)(J.word + (size_t)y * w + xv));
-            cs[0] = code_of(q.x & 0xFFFFu, bd);
-            cs[1] = code_of(q.x >> 16, bd);
-            cs[2] = code_of(q.y & 0xFFFFu, bd);
-            cs[3] = code_of(q.y >> 16, bd);
-            cs[4] = code_of(q.z & 0xFFFFu, bd);
-            cs[5] = code_of(q.z >> 16, bd);
-            cs[6] = code_of(q.w & 0xFFFFu, bd);
-            cs[7] = code_of(q.w >> 16, bd);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int x = xv + k;
-                cs[k] = (y >= 0 && y < h && x >= 0 && x < w) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
-            }
+            return make_uint4(codes2(q.x, base2, size2), codes2(q.y, base2, size2), codes2(q.z, base2, size2),
+                              codes2(q.w, base2, size2));
         }
+        uint32_t c2[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            uint32_t pairv = 0;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int x = xv + 2 * k + e;
+                const uint32_t code = (y >= 0 && y < h && x >= 0 && x < w) ? code_of(J.word[(size_t)y * w + x], bd) : kNone;
+                pairv |= code << (16 * e);
+            }
+            c2[k] = pairv;
+        }
+        return make_uint4(c2[0], c2[1], c2[2], c2[3]);
     };
-    // 2. the codes the region holds (occ) and the codes own pixels need (srv), 8 elements per thread and step; the codes
-    // themselves are kept in shared memory (row r, vector v at 16-bit element r S + 8 v) when they fit below the rank
-    // tables, so the rank plane is built without a second read of the scale
+    // 2. the codes the region holds (occ) and the codes own pixels need (srv): a warp per region row, a lane per 8
+    // pixels; the codes themselves are kept in shared memory (row r, vector v at 16-bit element r S + 8 v) when they
+    // fit below the rank tables, so the rank plane is built without a second read of the scale
     uint16_t *codes16 = (uint16_t *)(smem + L.rplane);
     const bool staged = (size_t)RH * S * 2 <= L.rank;
-    {
-        const int nv = S >> 3, total = RH * nv;
-        for (int i = tid; i < total; i += kCvThreads) {
-            const int r = i / nv, v = i - r * nv, xv = xs + 8 * v;
-            uint16_t cs[8];
-            load8(r, v, cs);
-            if (staged)
-                ((uint4 *)codes16)[i] = make_uint4(cs[0] | ((uint32_t)cs[1] << 16), cs[2] | ((uint32_t)cs[3] << 16),
-                                                   cs[4] | ((uint32_t)cs[5] << 16), cs[6] | ((uint32_t)cs[7] << 16));
-            const bool row_in_tile = r >= P && r < P + rows;
+    const int nv = S >> 3;  // vectors of a region row
+    for (int r = warp; r < RH; r += kWarps) {
+        const bool row_in_tile = r >= P && r < P + rows;
+        for (int v = lane; v < nv; v += 32) {
+            const int xv = xs + 8 * v;
+            const uint4 q = load8(r, v);
+            if (staged) ((uint4 *)codes16)[r * nv + v] = q;
+            const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
             uint16_t prev = kNone, prev_srv = kNone;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const uint16_t code = cs[k];
+                const uint16_t code = (uint16_t)(wv[k >> 1] >> (16 * (k & 1)));
                 if (code == kNone) continue;
                 if (code != prev) atomicOr(&occ[code >> 5], 1u << (code & 31));
                 prev = code;
@@ -285,16 +303,16 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
     auto build_plane = [&](int b0) {  // b0 < 0: absolute ranks; else ranks of the pass from b0 (others: no rank)
         for (int i = tid; i < RH * CS / 16; i += kCvThreads) ((uint4 *)rplane)[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
         __syncthreads();
-        const int nv = S >> 3, total = RH * nv;
-        for (int i = tid; i < total; i += kCvThreads) {
+        for (int i = tid; i < RH * nv; i += kCvThreads) {
             const int r = i / nv, v = i - r * nv;
-            uint16_t cs[8];
-            load8(r, v, cs);
+            const uint4 q = load8(r, v);
+            const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const int j = 8 * v + k - ox;  // region column
-                if (j < 0 || j >= RW || cs[k] == kNone) continue;
-                const int rk0 = rank[cs[k]];
+                const uint16_t code = (uint16_t)(wv[k >> 1] >> (16 * (k & 1)));
+                if (j < 0 || j >= RW || code == kNone) continue;
+                const int rk0 = rank[code];
                 if (rk0 == kNone) continue;
                 const int rk = b0 < 0 ? rk0 : rk0 - b0;
                 if (b0 >= 0 && (rk < 0 || rk >= kCvBins)) continue;
@@ -303,25 +321,40 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         }
     };
     if (!per_pass && staged) {
-        // the codes, vector by vector, into 8-bit ranks in place: the rank bytes of vector i (row r, bytes r CS + 8 v
-        // + k - ox) lie within the code bytes of vector i or of earlier ones (16 i + 15 at most, as CS <= 2 S), so a
-        // step's writes only cover codes read before its barrier; every region column gets a rank or kNoRank
-        const int nv = S >> 3, total = RH * nv;
-        for (int c0 = 0; c0 < total; c0 += kCvThreads) {
-            const int i = c0 + tid;
-            uint4 q = make_uint4(0, 0, 0, 0);
-            if (i < total) q = ((const uint4 *)codes16)[i];
-            __syncthreads();
-            if (i < total) {
-                const int r = i / nv, v = i - r * nv;
-                const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
+        // the codes, a warp per row as they were staged, into 8-bit ranks in place: the rank bytes of row r (r CS ..
+        // r CS + RW) lie within the code bytes of rows r and earlier (CS <= 2 S), so a step's writes only cover codes
+        // read before its barrier, and the next step reads rows whose codes lie beyond them; every region column gets
+        // a rank or kNoRank
+        auto rank_of = [&](uint32_t wv, int e) -> uint32_t {
+            const uint16_t code = (uint16_t)(wv >> (16 * e));
+            const unsigned rk = code == kNone ? kNoRank : rank[code];
+            return rk == kNone ? kNoRank : rk;
+        };
+        for (int r0 = 0; r0 < RH; r0 += kWarps) {
+            const int r = r0 + warp;
+            uint4 q[2];
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int j = 8 * v + k - ox;  // region column
-                    if (j < 0 || j >= RW) continue;
-                    const uint16_t code = (uint16_t)(wv[k >> 1] >> (16 * (k & 1)));
-                    const unsigned rk = code == kNone ? kNoRank : rank[code];
-                    rplane[r * CS + j] = (uint8_t)(rk == kNone ? kNoRank : rk);
+            for (int u = 0; u < 2; u++) {
+                const int v = lane + 32 * u;
+                q[u] = (r < RH && v < nv) ? ((const uint4 *)codes16)[r * nv + v] : make_uint4(0, 0, 0, 0);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int v = lane + 32 * u;
+                if (r >= RH || v >= nv) continue;
+                const uint32_t wv[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+                if (ox == 0 && 8 * v + 8 <= RW) {  // the vector's 8 columns are region columns 8 v .. 8 v + 7
+                    const uint32_t lo = rank_of(wv[0], 0) | (rank_of(wv[0], 1) << 8) | (rank_of(wv[1], 0) << 16) | (rank_of(wv[1], 1) << 24);
+                    const uint32_t hi = rank_of(wv[2], 0) | (rank_of(wv[2], 1) << 8) | (rank_of(wv[3], 0) << 16) | (rank_of(wv[3], 1) << 24);
+                    *(uint2 *)(rplane + r * CS + 8 * v) = make_uint2(lo, hi);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int j = 8 * v + k - ox;  // region column
+                        if (j < 0 || j >= RW) continue;
+                        rplane[r * CS + j] = (uint8_t)rank_of(wv[k >> 1], k & 1);
+                    }
                 }
             }
         }
@@ -523,6 +556,13 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
                 if (lane == __ffs(m) - 1) at = atomicAdd(&list_n, (unsigned)__popc(m));
                 at = __shfl_sync(kFull, at, __ffs(m) - 1);
                 if (pos) blist[at + __popc(m & ((1u << lane) - 1u))] = c;
+                // the first radix digit of the top-k selection, counted once per group of equal digits
+                const unsigned dg = pos ? (__float_as_uint(c) >> 21) - kCvDigit0 : 0xFFFFFFFFu;
+                const unsigned peers = __match_any_sync(kFull, dg);
+                if (pos && lane == __ffs(peers) - 1) {
+                    if (dg < kCvDigits) atomicAdd(&hist1[dg], (unsigned)__popc(peers));
+                    else atomicAdd(&SL.hist[dg + kCvDigit0], (unsigned)__popc(peers));  // not reached: c in [0.5, 2^13)
+                }
             }
             if (served && J.plane) J.plane[(size_t)(y0 + r) * w + x0 + cc] = c;
             if (pos) {
@@ -548,6 +588,7 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         red_cnt[warp] = my_cnt;
     }
     __syncthreads();
+    if (tid < kCvDigits && hist1[tid]) atomicAdd(&SL.hist[kCvDigit0 + tid], hist1[tid]);
     if (tid == 0) {
         unsigned long long s = 0;
         unsigned c = 0;
@@ -600,9 +641,21 @@ cudaError_t launch_cvalues_tx(const CvBatch &b, cudaStream_t s)
 int tile_cols_of(const CvJob &j) { return j.tile_cols == 128 ? 128 : 64; }
 }  // namespace
 
-cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s)
+cudaError_t launch_cvalues(const CvBatch &batch, cudaStream_t s)
 {
-    if (b.total_tiles <= 0) return cudaSuccess;
+    if (batch.total_tiles <= 0) return cudaSuccess;
+    CvBatch b = batch;
+    // the values whose codes need c-values, as one range when they are one (they are for CAMBI's thresholds)
+    int lo = -1, hi = -2;
+    bool one_range = true;
+    for (int code = 0; code < b.band.band_size; code++) {
+        if (!cvalue_dists(code, b.band)) continue;
+        if (lo < 0) lo = code;
+        else if (code != hi + 1) one_range = false;
+        hi = code;
+    }
+    b.need_lo = lo < 0 ? 0 : lo + b.band.band_base;
+    b.need_span = !one_range ? -1 : lo < 0 ? -1 : hi - lo;
     bool has64 = false, has128 = false;
     for (int j = 0; j < b.njobs; j++) (tile_cols_of(b.job[j]) == 128 ? has128 : has64) = true;
     if (!(has64 && has128)) return has128 ? launch_cvalues_tx<128>(b, s) : launch_cvalues_tx<64>(b, s);

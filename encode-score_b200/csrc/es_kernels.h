@@ -111,6 +111,9 @@ cudaError_t launch_decimate_mode(DecBatch &b, cudaStream_t s);
 // ---- c-values --------------------------------------------------------------------------------------------------------
 // Per picture-scale counters in device memory. The c-values are exact multiples of 2^-24 (they are at least 0.5), so
 // their sum is kept exactly as an integer in those units; the order of additions does not matter.
+// The c-value kernel also counts the positive values by the top 11 bits of their floats (the first radix digit of the
+// top-k selection): at least 0.5 and below 2^13, so those digits lie in kCvDigit0 .. kCvDigit0 + 55.
+constexpr unsigned kCvDigit0 = 0x3F000000u >> 21, kCvDigits = 64;
 struct CvSlot {
     unsigned long long sum_fx, count;  // positive c-values: sum in 2^-24 units, number
     unsigned long long list_n;         // values appended to `list`
@@ -118,7 +121,8 @@ struct CvSlot {
     unsigned long long remaining, above_fx, above_n;
     unsigned prefix, mask;             // radix select state
     float *list;                       // positive c-values (capacity n)
-    unsigned hist[2048];
+    unsigned hist[2048];               // counts of the current radix digit
+    unsigned long long dsum[1024];     // last round: sums (2^-24 units) of the values of each last digit
 };
 
 struct CvJob {
@@ -146,6 +150,7 @@ struct CvBatch {
     unsigned long long *tile_mass;
     // Optional: run[job.run_index] == 0 skips the job's tiles.
     const int *run;
+    int need_lo, need_span;  // set by the launcher: as Prep0Batch's
 };
 // Blocks of a tile-list launch.
 constexpr int kCvListBlocks = 148 * 4;
@@ -160,10 +165,10 @@ cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s);
 // Clears the counters of slots [0, nslots) and sets each slot's n and k.
 cudaError_t launch_slots_reset(CvSlot *slots, int nslots, const unsigned long long *n, const unsigned long long *k,
                                cudaStream_t s);
-// One radix round of the exact k-th largest c-value of every slot whose positive count exceeds k.
-cudaError_t launch_select_round(CvSlot *slots, int nslots, int shift, int width, cudaStream_t s);
-// Sum and count of the values above the selected threshold.
-cudaError_t launch_sum_above(CvSlot *slots, int nslots, cudaStream_t s);
+// The exact k-th largest c-value, and the sum and count of the values above it, of every slot whose positive count
+// exceeds k, after the c-value launches (which leave the first digit's counts in each slot): three radix rounds of 11,
+// 11 and 10 bits over the slots' lists, the last one also summing what lies above the selected value.
+cudaError_t launch_topk(CvSlot *slots, int nslots, cudaStream_t s);
 struct ScoreJob {
     int first_slot;  // kScales consecutive slots
     int window;

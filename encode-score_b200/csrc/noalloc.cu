@@ -79,6 +79,7 @@ __global__ void noalloc_setup_kernel(CvSlot *slots, float *lut, const __grid_con
     }
     CvSlot &S = slots[blockIdx.x];
     for (int i = threadIdx.x; i < 2048; i += blockDim.x) S.hist[i] = 0;
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) S.dsum[i] = 0;
     if (threadIdx.x == 0) {
         S.sum_fx = S.count = S.list_n = 0;
         S.n = st.n[blockIdx.x];
@@ -177,10 +178,7 @@ extern "C" int es_cambi_score_noalloc(uint64_t img, int pitch, int w, int h, int
         cb.lut = (const float *)(base + c.lut);
         cb.slots = slots;
         cuda_check(launch_cvalues(cb, s), "cambi c-values");
-        static const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
-        for (int round = 0; round < 3; round++)
-            cuda_check(launch_select_round(slots, kScales, shifts[round], widths[round], s), "cambi top-k");
-        cuda_check(launch_sum_above(slots, kScales, s), "cambi top-k");
+        cuda_check(launch_topk(slots, kScales, s), "cambi top-k");
         ScoreBatch sb{};
         sb.njobs = 1;
         sb.job[0].first_slot = 0;
