@@ -105,8 +105,11 @@ __global__ void __launch_bounds__(256) thumb_rows_kernel(const __grid_constant__
 // Thread l: the total of lag l, sum over probe frames i and pixels p (in that order) of |ref[l + i][p] - probe[i][p]|,
 // the difference in float and the sum in double (src/main.cpp:342-346). Frames are stored one after another, so the
 // pairs a lag reads are two contiguous runs of n_probe x 2304 floats. Each lag is one chain of dependent additions;
-// one warp per block spreads the lags over the SMs, and with 16-byte aligned arrays (`vec`) each lane reads its next
-// 8 values with two 16-byte loads, so a warp's loads touch one sector per lane per 8 additions.
+// one warp per block spreads the lags over the SMs, and with 16-byte aligned arrays (`vec`) each lane reads its values
+// 8 at a time with two 16-byte loads per array, kDepth groups of 8 ahead of the additions, so the chain waits on the
+// additions rather than on the loads; the order of the additions is unchanged.
+constexpr int kDepth = 4;
+
 __global__ void __launch_bounds__(32) offset_totals_kernel(const float *ref, const float *probe, int n_probe, int lags, double *totals,
                                                            int vec)
 {
@@ -118,16 +121,39 @@ __global__ void __launch_bounds__(32) offset_totals_kernel(const float *ref, con
     auto add = [&](float a, float p) { total = __dadd_rn(total, (double)fabsf(__fsub_rn(a, p))); };
     if (vec) {
         const float4 *r4 = (const float4 *)r, *p4 = (const float4 *)probe;
-        for (long long k = 0; k < count / 4; k += 2) {
-            const float4 a0 = __ldg(r4 + k), a1 = __ldg(r4 + k + 1), p0 = __ldg(p4 + k), p1 = __ldg(p4 + k + 1);
-            add(a0.x, p0.x);
-            add(a0.y, p0.y);
-            add(a0.z, p0.z);
-            add(a0.w, p0.w);
-            add(a1.x, p1.x);
-            add(a1.y, p1.y);
-            add(a1.z, p1.z);
-            add(a1.w, p1.w);
+        const long long nq = count / 4;  // float4s per array, a multiple of 2
+        float4 ra[kDepth][2], pa[kDepth][2];
+#pragma unroll
+        for (int d = 0; d < kDepth; d++) {
+            const long long q = 2 * d;
+            if (q < nq) {
+                ra[d][0] = __ldg(r4 + q);
+                ra[d][1] = __ldg(r4 + q + 1);
+                pa[d][0] = __ldg(p4 + q);
+                pa[d][1] = __ldg(p4 + q + 1);
+            }
+        }
+        for (long long k = 0; k < nq; k += 2 * kDepth) {
+#pragma unroll
+            for (int d = 0; d < kDepth; d++) {
+                if (k + 2 * d >= nq) break;
+                const float4 a0 = ra[d][0], a1 = ra[d][1], p0 = pa[d][0], p1 = pa[d][1];
+                const long long q = k + 2 * d + 2 * kDepth;  // the group this slot holds next
+                if (q < nq) {
+                    ra[d][0] = __ldg(r4 + q);
+                    ra[d][1] = __ldg(r4 + q + 1);
+                    pa[d][0] = __ldg(p4 + q);
+                    pa[d][1] = __ldg(p4 + q + 1);
+                }
+                add(a0.x, p0.x);
+                add(a0.y, p0.y);
+                add(a0.z, p0.z);
+                add(a0.w, p0.w);
+                add(a1.x, p1.x);
+                add(a1.y, p1.y);
+                add(a1.z, p1.z);
+                add(a1.w, p1.w);
+            }
         }
     } else {
 #pragma unroll 8

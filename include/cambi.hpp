@@ -13,7 +13,7 @@
 class Cambi {
 public:
     // `depth` is the bit depth of the planes it will be given, 8 or 10 (src/cambi.hpp:11-12).
-    Cambi(const Kernels &k, int w, int h, int depth) { es_check(es_cambi_create(k.module(), w, h, depth, &c_), "cambi buffers"); }
+    Cambi(const Kernels &k, int w, int h, int depth) { es_check(es_cambi_create(k.handle(), w, h, depth, &c_), "cambi buffers"); }
     ~Cambi() { es_cambi_destroy(c_); }
     Cambi(const Cambi &) = delete;
     Cambi &operator=(const Cambi &) = delete;

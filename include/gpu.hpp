@@ -41,8 +41,11 @@ public:
         es_check(es_module_get(module_, name, &f), name);
         return (CUfunction)f;
     }
-    // The library's module handle (the reference returns its CUmodule; this one is only meaningful to es_b200.h).
-    es_module *module() const { return module_; }
+    // src/gpu.hpp:19. The library's kernels live in the CUDA runtime's own module of libes_b200.so, not in a module
+    // loaded with cuModuleLoadData, so there is no CUmodule to hand out: this returns a null handle (the reference's
+    // program never calls it). handle() is the library's own module handle, for the es_b200.h calls.
+    CUmodule module() const { return nullptr; }
+    es_module *handle() const { return module_; }
     // src/gpu.cpp:15-19
     static void launch(CUfunction f, unsigned w, unsigned h, void **args, CUstream stream = nullptr)
     {
