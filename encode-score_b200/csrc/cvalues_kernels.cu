@@ -28,6 +28,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCvChunk = 4;                   // rows whose c-values are computed together (threads = 4 x tile width)
+constexpr int kRowBufs = 2;                   // column-count buffers: rows of a chunk whose window counts share a barrier
 constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
 constexpr unsigned kNoRank = 0xFFu;           // rank plane: no relevant code
 constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks can hold
@@ -61,7 +62,7 @@ __host__ __device__ inline CvLayout cv_layout(int tx, int pad)
     l.rplane = 0;
     l.wcount = align16(l.rplane + rh * cv_cs(tx, pad));
     l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * cv_ws(tx) * 2);
-    l.rank = align16(l.cols + (size_t)kCvBins * cv_cstr(tx, pad));
+    l.rank = align16(l.cols + (size_t)kRowBufs * kCvBins * cv_cstr(tx, pad));
     l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
     l.list = align16(l.relneed + (size_t)kMaxBand * 2);
@@ -381,7 +382,7 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
     // holds the ranks' column counts (8 bits: at most 2 pad + 1 rows) and B[j][x] = 1 for x <= j <= x + 2 pad; exact
     // in the 32-bit accumulators. Warp w makes output columns 8 w .. 8 w + 7 (one n tile) for ranks 0-15 and 16-31 (two
     // m tiles), over the k-steps of 32 region columns its window reaches.
-    uint8_t *colc = smem + L.cols;                       // [rank][CSTR]: column counts of the pass's ranks
+    uint8_t *colc = smem + L.cols;                       // [buffer][rank][CSTR]: column counts of the pass's ranks
     uint16_t *wc16 = (uint16_t *)(smem + L.wcount);      // [chunk row][rank][kCvWS]: window counts
     const int NK = cv_nk(TX, P), CSTR = cv_cstr(TX, P);
     const int g = lane >> 2, t = lane & 3;
@@ -407,7 +408,7 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         const int off = per_pass ? 0 : b0;  // plane value of pass rank k: k + off
         if (per_pass) build_plane(b0);
         if (tid < kCvTY) rowneed[tid] = 0;
-        for (int i = tid; i < kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
+        for (int i = tid; i < kRowBufs * kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
         __syncthreads();
         // the pass ranks each row's pixels read: first the served pass ranks present in each row (TX / 4 lanes per
         // row, 4 pixels per lane from two aligned words of the rank plane), then, per row, the ranks those read
@@ -448,21 +449,43 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
             const int k = (int)v - off;
             return (v != kNoRank && k >= 0 && k < kCvBins) ? k : -1;
         };
-        if (pass_any) {  // column counts of the first 2 pad + 1 region rows
-            const int last = min(2 * P, RH - 1);
+        // buffer bf holds the column counts of tile row t = bf (mod kRowBufs): region rows t .. t + 2 pad; first the
+        // rows 0 .. kRowBufs - 1
+        if (pass_any) {
             for (int c = tid; c < RW; c += kCvThreads)
-                for (int rr = 0; rr <= last; rr++) {
-                    const int k = rank_at(rr, c);
-                    if (k >= 0) colc[k * CSTR + c]++;
+#pragma unroll
+                for (int bf = 0; bf < kRowBufs; bf++) {
+                    uint8_t *col = colc + bf * kCvBins * CSTR + c;
+                    for (int rr = bf; rr <= min(bf + 2 * P, RH - 1); rr++) {
+                        const int k = rank_at(rr, c);
+                        if (k >= 0) col[k * CSTR]++;
+                    }
                 }
         }
         __syncthreads();
+        // moves every buffer on by kRowBufs tile rows, from the group of tile rows starting at t0
+        auto slide = [&](int t0) {
+            for (int c = tid; c < RW; c += kCvThreads)
+#pragma unroll
+                for (int bf = 0; bf < kRowBufs; bf++) {
+                    uint8_t *col = colc + bf * kCvBins * CSTR + c;
+#pragma unroll
+                    for (int q = 0; q < kRowBufs; q++) {
+                        const int leave = t0 + bf + q, enter = leave + 2 * P + 1;
+                        const int kl = rank_at(leave, c), ke = enter < RH ? rank_at(enter, c) : -1;
+                        if (kl != ke) {
+                            if (kl >= 0) col[kl * CSTR]--;
+                            if (ke >= 0) col[ke * CSTR]++;
+                        }
+                    }
+                }
+        };
         // window counts of chunk row i, for the m tiles the row reads, over N k-steps (N the same for the warp)
-        auto window_counts_n = [&](auto n_ksteps, int i, uint32_t need) {
+        auto window_counts_n = [&](auto n_ksteps, int i, uint32_t need, int bf) {
             constexpr int N = decltype(n_ksteps)::value;
             const bool m0 = (need & 0xFFFFu) != 0, m1 = (need >> 16) != 0;
             int acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-            const uint32_t at0 = cbase + lrow * CSTR + 32 * ks_lo + lcol;
+            const uint32_t at0 = cbase + (uint32_t)(bf * kCvBins * CSTR) + lrow * CSTR + 32 * ks_lo + lcol;
 #pragma unroll
             for (int kk = 0; kk < N; kk++) {
                 uint32_t a0, a1, a2, a3;
@@ -486,14 +509,14 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
                 *(uint32_t *)(wrow + 24 * kCvWS) = __byte_perm((uint32_t)acc[1][2], (uint32_t)acc[1][3], 0x5410);
             }
         };
-        auto window_counts = [&](int i, uint32_t need) {
+        auto window_counts = [&](int i, uint32_t need, int bf) {
             switch (ks_hi - ks_lo) {  // the same for the whole warp
-            case 0: window_counts_n(std::integral_constant<int, 1>{}, i, need); break;
-            case 1: window_counts_n(std::integral_constant<int, 2>{}, i, need); break;
-            case 2: window_counts_n(std::integral_constant<int, 3>{}, i, need); break;
-            case 3: window_counts_n(std::integral_constant<int, 4>{}, i, need); break;
-            case 4: window_counts_n(std::integral_constant<int, 5>{}, i, need); break;
-            default: window_counts_n(std::integral_constant<int, 6>{}, i, need); break;
+            case 0: window_counts_n(std::integral_constant<int, 1>{}, i, need, bf); break;
+            case 1: window_counts_n(std::integral_constant<int, 2>{}, i, need, bf); break;
+            case 2: window_counts_n(std::integral_constant<int, 3>{}, i, need, bf); break;
+            case 3: window_counts_n(std::integral_constant<int, 4>{}, i, need, bf); break;
+            case 4: window_counts_n(std::integral_constant<int, 5>{}, i, need, bf); break;
+            default: window_counts_n(std::integral_constant<int, 6>{}, i, need, bf); break;
             }
         };
         const int ci = tid / TX, cc = tid % TX;  // this thread's pixel in a chunk
@@ -502,23 +525,22 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
             bool chunk_any = false;
             for (int i = 0; i < n_rows; i++) {
                 const int r = r0 + i;
-                if (r > 0 && pass_any) {  // slide the column counts down to region rows r .. r + 2 pad
-                    __syncthreads();      // every warp has read the counts of the row before
-                    for (int c = tid; c < RW; c += kCvThreads) {
-                        const int kl = rank_at(r - 1, c), ke = r + 2 * P < RH ? rank_at(r + 2 * P, c) : -1;
-                        if (kl != ke) {
-                            if (kl >= 0) colc[kl * CSTR + c]--;
-                            if (ke >= 0) colc[ke * CSTR + c]++;
-                        }
-                    }
+                if (i > 0 && i % kRowBufs == 0 && pass_any) {  // the buffers on to rows r .. r + kRowBufs - 1
+                    __syncthreads();  // every warp has read the counts of the rows before
+                    slide(r - kRowBufs);
                     __syncthreads();
                 }
                 const uint32_t need = rowneed[r];
                 chunk_any |= need != 0;
-                if (need) window_counts(i, need);
+                if (need) window_counts(i, need, r % kRowBufs);
             }
-            if (!chunk_any) continue;
             __syncthreads();
+            // the buffers move past this chunk beside its c-values (they touch no buffer the c-values read)
+            if (pass_any && r0 + kCvChunk < rows) slide(r0 + kCvChunk - kRowBufs);
+            if (!chunk_any) {
+                __syncthreads();
+                continue;
+            }
             // the chunk's c-values, one pixel per thread
             float c = 0.0f;
             bool served = false;
