@@ -450,6 +450,7 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
     if (!src_only) {
         const uint16_t *a = J.ry, *b = J.dy[p];
         const size_t nv = (((uintptr_t)a | (uintptr_t)b) & 15) ? 0 : n / 8;
+#pragma unroll 4
         for (size_t i = i0; i < nv; i += stride) {
             const uint4 x = __ldg((const uint4 *)a + i), y = __ldg((const uint4 *)b + i);
             sy += sq(x.x, y.x) + sq(x.y, y.y) + sq(x.z, y.z) + sq(x.w, y.w);
@@ -469,6 +470,7 @@ __global__ void __launch_bounds__(256) pair_sums_kernel(const __grid_constant__ 
         cs += (unsigned long long)__double2ll_rn(__dmul_rn(__dsqrt_rn((double)(eu * eu + ev * ev)), 1073741824.0));
     };
     const size_t cnv = (((uintptr_t)u | (uintptr_t)v | (uintptr_t)J.ru | (uintptr_t)J.rv) & 15) ? 0 : cn / 8;
+#pragma unroll 2
     for (size_t i = i0; i < cnv; i += stride) {
         const uint4 uq = __ldg((const uint4 *)u + i), vq = __ldg((const uint4 *)v + i);
         if (!src_only) {

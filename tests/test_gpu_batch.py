@@ -155,7 +155,14 @@ def test_batch_rejects_bad_arguments(cuda, module):
     with pytest.raises(es_b200.EsError):
         es_b200.Batch(module, [(15, 16, 10, 1)])
     with pytest.raises(es_b200.EsError):
-        es_b200.Batch(module, [(64, 64, 10, 16)] * 2)  # 34 pictures
+        es_b200.Batch(module, [(64, 64, 10, 16)] * 4)  # 68 pictures
+    with pytest.raises(es_b200.EsError):
+        es_b200.Batch(module, [(64, 64, 10, 1)] * 33)  # 33 sources
+    with pytest.raises(es_b200.EsError):
+        es_b200.Batch(module, [(64, 64, 10, 1)], tuning={(64, 64): {"rows": [64] * 5, "cols": [96] * 5}})
+    # the largest batch: 32 sources and 64 pictures
+    big = es_b200.Batch(module, [(64, 64, 10, 1)] * 32, use_graphs=False)
+    big.close()
     b = es_b200.Batch(module, [(64, 64, 10, 1)])
     with pytest.raises(es_b200.EsError):
         b.collect(0)
