@@ -72,7 +72,7 @@ def main() -> None:
             return times["cambi_cvalues"][0] / args.steps
 
         t0 = time.time()
-        rows, cols = [64] * 5, [128, 128, 64, 64, 64]  # the library's defaults
+        rows, cols = [64] * 5, [64] * 5  # the library's defaults
         best_ms = time_shape(rows, cols)
         base_ms = best_ms
         tried = [[list(rows), list(cols), best_ms]]

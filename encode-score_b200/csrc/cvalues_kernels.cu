@@ -28,7 +28,10 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCvChunk = 4;                   // rows whose c-values are computed together (threads = 4 x tile width)
-constexpr int kRowBufs = 2;                   // column-count buffers: rows of a chunk whose window counts share a barrier
+// Column-count buffers: kRowBufs rows of a chunk share one slide and its pair of barriers, each row reading its own
+// buffer. One buffer (a slide and two barriers per row) measured fastest: with 2 or 4 the extra slide work cost more
+// than the barriers saved.
+constexpr int kRowBufs = 1;
 constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
 constexpr unsigned kNoRank = 0xFFu;           // rank plane: no relevant code
 constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks can hold
@@ -207,18 +210,21 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         }
         return make_uint4(c2[0], c2[1], c2[2], c2[3]);
     };
-    // 2. the codes the region holds (occ) and the codes own pixels need (srv): a warp per region row, a lane per 8
-    // pixels; the codes themselves are kept in shared memory (row r, vector v at 16-bit element r S + 8 v) when they
-    // fit below the rank tables, so the rank plane is built without a second read of the scale
+    // 2. the codes the region holds (occ) and the codes own pixels need (srv), 8 pixels per thread and step (all
+    // threads busy: a warp per row would leave lanes idle on narrow regions); the codes themselves are kept in shared
+    // memory (row r, vector v at 16-bit element r S + 8 v) when they fit below the rank tables, so the rank plane is
+    // built without a second read of the scale
     uint16_t *codes16 = (uint16_t *)(smem + L.rplane);
     const bool staged = (size_t)RH * S * 2 <= L.rank;
     const int nv = S >> 3;  // vectors of a region row
-    for (int r = warp; r < RH; r += kWarps) {
+    const unsigned nv_magic = 0xFFFFFFFFu / (unsigned)nv + 1u;  // i / nv = umulhi(i, magic) for i < 2^16, nv < 64
+    for (int i = tid; i < RH * nv; i += kCvThreads) {
+        const int r = (int)__umulhi((unsigned)i, nv_magic), v = i - r * nv;
         const bool row_in_tile = r >= P && r < P + rows;
-        for (int v = lane; v < nv; v += 32) {
+        {
             const int xv = xs + 8 * v;
             const uint4 q = load8(r, v);
-            if (staged) ((uint4 *)codes16)[r * nv + v] = q;
+            if (staged) ((uint4 *)codes16)[i] = q;
             const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
             uint16_t prev = kNone, prev_srv = kNone;
 #pragma unroll
@@ -322,37 +328,31 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         }
     };
     if (!per_pass && staged) {
-        // the codes, a warp per row as they were staged, into 8-bit ranks in place: the rank bytes of row r (r CS ..
-        // r CS + RW) lie within the code bytes of rows r and earlier (CS <= 2 S), so a step's writes only cover codes
-        // read before its barrier, and the next step reads rows whose codes lie beyond them; every region column gets
-        // a rank or kNoRank
+        // the codes, vector by vector, into 8-bit ranks in place: the rank bytes of vector i (row r, bytes r CS + 8 v
+        // + k - ox) lie within the code bytes of vector i or of earlier ones (16 i + 15 at most, as CS <= 2 S), so a
+        // step's writes only cover codes read before its barrier; every region column gets a rank or kNoRank
         auto rank_of = [&](uint32_t wv, int e) -> uint32_t {
             const uint16_t code = (uint16_t)(wv >> (16 * e));
             const unsigned rk = code == kNone ? kNoRank : rank[code];
             return rk == kNone ? kNoRank : rk;
         };
-        for (int r0 = 0; r0 < RH; r0 += kWarps) {
-            const int r = r0 + warp;
-            uint4 q[2];
-#pragma unroll
-            for (int u = 0; u < 2; u++) {
-                const int v = lane + 32 * u;
-                q[u] = (r < RH && v < nv) ? ((const uint4 *)codes16)[r * nv + v] : make_uint4(0, 0, 0, 0);
-            }
+        const int total = RH * nv;
+        for (int c0 = 0; c0 < total; c0 += kCvThreads) {
+            const int i = c0 + tid;
+            uint4 q = make_uint4(0, 0, 0, 0);
+            if (i < total) q = ((const uint4 *)codes16)[i];
             __syncthreads();
-#pragma unroll
-            for (int u = 0; u < 2; u++) {
-                const int v = lane + 32 * u;
-                if (r >= RH || v >= nv) continue;
-                const uint32_t wv[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
-                if (ox == 0 && 8 * v + 8 <= RW) {  // the vector's 8 columns are region columns 8 v .. 8 v + 7
+            if (i < total) {
+                const int r = (int)__umulhi((unsigned)i, nv_magic), v = i - r * nv;
+                const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
+                if (ox == 0 && 8 * v + 8 <= RW) {
                     const uint32_t lo = rank_of(wv[0], 0) | (rank_of(wv[0], 1) << 8) | (rank_of(wv[1], 0) << 16) | (rank_of(wv[1], 1) << 24);
                     const uint32_t hi = rank_of(wv[2], 0) | (rank_of(wv[2], 1) << 8) | (rank_of(wv[3], 0) << 16) | (rank_of(wv[3], 1) << 24);
                     *(uint2 *)(rplane + r * CS + 8 * v) = make_uint2(lo, hi);
                 } else {
 #pragma unroll
                     for (int k = 0; k < 8; k++) {
-                        const int j = 8 * v + k - ox;  // region column
+                        const int j = 8 * v + k - ox;
                         if (j < 0 || j >= RW) continue;
                         rplane[r * CS + j] = (uint8_t)rank_of(wv[k >> 1], k & 1);
                     }

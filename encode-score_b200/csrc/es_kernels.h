@@ -156,9 +156,10 @@ struct CvBatch {
 constexpr int kCvListBlocks = 148 * 4;
 constexpr int kCvTX = 64, kCvTY = 64, kCvThreads = 256, kCvBins = 32;
 size_t cvalues_smem_bytes(int max_pad, int tile_cols);
-// The c-value tile width of a scale when nothing else asks for one: 128 columns where pictures are wide (scales 0 and
-// 1: the staged margins cost less per output pixel), 64 below (more, shorter-lived tiles for the small scales).
-inline int cv_default_tile_cols(int scale) { return scale < 2 ? 128 : 64; }
+// The c-value tile width of a scale when nothing else asks for one: 64 columns (128-column tiles stage less margin per
+// output pixel, but two 512-thread blocks per SM measured slower than four 256-thread ones at every scale of a 4K
+// picture; the autotuner may still pick them).
+inline int cv_default_tile_cols(int /*scale*/) { return 64; }
 cudaError_t launch_cvalues(const CvBatch &b, cudaStream_t s);
 
 // ---- top-k pooling and score -------------------------------------------------------------------------------------

@@ -311,7 +311,7 @@ typedef struct {
     int n_encodes; /* 1 to 16 */
     int cv_tile_rows[5]; /* rows of the c-value tiles per scale: 64, 32 or 16 (0 = 64); an autotuner's choice. With
                           * the learned proposal on, scales 0 and 1 use 64. */
-    int cv_tile_cols[5]; /* columns of the c-value tiles per scale: 64 or 128 (0 = 128 at scales 0 and 1, 64 below);
+    int cv_tile_cols[5]; /* columns of the c-value tiles per scale: 64 or 128 (0 = 64);
                           * an autotuner's choice. With the learned proposal on, every scale uses 64. */
 } es_batch_source;
 typedef struct {
