@@ -34,8 +34,8 @@ __device__ __forceinline__ uint16_t mode3(uint16_t a, uint16_t b, uint16_t c)
 // The plane is staged with its margins (16-byte loads for tiles inside the picture; an 8-bit plane becomes 10-bit
 // anti-dithered values in a second buffer). A warp per staged row packs the flat pixels into bit words by ballot. Each
 // warp then walks 8 rows of the tile, a lane taking two neighbouring columns as the two halves of 32-bit words: the 7
-// flat bits around each column come from one funnel shift and two popcounts and are summed over 7 rows as they go, and
-// the 3 x 3 mode filter runs on both columns at once with 16-bit SIMD compares and minima. The scale-0 words at even
+// flat bits around each column come from one funnel shift and two popcounts and are summed over 7 rows as they go (both
+// counts in one register), and the 3 x 3 mode filter reads both columns' neighbours with 32-bit loads. The scale-0 words at even
 // positions, with a ring of them one step outside the tile (made on their own), then give the tile's scale-1 words
 // (decimation and mode filter of the decimated values) without another read of scale 0.
 // Staged region: columns x0-8 .. x0+71 (index x - (x0-8)), rows y0-5 .. y0+69 (index y - (y0-5)).
@@ -47,16 +47,15 @@ constexpr int kP0FR = 73, kP0FX = 5;     // flat rows y0-5 .. y0+67; bit i of a 
 constexpr int kP0D = 34;                 // scale-0 words (x0-2+2X, y0-2+2Y), X, Y in 0 .. 33
 
 // The mode of three values per 16-bit half (the smallest when all three differ), values below 2^15.
+// The mode of three values per 16-bit half (the smallest when all three differ), as two scalar modes: the 16-bit SIMD
+// compares measured slower than the scalar selects.
 __device__ __forceinline__ uint32_t mode3x2(uint32_t a, uint32_t b, uint32_t c)
 {
-    const uint32_t eab = __vcmpeq2(a, b), eac = __vcmpeq2(a, c), ebc = __vcmpeq2(b, c);
-    const uint32_t mn = __vminu2(a, __vminu2(b, c));
-    const uint32_t bc = (b & ebc) | (mn & ~ebc);
-    const uint32_t e = eab | eac;
-    return (a & e) | (bc & ~e);
+    return (uint32_t)mode3((uint16_t)a, (uint16_t)b, (uint16_t)c) |
+           ((uint32_t)mode3((uint16_t)(a >> 16), (uint16_t)(b >> 16), (uint16_t)(c >> 16)) << 16);
 }
 
-__global__ void __launch_bounds__(256, 4) prep0_kernel(const __grid_constant__ Prep0Batch b)
+__global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ Prep0Batch b)
 {
     __shared__ __align__(16) uint16_t buf[2][kP0R][kP0C];  // [0]: the staged plane; [1]: 8-bit planes at 10 bits
     __shared__ uint32_t flatbits[kP0FR][4];                // 3 words of bits and a zero word
