@@ -187,12 +187,74 @@ __device__ __forceinline__ T half_warp_sum(T v)
 
 // Dynamic shared memory: the region planes, then the source's fine and mid numerators of each thread's 16 rows, kept
 // for the encodes' cross products (|fine| <= 9 x 1023 fits 16 bits) in shared memory so that three blocks fit an SM's
-// registers.
+// registers, and two buffers of raw region values: the next picture's region is copied in (cp.async) while the
+// current one is summed.
 struct WinStatsSmem {
     WinSmem sm;
     int mr[kWin][256];
     int16_t fr[kWin][256];
+    uint16_t raw[2][kWR][kWS];  // raw[b][r][j]: pixel (x0 - 4 + j, y0 - 4 + r) of a picture, coordinates clamped, unshifted
 };
+
+__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst_smem)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Queues the copy of `src`'s region at tile (x0, y0) into raw (unshifted; rows clamped): 8-byte asynchronous copies
+// where the columns lie inside the picture and the rows are 8-byte aligned, else plain loads and stores now. Every
+// thread commits one group of copies (possibly empty).
+__device__ __forceinline__ void stage_raw_async(uint16_t (*raw)[kWS], const uint16_t *src, int w, int h, int x0, int y0)
+{
+    if (x0 >= kM && x0 + kWT + kM <= w && (w & 3) == 0 && ((uintptr_t)src & 7) == 0) {
+        for (int i = threadIdx.x; i < kWR * 18; i += 256) {
+            const int r = i / 18, q = i - r * 18;
+            const int y = min(max(y0 - kM + r, 0), h - 1);
+            cp_async8(&raw[r][4 * q], src + (size_t)y * w + (x0 - kM) + 4 * q);
+        }
+    } else {
+        for (int i = threadIdx.x; i < kWR * kWR; i += 256) {
+            const int r = i / kWR, j = i - r * kWR;
+            const int x = min(max(x0 - kM + j, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
+            raw[r][j] = src[(size_t)y * w + x];
+        }
+    }
+    cp_async_commit();
+}
+
+// window_horizontal_sums over a raw buffer, the sums shifted left by `up` (the values at the pipeline's depth).
+__device__ __forceinline__ void window_horizontal_sums_raw(WinSmem &sm, const uint16_t (*raw)[kWS], int up)
+{
+    for (int i = threadIdx.x; i < kWR * 8; i += 256) {
+        const int r = i >> 3, c0 = 8 * (i & 7);
+        const uint4 a = *(const uint4 *)&raw[r][c0], b = *(const uint4 *)&raw[r][c0 + 8];
+        const unsigned wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        int v[16];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            v[2 * k] = (int)(wv[k] & 0xFFFFu);
+            v[2 * k + 1] = (int)(wv[k] >> 16);
+        }
+        int s9 = 0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) s9 += v[k];
+        int h9[8], h3[10];
+        h9[0] = s9 << up;
+#pragma unroll
+        for (int k = 1; k < 8; k++) {
+            s9 += v[k + 8] - v[k - 1];
+            h9[k] = s9 << up;
+        }
+#pragma unroll
+        for (int k = 0; k < 10; k++) h3[k] = (v[k + 2] + v[k + 3] + v[k + 4]) << up;
+        *(uint4 *)&sm.h9[r][c0] = make_uint4(h9[0] | (h9[1] << 16), h9[2] | (h9[3] << 16), h9[4] | (h9[5] << 16), h9[6] | (h9[7] << 16));
+        *(uint4 *)&sm.h3[r][c0] = make_uint4(h3[0] | (h3[1] << 16), h3[2] | (h3[3] << 16), h3[4] | (h3[5] << 16), h3[6] | (h3[7] << 16));
+        if (c0 == 56) *(uint32_t *)&sm.h3[r][64] = h3[8] | (h3[9] << 16);
+    }
+}
 
 __global__ void __launch_bounds__(256, 3) window_stats_kernel(const __grid_constant__ WindowBatch B)
 {
@@ -201,8 +263,7 @@ __global__ void __launch_bounds__(256, 3) window_stats_kernel(const __grid_const
     WinSmem &sm = ws.sm;
     auto &fr_s = ws.fr;
     auto &mr_s = ws.mr;
-    int jb = 0;
-    while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_block) jb++;
+    const int jb = find_job(B.njobs, (int)blockIdx.x, [&](int k) { return B.job[k].first_block; });
     const WindowJob &J = B.job[jb];
     const int bid = blockIdx.x - J.first_block;
     const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
@@ -216,12 +277,19 @@ __global__ void __launch_bounds__(256, 3) window_stats_kernel(const __grid_const
     const bool gx_on = x > 0 && x < w - 1;
     unsigned long long src_f = 0, src_m = 0, src_xx = 0, src_yy = 0;
     long long src_xy = 0;
+    const int up = J.up;
+    stage_raw_async(ws.raw[0], J.yr, w, h, x0, y0);
     for (int p = 0; p <= J.nenc; p++) {
-        const uint16_t *plane = p == 0 ? J.yr : J.yd[p - 1];
+        const uint16_t(*raw)[kWS] = ws.raw[p & 1];
+        __syncthreads();  // the walk of picture p - 1 is done with the buffer picture p + 1 goes to
+        if (p < J.nenc) {
+            stage_raw_async(ws.raw[(p + 1) & 1], J.yd[p], w, h, x0, y0);
+            cp_async_wait<1>();  // picture p's copies are in; p + 1's may still be in flight
+        } else {
+            cp_async_wait<0>();
+        }
         __syncthreads();
-        stage_window_region(sm, plane, w, h, J.up, x0, y0);
-        __syncthreads();
-        window_horizontal_sums(sm);
+        window_horizontal_sums_raw(sm, raw, up);
         __syncthreads();
         // tile row t is region row t + 4; h3 column c + 1 is centred at x, c and c + 2 at x -+ 1
         auto h3c = [&](int t) { return (int)sm.h3[t + kM][c + 1]; };
@@ -242,7 +310,7 @@ __global__ void __launch_bounds__(256, 3) window_stats_kernel(const __grid_const
         for (int i = 0; i < kWin; i++) {
             const int t = r0 + i, y = y0 + t;
             const int s3_next = s3 - h3c(t - 1) + h3c(t + 2);
-            const int f = 9 * (int)sm.y[t + kM][c + kM] - s3, m = 9 * s3 - s9;
+            const int f = 9 * ((int)raw[t + kM][c + kM] << up) - s3, m = 9 * s3 - s9;
             const int gx = gx_on ? s3r - s3l : 0;
             const int gy = (y > 0 && y < h - 1) ? s3_next - s3_prev : 0;
             if (p == 0) {
