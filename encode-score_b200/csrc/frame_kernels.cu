@@ -124,28 +124,6 @@ struct WinSmem {
     uint16_t h9[kWR][kWT];  // h9[r][c]: 9-sum of row r centred at x0 + c
 };
 
-// Stages the region of `src` (w x h, values shifted left by `up`; null reads 0) at tile (x0, y0).
-__device__ __forceinline__ void stage_window_region(WinSmem &sm, const uint16_t *src, int w, int h, int up, int x0, int y0)
-{
-    if (src && x0 >= kM && x0 + kWT + kM <= w && (w & 3) == 0 && ((uintptr_t)src & 7) == 0) {
-        // interior columns: 18 loads of 4 pixels per row (x0 - 4 is a multiple of 4)
-        for (int i = threadIdx.x; i < kWR * 18; i += 256) {
-            const int r = i / 18, q = i - r * 18;
-            const int y = min(max(y0 - kM + r, 0), h - 1);
-            uint2 v = __ldg((const uint2 *)(src + (size_t)y * w + (x0 - kM)) + q);
-            v.x <<= up;  // both 16-bit samples: they stay below 2^10 after the shift
-            v.y <<= up;
-            *(uint2 *)&sm.y[r][4 * q] = v;
-        }
-    } else {
-        for (int i = threadIdx.x; i < kWR * kWR; i += 256) {
-            const int r = i / kWR, j = i - r * kWR;
-            const int x = min(max(x0 - kM + j, 0), w - 1), y = min(max(y0 - kM + r, 0), h - 1);
-            sm.y[r][j] = src ? (uint16_t)(src[(size_t)y * w + x] << up) : (uint16_t)0;
-        }
-    }
-}
-
 // h3 and h9 of every region row: item (r, s) covers columns 8 s .. 8 s + 7 from y[r][8 s .. 8 s + 15].
 __device__ __forceinline__ void window_horizontal_sums(WinSmem &sm)
 {
@@ -383,18 +361,28 @@ __device__ __forceinline__ void window_mids(const WinSmem &sm, int c, int r0, in
     }
 }
 
+// Dynamic shared memory of persist_kernel: the region planes, the odd running sums of the region, and two buffers of
+// raw picture regions (the pictures' regions are copied in asynchronously, the first one while the sums advance).
+struct PersistSmem {
+    WinSmem sm;
+    uint16_t o_reg[kWR][kWS];
+    uint16_t raw[2][kWR][kWS];
+};
+
 __global__ void __launch_bounds__(256, 3) persist_kernel(const __grid_constant__ PersistBatch B)
 {
-    __shared__ __align__(16) WinSmem sm;
-    __shared__ __align__(16) uint16_t o_reg[kWR][kWS];
-    int jb = 0;
-    while (jb + 1 < B.njobs && (int)blockIdx.x >= B.job[jb + 1].first_block) jb++;
+    extern __shared__ __align__(16) unsigned char persist_dyn[];
+    PersistSmem &ps = *(PersistSmem *)persist_dyn;
+    WinSmem &sm = ps.sm;
+    auto &o_reg = ps.o_reg;
+    const int jb = find_job(B.njobs, (int)blockIdx.x, [&](int k) { return B.job[k].first_block; });
     const PersistJob &J = B.job[jb];
     const int bid = blockIdx.x - J.first_block;
     const int w = J.w, h = J.h, ww = w / kWin, wh = h / kWin;
     const int tiles_x = (w + kWT - 1) / kWT;
     const int x0 = (bid % tiles_x) * kWT, y0 = (bid / tiles_x) * kWT;
     const int tid = threadIdx.x, lane = tid & 31;
+    if (J.stats) stage_raw_async(ps.raw[0], J.y_c, w, h, x0, y0);  // the centre frame's region, while the sums advance
     // advance the running sums over the region: E(c) = O(c-1) - y(c) + y(c+6), O(c) = E(c-1) - y(c-7) + y(c-1)
     const uint16_t *pl[4] = {J.y_m13, J.y_m7, J.y_c, J.y_f};
     uintptr_t align = (uintptr_t)J.e_old | (uintptr_t)J.o_old | (uintptr_t)J.e_new | (uintptr_t)J.o_new;
@@ -468,11 +456,15 @@ __global__ void __launch_bounds__(256, 3) persist_kernel(const __grid_constant__
     sbb = half_warp_sum(sbb);
     long long own = 0;
     for (int p = 0; p <= J.nenc; p++) {
-        const uint16_t *plane = p == 0 ? J.y_c : J.yd[p - 1];
+        __syncthreads();  // picture p - 1's sums are read, and its buffer is the one picture p + 1 goes to
+        if (p < J.nenc) {
+            stage_raw_async(ps.raw[(p + 1) & 1], J.yd[p], w, h, x0, y0);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         __syncthreads();
-        stage_window_region(sm, plane, w, h, J.up, x0, y0);
-        __syncthreads();
-        window_horizontal_sums(sm);
+        window_horizontal_sums_raw(sm, ps.raw[p & 1], J.up);
         __syncthreads();
         int m[kWin];
         window_mids(sm, c, r0, m);
@@ -840,8 +832,10 @@ cudaError_t launch_persist(PersistBatch &b, cudaStream_t s)
         blocks += ((J.w + kWT - 1) / kWT) * ((J.h + kWT - 1) / kWT);
     }
     if (blocks == 0) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PersistSmem));
+    if (e != cudaSuccess) return e;
     LaunchTimer t("persist_stats", s);
-    persist_kernel<<<blocks, 256, 0, s>>>(b);
+    persist_kernel<<<blocks, 256, sizeof(PersistSmem), s>>>(b);
     return after_launch();
 }
 
