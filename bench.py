@@ -690,20 +690,35 @@ def main() -> None:
     # ---- end-to-end leg: host frames, copies inside the timed region ------------------------------------------
     e2e = None
     if not args.no_e2e:
+        # each step's twelve planes in one page-locked arena (each plane 256-byte aligned), copied with one
+        # cudaMemcpyAsync per step: per-copy overheads of twelve small copies left the link idle between them
+        plane_list = [(pic, a) for pic in [pool[0].source] + pool[0].encodes for a in (pic.y, pic.u, pic.v)]
+        offsets, at = [], 0
+        for _, a in plane_list:
+            offsets.append(at)
+            at += (a.size + 127) // 128 * 128
+        arena_elems = at
         host_pool = []
         for step in pool:
-            pics = []
-            for pic in [step.source] + step.encodes:
-                pics.append([torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).pin_memory() for a in (pic.y, pic.u, pic.v)])
-            host_pool.append(pics)
+            arena = torch.empty(arena_elems, dtype=torch.int16).pin_memory()
+            planes = [a for pic in [step.source] + step.encodes for a in (pic.y, pic.u, pic.v)]
+            for off, a in zip(offsets, planes):
+                arena[off:off + a.size] = torch.from_numpy(np.ascontiguousarray(a).view(np.int16).ravel())
+            host_pool.append(arena)
         # three input slots: step g + 1's copy is queued before step g - 1 is collected, so the copy stream never waits
         # for the host (with two slots and the copy queued after the collect, the host's collect time left the copy
         # engine idle for a fifth of each step)
         depth = 3
-        slots = [[[torch.empty_like(t, device="cuda") for t in pic] for pic in host_pool[0]] for _ in range(depth)]
-        views = [[es_b200.FrameView(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(), w * 2, w, 0, 2, 0, pic.depth)
-                  for p, pic in zip(slot, [pool[0].source] + pool[0].encodes)] for slot in slots]
-        h2d = sum(t.numel() * t.element_size() for pic in host_pool[0] for t in pic)
+        slots = [torch.empty(arena_elems, dtype=torch.int16, device="cuda") for _ in range(depth)]
+        views = []
+        for slot in slots:
+            base = slot.data_ptr()
+            vs = []
+            for k, pic in enumerate([pool[0].source] + pool[0].encodes):
+                y, u, v = (base + 2 * offsets[3 * k + i] for i in range(3))
+                vs.append(es_b200.FrameView(y, u, v, w * 2, w, 0, 2, 0, pic.depth))
+            views.append(vs)
+        h2d = sum(a.size * 2 for _, a in plane_list)  # the planes' bytes (the arena's alignment gaps are copied too)
         windows = (w // 16) * (h // 16)
         d2h = 8 * (3 * n_enc + 3 * (n_enc + 1)) + 136 * n_enc + 2 * 6 * windows * n_enc + 48 * (1 + n_enc)
         fr2 = {"plain": PlainForm, "batched": BatchedForm, "learned": LearnedForm}[head]()
@@ -716,9 +731,7 @@ def main() -> None:
             s = g % depth
             with torch.cuda.stream(copy_stream):
                 copy_stream.wait_event(free[s])  # the step that last read this slot is done
-                for dst_pic, src_pic in zip(slots[s], host_pool[g % len(host_pool)]):
-                    for d, hsrc in zip(dst_pic, src_pic):
-                        d.copy_(hsrc, non_blocking=True)
+                slots[s].copy_(host_pool[g % len(host_pool)], non_blocking=True)
                 copied[s].record(copy_stream)
 
         def e2e_step(g, g_first, g_end):
