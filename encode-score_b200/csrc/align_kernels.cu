@@ -102,64 +102,144 @@ __global__ void __launch_bounds__(256) thumb_rows_kernel(const __grid_constant__
     }
 }
 
-// Thread l: the total of lag l, sum over probe frames i and pixels p (in that order) of |ref[l + i][p] - probe[i][p]|,
-// the difference in float and the sum in double (src/main.cpp:342-346). Frames are stored one after another, so the
-// pairs a lag reads are two contiguous runs of n_probe x 2304 floats. Each lag is one chain of dependent additions;
-// one warp per block spreads the lags over the SMs, and with 16-byte aligned arrays (`vec`) each lane reads its values
-// 8 at a time with two 16-byte loads per array, kDepth groups of 8 ahead of the additions, so the chain waits on the
-// additions rather than on the loads; the order of the additions is unchanged.
-constexpr int kDepth = 4;
+// The total of lag l: the sum over probe frames i and pixels p (in that order) of |ref[l + i][p] - probe[i][p]|, the
+// difference in float and the sum in double (src/main.cpp:342-346). Frames are stored one after another, so a lag
+// reads two contiguous runs of n_probe x 2304 floats. One warp per lag, chunks of kChunk values, lane j holding values
+// j*kLaneVals .. j*kLaneVals + kLaneVals - 1 of a chunk.
+//
+// The running total s is a double >= 0 and every value x is a float >= 0. While s stays in one binade [2^e, 2^(e+1)),
+// s = m * u with u = 2^(e-52) and m an integer in [2^52, 2^53), and the rounded sum RN(s + x) is (m + n + r) * u where
+// n = floor(x / u) and r is 1 when the remainder of x / u is above one half, 0 below, and on an exact half the value
+// that makes m + n + r even (ties to even). x / u is exact (x has a 24-bit mantissa, u is a power of two), so n and the
+// remainder's class come from integer shifts of x's mantissa. The only state one step passes to the next beyond the
+// increment is the parity of m, so a run of values is a map from the parity coming in to (increment, parity going
+// out): a pair of increments and a pair of parities. These maps compose in order, which makes the chunk an ordered
+// warp reduction instead of a chain of kChunk dependent additions. If the chunk's end stays below 2^53 (m + the
+// increment), every intermediate sum stayed in the binade (each exact sum is within one half of the next rounded
+// one), so the result is exactly the in-order chain's. A chunk that crosses a binade, starts from s = 0, or holds a
+// value the shifts cannot represent (an increment of 2^53 or more, an infinity or NaN) is added in order, one value at
+// a time, from shared memory. Adding zeros leaves s as it is, so a chunk of zeros and the padding of the last chunk
+// are skipped. The result equals the in-order double sum bit for bit.
+constexpr int kLaneVals = 16, kChunk = 32 * kLaneVals, kLagWarps = 4;
 
-__global__ void __launch_bounds__(32) offset_totals_kernel(const float *ref, const float *probe, int n_probe, int lags, double *totals,
-                                                           int vec)
+struct ParityMap {
+    unsigned long long inc0, inc1;  // increments of m for parity 0 / 1 coming in
+    unsigned bits;                  // bit 0: parity out for 0 in, bit 1: for 1 in, bit 2: the chunk must be added in order
+};
+
+__device__ __forceinline__ ParityMap compose(const ParityMap &a, const ParityMap &b)
 {
-    const int l = blockIdx.x * 32 + threadIdx.x;
-    if (l >= lags) return;
+    const unsigned a0 = a.bits & 1u, a1 = (a.bits >> 1) & 1u, b0 = b.bits & 1u, b1 = (b.bits >> 1) & 1u;
+    ParityMap r;
+    r.inc0 = a.inc0 + (a0 ? b.inc1 : b.inc0);
+    r.inc1 = a.inc1 + (a1 ? b.inc1 : b.inc0);
+    r.bits = (a0 ? b1 : b0) | ((a1 ? b1 : b0) << 1) | ((a.bits | b.bits) & 4u);
+    return r;
+}
+
+template <bool kVec>
+__global__ void __launch_bounds__(32 * kLagWarps) offset_totals_kernel(const float *ref, const float *probe, int n_probe, int lags,
+                                                                      double *totals)
+{
+    __shared__ __align__(16) double serial[kLagWarps][kChunk];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, l = blockIdx.x * kLagWarps + w;
+    if (l >= lags) return;  // whole warps: one lag per warp
     const float *r = ref + (size_t)l * kThumbPixels;
-    const long long count = (long long)n_probe * kThumbPixels;  // a multiple of 8
-    double total = 0.0;
-    auto add = [&](float a, float p) { total = __dadd_rn(total, (double)fabsf(__fsub_rn(a, p))); };
-    if (vec) {
-        const float4 *r4 = (const float4 *)r, *p4 = (const float4 *)probe;
-        const long long nq = count / 4;  // float4s per array, a multiple of 2
-        float4 ra[kDepth][2], pa[kDepth][2];
+    const long long count = (long long)n_probe * kThumbPixels;
+    const long long chunks = (count + kChunk - 1) / kChunk;
+    constexpr int Q = kLaneVals / 4;
+    float4 ra[Q], pa[Q];
+    auto load = [&](long long c) {  // the next chunk's values, zeros past the end
+        const long long v0 = c * kChunk + lane * kLaneVals;
 #pragma unroll
-        for (int d = 0; d < kDepth; d++) {
-            const long long q = 2 * d;
-            if (q < nq) {
-                ra[d][0] = __ldg(r4 + q);
-                ra[d][1] = __ldg(r4 + q + 1);
-                pa[d][0] = __ldg(p4 + q);
-                pa[d][1] = __ldg(p4 + q + 1);
-            }
-        }
-        for (long long k = 0; k < nq; k += 2 * kDepth) {
-#pragma unroll
-            for (int d = 0; d < kDepth; d++) {
-                if (k + 2 * d >= nq) break;
-                const float4 a0 = ra[d][0], a1 = ra[d][1], p0 = pa[d][0], p1 = pa[d][1];
-                const long long q = k + 2 * d + 2 * kDepth;  // the group this slot holds next
-                if (q < nq) {
-                    ra[d][0] = __ldg(r4 + q);
-                    ra[d][1] = __ldg(r4 + q + 1);
-                    pa[d][0] = __ldg(p4 + q);
-                    pa[d][1] = __ldg(p4 + q + 1);
+        for (int t = 0; t < Q; t++) {
+            const long long v = v0 + 4 * t;
+            if (kVec) {
+                if (v < count) {
+                    ra[t] = __ldg((const float4 *)(r + v));
+                    pa[t] = __ldg((const float4 *)(probe + v));
+                } else {
+                    ra[t] = pa[t] = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
-                add(a0.x, p0.x);
-                add(a0.y, p0.y);
-                add(a0.z, p0.z);
-                add(a0.w, p0.w);
-                add(a1.x, p1.x);
-                add(a1.y, p1.y);
-                add(a1.z, p1.z);
-                add(a1.w, p1.w);
+            } else {
+                float a[4], b[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    a[k] = v + k < count ? __ldg(r + v + k) : 0.f;
+                    b[k] = v + k < count ? __ldg(probe + v + k) : 0.f;
+                }
+                ra[t] = make_float4(a[0], a[1], a[2], a[3]);
+                pa[t] = make_float4(b[0], b[1], b[2], b[3]);
             }
         }
-    } else {
-#pragma unroll 8
-        for (long long k = 0; k < count; k++) add(__ldg(r + k), __ldg(probe + k));
+    };
+    double s = 0.0;
+    if (chunks > 0) load(0);
+    for (long long c = 0; c < chunks; c++) {
+        float x[kLaneVals];
+#pragma unroll
+        for (int t = 0; t < Q; t++) {
+            x[4 * t + 0] = fabsf(__fsub_rn(ra[t].x, pa[t].x));
+            x[4 * t + 1] = fabsf(__fsub_rn(ra[t].y, pa[t].y));
+            x[4 * t + 2] = fabsf(__fsub_rn(ra[t].z, pa[t].z));
+            x[4 * t + 3] = fabsf(__fsub_rn(ra[t].w, pa[t].w));
+        }
+        if (c + 1 < chunks) load(c + 1);
+        const unsigned long long sbits = (unsigned long long)__double_as_longlong(s);
+        const int E = (int)(sbits >> 52);  // s >= 0: the biased exponent
+        const int ue = E - 1075;           // u = 2^ue
+        ParityMap m;
+        m.inc0 = m.inc1 = 0;
+        m.bits = 2u | ((E == 0 || E == 0x7ff) ? 4u : 0u);
+        bool nonzero = false;
+#pragma unroll
+        for (int j = 0; j < kLaneVals; j++) {
+            const unsigned xb = __float_as_uint(x[j]);
+            nonzero |= xb != 0;
+            const int ex = (int)(xb >> 23);  // x >= 0
+            const unsigned M = ex ? (xb & 0x7fffffu) | 0x800000u : xb;  // x = M * 2^(ex - 150), subnormals 2^-149
+            const int sh = (ex ? ex - 150 : -149) - ue;                 // x / u = M * 2^sh
+            const int left = max(sh, 0), right = min(max(-sh, 0), 25);  // M < 2^24: 25 right shifts leave 0 and a low remainder
+            if (ex == 255 || left > 29) m.bits |= 4u;
+            const unsigned long long n = ((unsigned long long)M << min(left, 29)) >> right;
+            const unsigned twice_rem = (M & ((1u << right) - 1u)) << 1, one = 1u << right;
+            const unsigned above = twice_rem > one, tie = twice_rem == one, nb = (unsigned)n & 1u;
+            const unsigned p0 = m.bits & 1u, p1 = (m.bits >> 1) & 1u;
+            const unsigned r0 = above | (tie & (p0 ^ nb)), r1 = above | (tie & (p1 ^ nb));
+            m.inc0 += n + r0;
+            m.inc1 += n + r1;
+            m.bits = (m.bits & 4u) | ((p0 ^ nb ^ r0) & 1u) | (((p1 ^ nb ^ r1) & 1u) << 1);
+        }
+        if (!__any_sync(0xffffffffu, nonzero)) continue;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {  // ordered: lane j's run, then lane j + off's
+            ParityMap o;
+            o.inc0 = __shfl_down_sync(0xffffffffu, m.inc0, off);
+            o.inc1 = __shfl_down_sync(0xffffffffu, m.inc1, off);
+            o.bits = __shfl_down_sync(0xffffffffu, m.bits, off);
+            if (lane + off < 32) m = compose(m, o);
+        }
+        const unsigned long long inc0 = __shfl_sync(0xffffffffu, m.inc0, 0), inc1 = __shfl_sync(0xffffffffu, m.inc1, 0);
+        bool in_order = (__shfl_sync(0xffffffffu, m.bits, 0) & 4u) != 0;
+        if (!in_order) {
+            const unsigned long long mant = (sbits & 0xfffffffffffffull) | (1ull << 52);
+            const unsigned long long end = mant + ((mant & 1ull) ? inc1 : inc0);
+            if (end < (1ull << 53))
+                s = __longlong_as_double((long long)(((unsigned long long)E << 52) | (end & 0xfffffffffffffull)));
+            else
+                in_order = true;
+        }
+        if (in_order) {
+#pragma unroll
+            for (int j = 0; j < kLaneVals; j++) serial[w][lane * kLaneVals + j] = (double)x[j];
+            __syncwarp();
+            if (lane == 0)
+                for (int i = 0; i < kChunk; i++) s = __dadd_rn(s, serial[w][i]);
+            s = __shfl_sync(0xffffffffu, s, 0);
+            __syncwarp();
+        }
     }
-    totals[l] = total;
+    if (lane == 0) totals[l] = s;
 }
 
 }  // namespace
@@ -181,9 +261,11 @@ cudaError_t launch_thumbnails(const ThumbBatch &b, cudaStream_t s)
 cudaError_t launch_offset_totals(const float *ref, const float *probe, int n_probe, int lags, double *totals, cudaStream_t s)
 {
     if (lags <= 0) return cudaSuccess;
-    const int vec = (((uintptr_t)ref | (uintptr_t)probe) & 15) == 0;
+    const bool vec = (((uintptr_t)ref | (uintptr_t)probe) & 15) == 0;  // rows of 2304 floats keep the alignment
     LaunchTimer t("align_offset_totals", s);
-    offset_totals_kernel<<<(lags + 31) / 32, 32, 0, s>>>(ref, probe, n_probe, lags, totals, vec);
+    const int blocks = (lags + kLagWarps - 1) / kLagWarps;
+    if (vec) offset_totals_kernel<true><<<blocks, 32 * kLagWarps, 0, s>>>(ref, probe, n_probe, lags, totals);
+    else offset_totals_kernel<false><<<blocks, 32 * kLagWarps, 0, s>>>(ref, probe, n_probe, lags, totals);
     return after_launch();
 }
 

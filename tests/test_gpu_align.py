@@ -95,6 +95,46 @@ def test_offset_totals_equal_the_oracle_bit_for_bit(cuda, module):
     assert int(np.argmin(got)) == 9
 
 
+def _rounding_case(kind, rng, n_ref, n_probe):
+    shape = (n_ref, 36, 64)
+    if kind == "tiny_differences":  # full mantissas, differences far below the total's unit, rare large ones
+        ref = rng.random(shape, dtype=np.float32)
+        probe = ref[5:5 + n_probe] * (np.float32(1) + np.ldexp(rng.integers(-4, 5, (n_probe, 36, 64)), -21).astype(np.float32))
+        probe[:, :, ::61] += np.float32(500)
+    elif kind == "exact_copy":  # lag 7 is every value zero
+        ref = (rng.integers(0, 1024, shape) / 4).astype(np.float32)
+        probe = ref[7:7 + n_probe].copy()
+    else:  # magnitudes from 2^-40 to 2^40: totals that cross many binades, values far below and far above the unit
+        ref = np.ldexp(rng.random(shape), rng.integers(-40, 41, shape)).astype(np.float32)
+        probe = np.ldexp(rng.random((n_probe, 36, 64)), rng.integers(-40, 20, (n_probe, 36, 64))).astype(np.float32)
+    return ref.astype(np.float32), probe.astype(np.float32)
+
+
+@pytest.mark.parametrize("kind", ["tiny_differences", "exact_copy", "wide_range"])
+@pytest.mark.parametrize("aligned", [True, False])
+def test_offset_totals_of_rounding_cases_bit_for_bit(cuda, module, kind, aligned):
+    """The lag totals where the in-order double sum rounds (exact halves among the cases), where a lag is all zeros,
+    and where the totals cross many binades; with 16-byte aligned arrays and with arrays one float off (scalar
+    loads), and a probe of an odd number of frames (the last chunk of each lag only part full)."""
+    rng = np.random.default_rng(21)
+    n_ref, n_probe = 31, 13
+    ref, probe = _rounding_case(kind, rng, n_ref, n_probe)
+    off = 0 if aligned else 1
+    d_ref = cuda.zeros(ref.size + 4, dtype=cuda.float32, device="cuda")
+    d_probe = cuda.zeros(probe.size + 4, dtype=cuda.float32, device="cuda")
+    d_ref[off:off + ref.size] = cuda.from_numpy(ref.ravel())
+    d_probe[off:off + probe.size] = cuda.from_numpy(probe.ravel())
+    lags = n_ref - n_probe + 1
+    totals = cuda.zeros(lags, dtype=cuda.float64, device="cuda")
+    es_b200.offset_totals(d_ref.data_ptr() + 4 * off, n_ref, d_probe.data_ptr() + 4 * off, n_probe, totals.data_ptr())
+    got = totals.cpu().numpy()
+    want = align.lag_totals(ref, probe)
+    bad = np.flatnonzero(got.view(np.uint64) != want.view(np.uint64))
+    assert bad.size == 0, f"{bad.size} lags differ, first {bad[0]}: {got[bad[0]]!r} != {want[bad[0]]!r}"
+    if kind == "exact_copy":
+        assert got[7] == 0.0 and (np.delete(got, 7) > 0).all()
+
+
 def test_find_offset_on_thumbnails_of_a_moving_sequence(cuda, module):
     """Source frames 0 .. 59 and an encode that starts 13 frames later (noisier): the thumbnails made on the GPU give
     the oracle's lag and offset; an encode of other pictures is refused."""
