@@ -46,13 +46,32 @@ constexpr int kP0X = 8, kP0Y = 5;        // staged index of x0, y0
 constexpr int kP0FR = 73, kP0FX = 5;     // flat rows y0-5 .. y0+67; bit i of a row is column x0-5+i
 constexpr int kP0D = 34;                 // scale-0 words (x0-2+2X, y0-2+2Y), X, Y in 0 .. 33
 
-// The mode of three values per 16-bit half (the smallest when all three differ), values below 2^15.
-// The mode of three values per 16-bit half (the smallest when all three differ), as two scalar modes: the 16-bit SIMD
-// compares measured slower than the scalar selects.
+// The mode of three values per 16-bit half (the smallest when all three differ), from SIMD minima and maxima only:
+// with two or three equal values the repeated one is the median, and it equals the largest unless the pair is the
+// two smallest, when it equals the smallest; with three different values the mode is the smallest. So the mode is
+// the median where the median equals the largest, else the smallest. The halves' differences are never negative, so
+// 32-bit subtraction keeps them apart, and "median below the largest" is a per-half nonzero test. (16-bit SIMD
+// compares, and two scalar modes, measured slower.)
+__device__ __forceinline__ uint32_t vmin_u16x2(uint32_t a, uint32_t b)
+{
+    uint32_t r;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t vmax_u16x2(uint32_t a, uint32_t b)
+{
+    uint32_t r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
 __device__ __forceinline__ uint32_t mode3x2(uint32_t a, uint32_t b, uint32_t c)
 {
-    return (uint32_t)mode3((uint16_t)a, (uint16_t)b, (uint16_t)c) |
-           ((uint32_t)mode3((uint16_t)(a >> 16), (uint16_t)(b >> 16), (uint16_t)(c >> 16)) << 16);
+    const uint32_t lo = vmin_u16x2(a, b), hi = vmax_u16x2(a, b);
+    const uint32_t mn = vmin_u16x2(lo, c), mx = vmax_u16x2(hi, c), md = vmax_u16x2(lo, vmin_u16x2(hi, c));
+    const uint32_t d = mx - md;  // per half, never negative: no borrow between the halves
+    const uint32_t t = (((d & 0x7FFF7FFFu) + 0x7FFF7FFFu) | d) & 0x80008000u;  // bit 15 of a half: median below max
+    const uint32_t nz = t | (t - (t >> 15));
+    return mn + ((md - mn) & ~nz);
 }
 
 __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ Prep0Batch b)
@@ -109,21 +128,26 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
         }
         __syncthreads();
     }
-    // flat: equal to the right and lower neighbours (the last column / row count as equal); nothing outside
+    // flat: equal to the right and lower neighbours (the last column / row count as equal); nothing outside. A warp
+    // takes whole flat rows, 3 ballots of 32 columns each (73 columns used).
     {
         const bool interior = x0 >= 5 && x0 + kP0T + 4 < w && y0 >= 5 && y0 + kP0T + 4 < h;
-        for (int task = warp; task < kP0FR * 3; task += 8) {
-            const int q = task / 3, k = task - q * 3;
-            const int i = 32 * k + lane, c = i + (kP0X - kP0FX), x = x0 - kP0FX + i, y = ys + q;
-            bool f = false;
-            if (i < kP0FR) {
-                const uint16_t v = buf[sel][q][c];
-                if (interior) f = v == buf[sel][q][c + 1] && v == buf[sel][q + 1][c];
-                else if (x >= 0 && x < w && y >= 0 && y < h)
-                    f = (x == w - 1 || v == buf[sel][q][c + 1]) && (y == h - 1 || v == buf[sel][q + 1][c]);
+        for (int q = warp; q < kP0FR; q += 8) {
+            const uint16_t *row = buf[sel][q], *nxt = buf[sel][q + 1];
+            const int y = ys + q;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const int i = 32 * k + lane, c = i + (kP0X - kP0FX), x = x0 - kP0FX + i;
+                bool f = false;
+                if (k < 2 || i < kP0FR) {
+                    const uint16_t v = row[c];
+                    if (interior) f = v == row[c + 1] && v == nxt[c];
+                    else if (x >= 0 && x < w && y >= 0 && y < h)
+                        f = (x == w - 1 || v == row[c + 1]) && (y == h - 1 || v == nxt[c]);
+                }
+                const uint32_t word = __ballot_sync(0xffffffffu, f);
+                if (lane == k) flatbits[q][k] = word;
             }
-            const uint32_t word = __ballot_sync(0xffffffffu, f);
-            if (lane == 0) flatbits[q][k] = word;
         }
     }
     __syncthreads();

@@ -28,10 +28,8 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCvChunk = 4;                   // rows whose c-values are computed together (threads = 4 x tile width)
-// Column-count buffers: kRowBufs rows of a chunk share one slide and its pair of barriers, each row reading its own
-// buffer. One buffer (a slide and two barriers per row) measured fastest: with 2 or 4 the extra slide work cost more
-// than the barriers saved.
-constexpr int kRowBufs = 1;
+// One column-count buffer, slid by one row between the rows' window counts (a slide and two barriers per row): two or
+// four buffers, each slid by two or four rows so that rows share barriers, measured slower (more slide work).
 constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
 constexpr unsigned kNoRank = 0xFFu;           // rank plane: no relevant code
 constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks can hold
@@ -65,7 +63,7 @@ __host__ __device__ inline CvLayout cv_layout(int tx, int pad)
     l.rplane = 0;
     l.wcount = align16(l.rplane + rh * cv_cs(tx, pad));
     l.cols = align16(l.wcount + (size_t)kCvChunk * kCvBins * cv_ws(tx) * 2);
-    l.rank = align16(l.cols + (size_t)kRowBufs * kCvBins * cv_cstr(tx, pad));
+    l.rank = align16(l.cols + (size_t)kCvBins * cv_cstr(tx, pad));
     l.nbr = align16(l.rank + (size_t)kMaxBand * 2);
     l.relneed = align16(l.nbr + (size_t)kMaxBand * 4);
     l.list = align16(l.relneed + (size_t)kMaxBand * 2);
@@ -183,7 +181,10 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
     uint32_t *nbr = (uint32_t *)(smem + L.nbr);          // rank -> neighbour rank offsets
     uint16_t *relneed = (uint16_t *)(smem + L.relneed);  // rank -> ranks read (bit 4: itself); 0: not served
     float *blist = (float *)(smem + L.list);
-    if (tid < 32) occ[tid] = srv[tid] = 0;
+    // during the staging the rank table's bytes are two flag arrays: [0, kMaxBand) codes held by the region,
+    // [kMaxBand, 2 kMaxBand) codes held by the tile's own pixels (plain byte stores: racing writers store the same 1)
+    uint8_t *seen = smem + L.rank;
+    for (int i = tid; i < 2 * kMaxBand / 16; i += kCvThreads) ((uint4 *)seen)[i] = make_uint4(0, 0, 0, 0);
     if (tid < kCvDigits) hist1[tid] = 0;
     if (tid == 0) list_n = 0;
     __syncthreads();
@@ -211,9 +212,9 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         return make_uint4(c2[0], c2[1], c2[2], c2[3]);
     };
     // 2. the codes the region holds (occ) and the codes own pixels need (srv), 8 pixels per thread and step (all
-    // threads busy: a warp per row would leave lanes idle on narrow regions); the codes themselves are kept in shared
-    // memory (row r, vector v at 16-bit element r S + 8 v) when they fit below the rank tables, so the rank plane is
-    // built without a second read of the scale
+    // threads busy: a warp per row would leave lanes idle on narrow regions), as flags turned into bit words after;
+    // the codes themselves are kept in shared memory (row r, vector v at 16-bit element r S + 8 v) when they fit below
+    // the rank tables, so the rank plane is built without a second read of the scale
     uint16_t *codes16 = (uint16_t *)(smem + L.rplane);
     const bool staged = (size_t)RH * S * 2 <= L.rank;
     const int nv = S >> 3;  // vectors of a region row
@@ -226,19 +227,25 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
             const uint4 q = load8(r, v);
             if (staged) ((uint4 *)codes16)[i] = q;
             const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
-            uint16_t prev = kNone, prev_srv = kNone;
+            const bool whole = row_in_tile && xv >= x0 && xv + 8 <= x0 + cols;  // all 8 pixels are the tile's
+            const bool part = row_in_tile && !whole && xv + 8 > x0 && xv < x0 + cols;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const uint16_t code = (uint16_t)(wv[k >> 1] >> (16 * (k & 1)));
                 if (code == kNone) continue;
-                if (code != prev) atomicOr(&occ[code >> 5], 1u << (code & 31));
-                prev = code;
+                seen[code] = 1;
                 const int x = xv + k;
-                if (row_in_tile && x >= x0 && x < x0 + cols && code != prev_srv && needed(code)) {
-                    atomicOr(&srv[code >> 5], 1u << (code & 31));
-                    prev_srv = code;
-                }
+                if (whole || (part && x >= x0 && x < x0 + cols)) seen[kMaxBand + code] = 1;
             }
+        }
+    }
+    __syncthreads();
+    for (int word = warp; word < 32; word += kWarps) {
+        const unsigned o = __ballot_sync(kFull, seen[32 * word + lane] != 0);
+        const unsigned t = __ballot_sync(kFull, seen[kMaxBand + 32 * word + lane] != 0);
+        if (lane == 0) {
+            occ[word] = o;
+            srv[word] = t & needbits[word];
         }
     }
     __syncthreads();
@@ -408,7 +415,7 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         const int off = per_pass ? 0 : b0;  // plane value of pass rank k: k + off
         if (per_pass) build_plane(b0);
         if (tid < kCvTY) rowneed[tid] = 0;
-        for (int i = tid; i < kRowBufs * kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
+        for (int i = tid; i < kCvBins * CSTR / 16; i += kCvThreads) ((uint4 *)colc)[i] = make_uint4(0, 0, 0, 0);
         __syncthreads();
         // the pass ranks each row's pixels read: first the served pass ranks present in each row (TX / 4 lanes per
         // row, 4 pixels per lane from two aligned words of the rank plane), then, per row, the ranks those read
@@ -449,43 +456,36 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
             const int k = (int)v - off;
             return (v != kNoRank && k >= 0 && k < kCvBins) ? k : -1;
         };
-        // buffer bf holds the column counts of tile row t = bf (mod kRowBufs): region rows t .. t + 2 pad; first the
-        // rows 0 .. kRowBufs - 1
+        // the column counts of tile row 0: region rows 0 .. 2 pad, a thread per column (splitting the rows between two
+        // threads and adding the halves measured no faster)
         if (pass_any) {
-            for (int c = tid; c < RW; c += kCvThreads)
-#pragma unroll
-                for (int bf = 0; bf < kRowBufs; bf++) {
-                    uint8_t *col = colc + bf * kCvBins * CSTR + c;
-                    for (int rr = bf; rr <= min(bf + 2 * P, RH - 1); rr++) {
-                        const int k = rank_at(rr, c);
-                        if (k >= 0) col[k * CSTR]++;
-                    }
+            for (int c = tid; c < RW; c += kCvThreads) {
+                uint8_t *col = colc + c;
+                for (int rr = 0; rr <= min(2 * P, RH - 1); rr++) {
+                    const int k = rank_at(rr, c);
+                    if (k >= 0) col[k * CSTR]++;
                 }
+            }
         }
         __syncthreads();
-        // moves every buffer on by kRowBufs tile rows, from the group of tile rows starting at t0
+        // moves the column counts on from tile row t0 to t0 + 1, a thread per column (the leaving and the entering
+        // pixel of a column on two threads measured slower: twice the rank reads)
         auto slide = [&](int t0) {
-            for (int c = tid; c < RW; c += kCvThreads)
-#pragma unroll
-                for (int bf = 0; bf < kRowBufs; bf++) {
-                    uint8_t *col = colc + bf * kCvBins * CSTR + c;
-#pragma unroll
-                    for (int q = 0; q < kRowBufs; q++) {
-                        const int leave = t0 + bf + q, enter = leave + 2 * P + 1;
-                        const int kl = rank_at(leave, c), ke = enter < RH ? rank_at(enter, c) : -1;
-                        if (kl != ke) {
-                            if (kl >= 0) col[kl * CSTR]--;
-                            if (ke >= 0) col[ke * CSTR]++;
-                        }
-                    }
+            const int enter = t0 + 2 * P + 1;
+            for (int c = tid; c < RW; c += kCvThreads) {
+                const int kl = rank_at(t0, c), ke = enter < RH ? rank_at(enter, c) : -1;
+                if (kl != ke) {
+                    if (kl >= 0) colc[kl * CSTR + c]--;
+                    if (ke >= 0) colc[ke * CSTR + c]++;
                 }
+            }
         };
         // window counts of chunk row i, for the m tiles the row reads, over N k-steps (N the same for the warp)
-        auto window_counts_n = [&](auto n_ksteps, int i, uint32_t need, int bf) {
+        auto window_counts_n = [&](auto n_ksteps, int i, uint32_t need) {
             constexpr int N = decltype(n_ksteps)::value;
             const bool m0 = (need & 0xFFFFu) != 0, m1 = (need >> 16) != 0;
             int acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-            const uint32_t at0 = cbase + (uint32_t)(bf * kCvBins * CSTR) + lrow * CSTR + 32 * ks_lo + lcol;
+            const uint32_t at0 = cbase + lrow * CSTR + 32 * ks_lo + lcol;
 #pragma unroll
             for (int kk = 0; kk < N; kk++) {
                 uint32_t a0, a1, a2, a3;
@@ -509,14 +509,14 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
                 *(uint32_t *)(wrow + 24 * kCvWS) = __byte_perm((uint32_t)acc[1][2], (uint32_t)acc[1][3], 0x5410);
             }
         };
-        auto window_counts = [&](int i, uint32_t need, int bf) {
+        auto window_counts = [&](int i, uint32_t need) {
             switch (ks_hi - ks_lo) {  // the same for the whole warp
-            case 0: window_counts_n(std::integral_constant<int, 1>{}, i, need, bf); break;
-            case 1: window_counts_n(std::integral_constant<int, 2>{}, i, need, bf); break;
-            case 2: window_counts_n(std::integral_constant<int, 3>{}, i, need, bf); break;
-            case 3: window_counts_n(std::integral_constant<int, 4>{}, i, need, bf); break;
-            case 4: window_counts_n(std::integral_constant<int, 5>{}, i, need, bf); break;
-            default: window_counts_n(std::integral_constant<int, 6>{}, i, need, bf); break;
+            case 0: window_counts_n(std::integral_constant<int, 1>{}, i, need); break;
+            case 1: window_counts_n(std::integral_constant<int, 2>{}, i, need); break;
+            case 2: window_counts_n(std::integral_constant<int, 3>{}, i, need); break;
+            case 3: window_counts_n(std::integral_constant<int, 4>{}, i, need); break;
+            case 4: window_counts_n(std::integral_constant<int, 5>{}, i, need); break;
+            default: window_counts_n(std::integral_constant<int, 6>{}, i, need); break;
             }
         };
         const int ci = tid / TX, cc = tid % TX;  // this thread's pixel in a chunk
@@ -525,18 +525,18 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
             bool chunk_any = false;
             for (int i = 0; i < n_rows; i++) {
                 const int r = r0 + i;
-                if (i > 0 && i % kRowBufs == 0 && pass_any) {  // the buffers on to rows r .. r + kRowBufs - 1
-                    __syncthreads();  // every warp has read the counts of the rows before
-                    slide(r - kRowBufs);
+                if (i > 0 && pass_any) {  // the counts on to row r
+                    __syncthreads();  // every warp has read the counts of the row before
+                    slide(r - 1);
                     __syncthreads();
                 }
                 const uint32_t need = rowneed[r];
                 chunk_any |= need != 0;
-                if (need) window_counts(i, need, r % kRowBufs);
+                if (need) window_counts(i, need);
             }
             __syncthreads();
-            // the buffers move past this chunk beside its c-values (they touch no buffer the c-values read)
-            if (pass_any && r0 + kCvChunk < rows) slide(r0 + kCvChunk - kRowBufs);
+            // the counts move past this chunk beside its c-values (they touch nothing the c-values read)
+            if (pass_any && r0 + kCvChunk < rows) slide(r0 + kCvChunk - 1);
             if (!chunk_any) {
                 __syncthreads();
                 continue;
