@@ -14,7 +14,7 @@
 //     sit in shared memory as a 32 x region-width byte matrix and slide down the rows (the leaving and entering row's
 //     rank per column); on rows whose pixels read the pass's ranks, the window counts of the 64 tile columns are one
 //     exact integer matrix product on the tensor cores (mma.sync u8, counts x a band of ones 2 pad + 1 wide), each warp
-//     making 8 columns. Every 4 rows all 8 warps compute the 256 c-values from those counts.
+//     making 16 ranks x 16 columns. Every 4 rows all 8 warps compute the 256 c-values from those counts.
 // Positive c-values are summed exactly (they are multiples of 2^-24) and counted, and each block appends them to its
 // scale's list (for the top-k selection) through a bounded shared-memory buffer; nothing per pixel is written unless
 // the caller asks for the c-value planes.
@@ -43,8 +43,8 @@ __host__ __device__ constexpr int cv_cs(int tx, int pad) { return (cv_rw(tx, pad
 // ldmatrix phase reads fall on different banks)
 __host__ __device__ constexpr int cv_nk(int tx, int pad) { return (cv_rw(tx, pad) + 31) >> 5; }
 __host__ __device__ constexpr int cv_cstr(int tx, int pad) { return 32 * cv_nk(tx, pad) + 16; }
-// k-steps one warp's window reaches (its 8 output columns and 2 pad more), at most
-constexpr int kCvMaxK = (8 + 2 * kMaxPad + 31) / 32 + 1;
+// k-steps one warp's window counts reach (output columns xb .. xb + 23 with xb % 32 <= 8, and 2 pad more), at most
+constexpr int kCvMaxK = (8 + 23 + 2 * kMaxPad) / 32 + 1;
 __host__ __device__ constexpr int cv_ws(int tx) { return tx + 2; }  // window-count row (u16): an odd number of words
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
@@ -393,21 +393,23 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
     uint16_t *wc16 = (uint16_t *)(smem + L.wcount);      // [chunk row][rank][kCvWS]: window counts
     const int NK = cv_nk(TX, P), CSTR = cv_cstr(TX, P);
     const int g = lane >> 2, t = lane & 3;
-    const int ks_lo = (8 * warp) >> 5, ks_hi = min(NK - 1, (8 * warp + 7 + 2 * P) >> 5);
-    uint32_t bfrag[kCvMaxK][2];  // this lane's B fragments: rows (region columns) 32 (ks_lo + kk) + 16 r + 4 t + i,
-                                 // column 8 w + g
+    // warp w makes the window counts of one m tile (ranks 16 mt .. 16 mt + 15) at two n tiles 16 columns apart,
+    // output columns xb .. xb + 7 and xb + 16 .. xb + 23: the column counts it loads serve 16 columns, and the second n
+    // tile's band of ones is the first's one half k-step on, so both share one set of B fragments
+    constexpr int kGroups = kWarps / 2;
+    const int mt = warp / kGroups, grp = warp % kGroups, xb = 32 * (grp >> 1) + 8 * (grp & 1);
+    const int ks_lo = xb >> 5, ks_hi = min(NK - 1, (xb + 23 + 2 * P) >> 5);
+    uint32_t bfrag[2 * kCvMaxK + 1];  // bfrag[h]: rows (region columns) 32 ks_lo + 16 (h - 1) + 4 t + i, column xb + g
 #pragma unroll
-    for (int kk = 0; kk < kCvMaxK; kk++)
+    for (int hh = 0; hh < 2 * kCvMaxK + 1; hh++) {
+        uint32_t word = 0;
 #pragma unroll
-        for (int r = 0; r < 2; r++) {
-            uint32_t word = 0;
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const int j = 32 * (ks_lo + kk) + 16 * r + 4 * t + i, x = 8 * warp + g;
-                word |= (uint32_t)(j >= x && j <= x + 2 * P) << (8 * i);
-            }
-            bfrag[kk][r] = word;
+        for (int i = 0; i < 4; i++) {
+            const int j = 32 * ks_lo + 16 * (hh - 1) + 4 * t + i, x = xb + g;
+            word |= (uint32_t)(j >= x && j <= x + 2 * P) << (8 * i);
         }
+        bfrag[hh] = word;
+    }
     const uint32_t cbase = (uint32_t)__cvta_generic_to_shared(colc);
     const int lrow = ((lane >> 3) & 1) * 8 + (lane & 7), lcol = (lane >> 4) * 16;  // this lane's ldmatrix row address
     for (int b0 = 0;;) {
@@ -483,30 +485,23 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
         // window counts of chunk row i, for the m tiles the row reads, over N k-steps (N the same for the warp)
         auto window_counts_n = [&](auto n_ksteps, int i, uint32_t need) {
             constexpr int N = decltype(n_ksteps)::value;
-            const bool m0 = (need & 0xFFFFu) != 0, m1 = (need >> 16) != 0;
+            if (((need >> (16 * mt)) & 0xFFFFu) == 0) return;  // no pixel of the row reads this m tile's ranks
             int acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-            const uint32_t at0 = cbase + lrow * CSTR + 32 * ks_lo + lcol;
+            const uint32_t at0 = cbase + (16 * mt + lrow) * CSTR + 32 * ks_lo + lcol;
 #pragma unroll
             for (int kk = 0; kk < N; kk++) {
                 uint32_t a0, a1, a2, a3;
-                if (m0) {
-                    ldmatrix_x4(at0 + 32 * kk, a0, a1, a2, a3);
-                    mma_u8(acc[0], a0, a1, a2, a3, bfrag[kk][0], bfrag[kk][1]);
-                }
-                if (m1) {
-                    ldmatrix_x4(at0 + 16 * CSTR + 32 * kk, a0, a1, a2, a3);
-                    mma_u8(acc[1], a0, a1, a2, a3, bfrag[kk][0], bfrag[kk][1]);
-                }
+                ldmatrix_x4(at0 + 32 * kk, a0, a1, a2, a3);
+                mma_u8(acc[0], a0, a1, a2, a3, bfrag[2 * kk + 1], bfrag[2 * kk + 2]);
+                mma_u8(acc[1], a0, a1, a2, a3, bfrag[2 * kk], bfrag[2 * kk + 1]);
             }
-            // rank 16 m + g (+ 8) at columns 8 w + 2 t and + 1 (counts below 2^16: the low halves of the accumulators)
-            uint16_t *wrow = wc16 + (size_t)i * kCvBins * kCvWS + g * kCvWS + 8 * warp + 2 * t;
-            if (m0) {
-                *(uint32_t *)wrow = __byte_perm((uint32_t)acc[0][0], (uint32_t)acc[0][1], 0x5410);
-                *(uint32_t *)(wrow + 8 * kCvWS) = __byte_perm((uint32_t)acc[0][2], (uint32_t)acc[0][3], 0x5410);
-            }
-            if (m1) {
-                *(uint32_t *)(wrow + 16 * kCvWS) = __byte_perm((uint32_t)acc[1][0], (uint32_t)acc[1][1], 0x5410);
-                *(uint32_t *)(wrow + 24 * kCvWS) = __byte_perm((uint32_t)acc[1][2], (uint32_t)acc[1][3], 0x5410);
+            // rank 16 mt + g (+ 8) at columns xb + 2 t and + 1, and 16 on (counts below 2^16: the low halves of the
+            // accumulators)
+            uint16_t *wrow = wc16 + (size_t)i * kCvBins * kCvWS + (16 * mt + g) * kCvWS + xb + 2 * t;
+#pragma unroll
+            for (int n = 0; n < 2; n++) {
+                *(uint32_t *)(wrow + 16 * n) = __byte_perm((uint32_t)acc[n][0], (uint32_t)acc[n][1], 0x5410);
+                *(uint32_t *)(wrow + 16 * n + 8 * kCvWS) = __byte_perm((uint32_t)acc[n][2], (uint32_t)acc[n][3], 0x5410);
             }
         };
         auto window_counts = [&](int i, uint32_t need) {
@@ -515,8 +510,7 @@ __global__ void __launch_bounds__(4 * TX, 256 / TX) cvalues_kernel(const __grid_
             case 1: window_counts_n(std::integral_constant<int, 2>{}, i, need); break;
             case 2: window_counts_n(std::integral_constant<int, 3>{}, i, need); break;
             case 3: window_counts_n(std::integral_constant<int, 4>{}, i, need); break;
-            case 4: window_counts_n(std::integral_constant<int, 5>{}, i, need); break;
-            default: window_counts_n(std::integral_constant<int, 6>{}, i, need); break;
+            default: window_counts_n(std::integral_constant<int, 5>{}, i, need); break;
             }
         };
         const int ci = tid / TX, cc = tid % TX;  // this thread's pixel in a chunk
