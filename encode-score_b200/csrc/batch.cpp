@@ -167,7 +167,7 @@ void init_source(Source &S, const es_batch_source &d)
         S.persist[i].reset(std::max<size_t>(1, win * kPersist * S.nenc));
         S.sums[i].reset((size_t)3 * S.nenc + 3 * (S.nenc + 1));
         S.figs[i].reset(S.nenc);
-        S.bins[i].reset(std::max<size_t>(1, win * kBinArrays * S.nenc));
+        S.bins[i].reset(win * kBinArrays * S.nenc + 4 * (size_t)S.nenc);  // the arrays, then 2 counts per encode
         S.h_sums[i].reset(S.sums[i].count);
         S.h_figs[i].reset(S.nenc);
         S.h_bins[i].reset(S.bins[i].count);
@@ -533,6 +533,7 @@ void record_texture(es_batch &b, long f, cudaStream_t s, cudaStream_t s2)
                 cj.persist[e] = texture ? qj.out[e] : nullptr;
                 cj.fig[e] = S.figs[at].ptr + e;
                 cj.bins[e] = S.bins[at].ptr + (size_t)e * kBinArrays * S.windows;
+                cj.bin_n[e] = bin_counts(S.bins[at].ptr, S.windows, S.nenc) + 2 * e;
             }
             cj.centre_mask = S.masks.ptr + (size_t)((f + kEncRing - kRadius) % kEncRing) * S.windows;
             cj.mask = S.masks.ptr + (size_t)(f % kEncRing) * S.windows;
@@ -557,6 +558,9 @@ void record_texture(es_batch &b, long f, cudaStream_t s, cudaStream_t s2)
     if (cb.njobs) {
         if (fork) cuda_check(cudaStreamWaitEvent(s, b.join_thr.e, 0), "event");
         else cuda_check(launch_collect_threshold(cb, s), "batch structure threshold");
+        for (auto &sp : b.sources)
+            if (sp->windows > 0)
+                cuda_check(cudaMemsetAsync(bin_counts(sp->bins[at].ptr, sp->windows, sp->nenc), 0, 8 * (size_t)sp->nenc, s), "clearing");
         cuda_check(launch_collect_sums(cb, s), "batch collecting figures");
     }
     for (auto &sp : b.sources) {
@@ -770,7 +774,8 @@ int es_batch_collect(es_batch *b, long f, const double *cached_source_cambi, es_
                 const double banding = sc[(size_t)b->encode_picture(s, e) * (1 + kScales)];
                 const es_frame_result res = collect_encode(
                     EncodeFigures{banding, source_banding, sse + 3 * e, scol, color + 3 * e, S.n, S.pd, S.windows,
-                                  &S.h_figs[at].ptr[e], S.h_bins[at].ptr + (size_t)e * kBinArrays * S.windows, texture},
+                                  &S.h_figs[at].ptr[e], S.h_bins[at].ptr + (size_t)e * kBinArrays * S.windows,
+                                  bin_counts(S.h_bins[at].ptr, S.windows, S.nenc) + 2 * e, texture},
                     frame_acc ? frame_acc[k] : nullptr, centre_acc ? centre_acc[k] : nullptr);
                 if (out) out[k] = res;
             }

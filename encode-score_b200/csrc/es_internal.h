@@ -150,9 +150,16 @@ struct EncodeFigures {
     size_t n;                                // luma samples
     int pd, windows;
     const FrameFigures *fig;
-    const uint16_t *bins;                    // 6 arrays of `windows` bins
+    const uint16_t *bins;                    // 6 arrays of up to `windows` bins, the counting ones from the start
+    const unsigned *bin_n;                   // bins in each of the first five arrays, in the lasting array
     bool texture;                            // the lasting texture of frame f - 6 is in `fig` / `bins`
 };
+// The two bin counts of encode e (of nenc) follow the 6 bin arrays of every encode in one buffer.
+template <typename T>
+inline unsigned *bin_counts(T *bins, int windows, int nenc)
+{
+    return (unsigned *)(bins + (size_t)windows * 6 * nenc);
+}
 // src/main.cpp:584-641 for one encode: adds the figures into frame_acc and, with texture, the lasting texture into
 // centre_acc (either may be null), and returns the frame's result.
 es_frame_result collect_encode(const EncodeFigures &in, es_accum *frame_acc, es_accum *centre_acc);

@@ -292,7 +292,10 @@ struct CollectJob {
     const uint8_t *centre_mask;         // structure mask of the centre frame
     uint8_t *mask;                      // out: structure mask of this frame
     FrameFigures *fig[kMaxEncodes];
-    uint16_t *bins[kMaxEncodes];        // out: 6 arrays of `windows` bins (amount 0-2, matching 0-1, lasting)
+    uint16_t *bins[kMaxEncodes];        // out: 6 arrays of up to `windows` bins (amount 0-2, matching 0-1, lasting),
+                                        // only those that count, from the start of each array in no fixed order
+    unsigned *bin_n[kMaxEncodes];       // out (cleared by the caller): [0] bins in each of the first five arrays
+                                        // (the structure windows), [1] in the lasting array
     float *threshold;                   // scratch: the frame's structure threshold
     double *partials;                   // scratch: [nenc][collect_blocks(windows)][kCollectSums]
     int nenc, windows;

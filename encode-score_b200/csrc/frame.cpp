@@ -200,6 +200,7 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
         cj.persist[e] = texture ? qj.out[e] : nullptr;
         cj.fig[e] = fr->figs[at].ptr + e;
         cj.bins[e] = fr->bins[at].ptr + (size_t)e * kBinArrays * fr->windows;
+        cj.bin_n[e] = bin_counts(fr->bins[at].ptr, fr->windows, fr->nenc) + 2 * e;
     }
     cj.centre_mask = fr->masks.ptr + (size_t)((f + kEncRing - kRadius) % kEncRing) * fr->windows;
     cj.mask = fr->masks.ptr + (size_t)(f % kEncRing) * fr->windows;
@@ -211,6 +212,7 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
         CollectBatch cb{};
         cb.job[0] = cj;
         cb.njobs = 1;
+        cuda_check(cudaMemsetAsync(cj.bin_n[0], 0, 8 * (size_t)fr->nenc, s), "clearing");
         cuda_check(launch_collect(cb, s), "collecting figures");
     }
 
@@ -226,15 +228,11 @@ void queue_frame(es_frame *fr, long f, const es_frame_view *source, int sx, int 
     fr->queued[at] = f;
 }
 
-void add_bins(es_histogram &hist, const uint16_t *bins, int n)
+// the n bins the collect kernel wrote (only those that count)
+void add_bins(es_histogram &hist, const uint16_t *bins, unsigned n)
 {
-    for (int i = 0; i < n; i++) {
-        const uint16_t b = bins[i];
-        if (b != kNone) {
-            hist.bins[b]++;
-            hist.n++;
-        }
-    }
+    for (unsigned i = 0; i < n; i++) hist.bins[bins[i]]++;
+    hist.n += n;
 }
 
 }  // namespace
@@ -281,15 +279,15 @@ es_frame_result es::collect_encode(const EncodeFigures &in, es_accum *frame_acc,
                 acc.sh_st_r[k] += fg.st_r[k];
                 acc.sh_st_x[k] += fg.sh_st_x[k];
             }
-            for (int k = 0; k < 3; k++) add_bins(acc.amount[k], in.bins + (size_t)k * in.windows, in.windows);
-            for (int k = 0; k < 2; k++) add_bins(acc.matching[k], in.bins + (size_t)(3 + k) * in.windows, in.windows);
+            for (int k = 0; k < 3; k++) add_bins(acc.amount[k], in.bins + (size_t)k * in.windows, in.bin_n[0]);
+            for (int k = 0; k < 2; k++) add_bins(acc.matching[k], in.bins + (size_t)(3 + k) * in.windows, in.bin_n[0]);
         }
     }
     if (in.texture && in.windows > 0 && centre_acc) {
         es_accum &cacc = *centre_acc;
         cacc.own += fg.own;
         cacc.mine += fg.mine;
-        add_bins(cacc.lasting, in.bins + (size_t)5 * in.windows, in.windows);
+        add_bins(cacc.lasting, in.bins + (size_t)5 * in.windows, in.bin_n[1]);
     }
     return res;
 }
@@ -331,7 +329,7 @@ int es_frame_create(const es_module *m, int w, int h, int pd, int n_encodes, es_
             fr->persist[i].reset(std::max<size_t>(1, win * kPersist * n_encodes));
             fr->sums[i].reset((size_t)3 * n_encodes + 3 * (n_encodes + 1));
             fr->figs[i].reset(n_encodes);
-            fr->bins[i].reset(std::max<size_t>(1, win * kBinArrays * n_encodes));
+            fr->bins[i].reset(win * kBinArrays * n_encodes + 4 * (size_t)n_encodes);  // the arrays, then 2 counts per encode
             fr->h_sums[i].reset(fr->sums[i].count);
             fr->h_figs[i].reset(n_encodes);
             fr->h_bins[i].reset(fr->bins[i].count);
@@ -400,7 +398,8 @@ int es_frame_collect(es_frame *fr, long f, const double *cached_source_cambi, es
             if (r) throw Error(r, es_last_error());
             const es_frame_result res = collect_encode(
                 EncodeFigures{banding, source_banding, sse + 3 * e, scol, color + 3 * e, fr->n, fr->pd, fr->windows,
-                              &fr->h_figs[at].ptr[e], fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows, texture},
+                              &fr->h_figs[at].ptr[e], fr->h_bins[at].ptr + (size_t)e * kBinArrays * fr->windows,
+                              bin_counts(fr->h_bins[at].ptr, fr->windows, fr->nenc) + 2 * e, texture},
                 frame_acc ? frame_acc[e] : nullptr, centre_acc ? centre_acc[e] : nullptr);
             if (out) out[e] = res;
         }

@@ -712,37 +712,34 @@ __global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_const
     double v[kCollectSums];
 #pragma unroll
     for (int k = 0; k < kCollectSums; k++) v[k] = 0.0;
+    uint16_t bin[6];  // amount 0-2, matching 0-1 (valid on structure windows), lasting (valid where v[19] is 1)
+    bool structure = false, lasting = false;
     if (i < n) {
         const float q = *J.threshold;
         const float *s = J.stats[e] + (size_t)i * 8;
-        uint16_t *bins = J.bins[e];
         const bool m = s[6] >= q && s[6] > 0.0f;
+        structure = m;
         const double er[3] = {(double)s[0], (double)s[1], (double)s[6]}, ed[3] = {(double)s[2], (double)s[3], (double)s[7]};
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             v[k] = er[k];
             v[3 + k] = ed[k];
-            uint16_t bin = kNone;
             if (m) {
                 v[6 + k] = er[k];
                 v[9 + k] = ed[k];
-                bin = hist_bin(__dmul_rn(100.0, __dsqrt_rn(__ddiv_rn(ed[k], fmax(er[k], 1e-9)))));
+                bin[k] = hist_bin(__dmul_rn(100.0, __dsqrt_rn(__ddiv_rn(ed[k], fmax(er[k], 1e-9)))));
             }
-            bins[(size_t)k * n + i] = bin;
         }
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const double x = (double)s[4 + k];
             v[12 + k] = x;
-            uint16_t bin = kNone;
             if (m) {
                 v[14 + k] = x;
-                bin = hist_bin(__ddiv_rn(__dmul_rn(100.0, x), fmax(er[k], 1e-9)));
+                bin[3 + k] = hist_bin(__ddiv_rn(__dmul_rn(100.0, x), fmax(er[k], 1e-9)));
             }
-            bins[(size_t)(3 + k) * n + i] = bin;
         }
         v[18] = m ? 1.0 : 0.0;
-        uint16_t lbin = kNone;
         if (J.persist[e]) {
             const float *ps = J.persist[e] + (size_t)i * 5;
             const double agree = __ddiv_rn((double)ps[2], __dsqrt_rn(fmax(__dmul_rn((double)ps[3], (double)ps[4]), 1e-9)));
@@ -750,10 +747,28 @@ __global__ void __launch_bounds__(kCW) collect_windows_kernel(const __grid_const
                 v[16] = (double)ps[0];
                 v[17] = (double)ps[1];
                 v[19] = 1.0;
-                lbin = hist_bin(__ddiv_rn(__dmul_rn(100.0, (double)ps[1]), (double)ps[0]));
+                lasting = true;
+                bin[5] = hist_bin(__ddiv_rn(__dmul_rn(100.0, (double)ps[1]), (double)ps[0]));
             }
         }
-        bins[(size_t)5 * n + i] = lbin;
+    }
+    // the bins that count, compacted (a histogram does not depend on their order): the five structure arrays share
+    // one position per window, the lasting array has its own; a warp reserves its places with one atomic each
+    {
+        uint16_t *bins = J.bins[e];
+        const unsigned below = (1u << lane) - 1u;
+        const unsigned sm = __ballot_sync(0xffffffffu, structure), lm = __ballot_sync(0xffffffffu, lasting);
+        unsigned sb = 0, lb = 0;
+        if (sm && lane == 0) sb = atomicAdd(&J.bin_n[e][0], (unsigned)__popc(sm));
+        if (lm && lane == 0) lb = atomicAdd(&J.bin_n[e][1], (unsigned)__popc(lm));
+        sb = __shfl_sync(0xffffffffu, sb, 0);
+        lb = __shfl_sync(0xffffffffu, lb, 0);
+        if (structure) {
+            const unsigned at = sb + __popc(sm & below);
+#pragma unroll
+            for (int k = 0; k < 5; k++) bins[(size_t)k * n + at] = bin[k];
+        }
+        if (lasting) bins[(size_t)5 * n + lb + __popc(lm & below)] = bin[5];
     }
 #pragma unroll
     for (int k = 0; k < kCollectSums; k++) {
