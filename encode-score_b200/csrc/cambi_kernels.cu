@@ -170,10 +170,11 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
         return (m2 & edge) | (mode3x2(left, m2, right) & ~edge);
     };
     const bool feat = J.feat != nullptr;  // the same for the whole block
-    const uint32_t idx2 = (uint32_t)J.mask_index * 0x10001u;
+    // mask bit 15 of each half where the count exceeds mask_index: counts <= 49 and 0x7FFF - mask_index added per
+    // half reach bit 15 exactly then, without a carry into the other half
+    const uint32_t idx2 = (0x7FFFu - (uint32_t)J.mask_index) * 0x10001u;
     const bool vec_store = (w & 1) == 0 && (((uintptr_t)J.word) & 3) == 0;
     const bool need_range = b.need_span >= 0;
-    const uint32_t lo2 = (uint32_t)b.need_lo * 0x10001u, span2 = (uint32_t)(b.need_span < 0 ? 0 : b.need_span) * 0x10001u;
     const int yb = y0 + 8 * g;
     uint32_t hv[14];  // h7 of flat rows yb-3 .. yb+10 (flat row index y - (y0-5))
     uint32_t cnt = 0;
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
         const uint32_t m2 = hmode(y + 1);
         uint32_t v2 = mode3x2(m0, m1, m2);
         if (y == 0 || y == h - 1) v2 = pair(y - ys, c);
-        const uint32_t mk = __vcmpgtu2(cnt, idx2) & 0x80008000u;
+        const uint32_t mk = (cnt + idx2) & 0x80008000u;
         const uint32_t word2 = v2 | mk;
         if (y < h) {
             if (vec_store && x + 1 < w) {
@@ -211,7 +212,9 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
                 fn += (ok & 1u) + (ok >> 31);
                 uint32_t hit;
                 if (need_range) {
-                    hit = __vcmpleu2(__vsub2(v2, lo2), span2) & __vcmpne2(mk, 0u) & ok;
+                    // a masked value in lo .. lo + span, per half (the unsigned difference wraps below lo)
+                    hit = (((v2 & 0xFFFFu) - b.need_lo) <= (unsigned)b.need_span && (mk & 0x8000u) && (ok & 1u)) ||
+                          (((v2 >> 16) - b.need_lo) <= (unsigned)b.need_span && (mk >> 31) && (ok >> 31));
                 } else {
                     hit = 0;
                     for (int k = 0; k < 2; k++) {

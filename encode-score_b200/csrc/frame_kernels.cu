@@ -400,8 +400,10 @@ __global__ void __launch_bounds__(256, 3) persist_kernel(const __grid_constant__
                 v[n].y <<= J.up;
             }
             const uint2 oo = __ldg((const uint2 *)(J.o_old + k)), eo = __ldg((const uint2 *)(J.e_old + k));
-            const uint2 e = make_uint2(__vadd2(__vsub2(oo.x, v[2].x), v[3].x), __vadd2(__vsub2(oo.y, v[2].y), v[3].y));
-            const uint2 o = make_uint2(__vadd2(__vsub2(eo.x, v[0].x), v[1].x), __vadd2(__vsub2(eo.y, v[0].y), v[1].y));
+            // no element leaves 0 .. 65535 (the leaving frame is part of the old sum), so 32-bit arithmetic on the
+            // pairs carries and borrows nothing between the halves
+            const uint2 e = make_uint2(oo.x - v[2].x + v[3].x, oo.y - v[2].y + v[3].y);
+            const uint2 o = make_uint2(eo.x - v[0].x + v[1].x, eo.y - v[0].y + v[1].y);
             *(uint2 *)&sm.y[r][4 * q] = e;
             *(uint2 *)&o_reg[r][4 * q] = o;
             if (r >= kM && r < kM + kWT && yu < h && q >= 1 && q <= 16) {
