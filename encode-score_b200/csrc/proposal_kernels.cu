@@ -8,9 +8,10 @@
 //  * training kernels (FP32, SIMT): valid 3 x 3 convolutions forward and backward on crops, the tile loss and Adam;
 //    weights are used rounded to bfloat16;
 //  * predict_kernel: one 128-thread block per scale-0 tile runs all four layers on the tile's 24 x 24 feature window
-//    in shared memory; the two 16 -> 16 layers are bfloat16 tensor-core products (mma.sync m16n8k16, FP32
-//    accumulation, A fragments by ldmatrix from [pixel][16 channel] planes), the first and last layers FP32 SIMT;
-//    tiles with no pixel that needs a c-value get -inf;
+//    in shared memory; the two 16 -> 16 layers are implicit-GEMM products on the fifth-generation tensor cores
+//    (tcgen05.mma, bfloat16 operands from shared-memory descriptors, FP32 accumulators in tensor memory, read back
+//    with tcgen05.ld), the first and last layers bfloat16 mma.sync products; tiles with no pixel that needs a c-value
+//    get -inf;
 //  * propose_kernel / audit_kernel: the per-step tile lists and the audit's estimate, all on the device.
 #include <cuda_bf16.h>
 
@@ -270,13 +271,27 @@ __global__ void net_adam_kernel(float *P, float *R, const float *G, float *M, fl
 // Inference: one block of 128 threads per scale-0 tile, all four layers in shared memory.
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kPT = 128;
-constexpr int kPredBlocks = 148 * 5;  // persistent grid: 5 blocks of 34 KB per SM
+constexpr int kPredBlocks = 148 * 5;  // persistent grid: 5 blocks of 42 KB (and 64 tensor-memory columns) per SM
+// Layers 1 and 2 are products of 128 output rows on the tensor cores, over the input's raster: output row oy iw + ox
+// (iw = the input's width), so a layer computes ceil(ow iw / 128) blocks of rows and reads the input up to row
+// 128 blocks + 2 iw + 2; its planes have that many rows (zero past the picture, computed and dropped).
+constexpr int kL1Blocks = (20 * 22 + 127) / 128, kL1Rows = 128 * kL1Blocks + 2 * 22 + 8;  // 4 blocks, 564 rows
+constexpr int kL2Blocks = (18 * 20 + 127) / 128, kL2Rows = 128 * kL2Blocks + 2 * 20 + 8;  // 3 blocks, 432 rows
+constexpr int kTmemCols = 16 * kL1Blocks;                                                  // 64
 struct PredSmem {
-    uint32_t f[kFeatTile * kFeatTile][2];         // features per pixel: (head, remainder) bfloat16 pairs of channels 0, 1
     float b0[16], w3[145];                        // layer 0's biases; layer 3's weights then bias (bfloat16 values)
     float b12[2][16];
-    __align__(16) uint32_t a1[22 * 22 * 8];       // layer-0 output, [pixel][16 channels] bfloat16; later layer 2's
-    __align__(16) uint32_t a2[20 * 20 * 8];       // layer-1 output
+    // layer 1's input (layer 0's 22 x 22 output): two planes of kL1Rows 16-byte rows, channels 8 h .. 8 h + 7 of pixel p
+    // in plane h, row p; later layer 2's 18 x 18 output in the head's layout ([pixel][16 channels], phys_half)
+    __align__(128) uint32_t a1[2 * kL1Rows * 4];
+    // layer 2's input (layer 1's 20 x 20 output), the same plane form; until layer 1 writes it, its first 4.6 KB hold
+    // the tile's features (per pixel the (head, remainder) bfloat16 pairs of channels 0, 1), rows the planes' padding
+    // does not reach
+    __align__(128) uint32_t a2[2 * kL2Rows * 4];
+    // the B operands of layers 1 and 2: [layer][tap][K half][output channel n][4 words of 2 input channels]
+    __align__(128) uint32_t wt[2 * 9 * 128];
+    uint64_t bar;   // the products' completion barrier
+    uint32_t tmem;  // the block's tensor-memory columns
     float part[kPT / 32];
 };
 
@@ -298,51 +313,115 @@ __device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t &r0, uint32_
 // so the 8 rows an ldmatrix phase reads (consecutive pixels) fall on different banks.
 __device__ __forceinline__ int phys_half(int p, int half) { return half ^ ((p >> 2) & 1); }
 
-// One 16 -> 16 layer: input plane `in` (iw x iw pixels of 16 bfloat16 channels, 32 bytes each), output plane `out`
-// (ow x ow, ow = iw - 2), bias, ReLU, bfloat16. Warp w takes m tiles w, w + 4, ...: 16 output pixels each, numbered
-// row by row; rows past the last pixel read a valid pixel and are not stored. frags: this layer's B fragments.
-__device__ __forceinline__ void mma_layer(const uint32_t *in, int iw, uint32_t *out, int ow, const uint32_t *frags,
-                                          const float *bias)
+// ---- fifth-generation tensor cores (tcgen05): products in tensor memory from shared-memory operands ----------------
+// A shared-memory matrix descriptor without swizzle, K-major: rows of 16 bytes (8 bfloat16 of K) contiguous, groups of
+// 8 rows `sbo` bytes apart, the two 8-wide halves of K `lbo` bytes apart; version 1 (sm_100) in bits 46-47.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int npx = ow * ow, tiles = (npx + 15) / 16;
-    const int g = lane >> 2, t = lane & 3;
-    const int mrow = ((lane >> 3) & 1) * 8 + (lane & 7), khalf = lane >> 4;  // this lane's ldmatrix row and k half
-    const uint32_t base = (uint32_t)__cvta_generic_to_shared(in);
-    uint32_t bf[9][4];  // this lane's B fragments of every tap, (n tile, register), kept across the m tiles
-#pragma unroll
-    for (int k = 0; k < 9; k++)
-#pragma unroll
-        for (int r = 0; r < 4; r++) bf[k][r] = frags[k * 4 * 32 + r * 32 + lane];
-    for (int mt = warp; mt < tiles; mt += kPT / 32) {
-        const int p = min(16 * mt + mrow, npx - 1);
-        const int oy = p / ow, ox = p - oy * ow;
-        float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-#pragma unroll
-        for (int k = 0; k < 9; k++) {
-            const int q = (oy + k / 3) * iw + ox + k % 3;
-            uint32_t a0, a1, a2, a3;
-            ldmatrix_x4(base + q * 32 + phys_half(q, khalf) * 16, a0, a1, a2, a3);
-            mma_bf16(c[0], a0, a1, a2, a3, bf[k][0], bf[k][1]);
-            mma_bf16(c[1], a0, a1, a2, a3, bf[k][2], bf[k][3]);
-        }
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const int ch = 8 * j + 2 * t;
-#pragma unroll
-            for (int hrow = 0; hrow < 2; hrow++) {
-                const int pr = 16 * mt + g + 8 * hrow;
-                if (pr >= npx) continue;
-                const float v0 = fmaxf(c[j][2 * hrow] + bias[ch], 0.0f), v1 = fmaxf(c[j][2 * hrow + 1] + bias[ch + 1], 0.0f);
-                out[pr * 8 + phys_half(pr, j) * 4 + t] = pack_bf16(v0, v1);  // channels 8 j + 2 t, + 1
-            }
-        }
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+           ((uint64_t)1 << 46);
+}
+// The instruction descriptor of a bfloat16 product with FP32 accumulation, both operands K-major, M = 128, N = 16.
+constexpr uint32_t kUmmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+// D (tensor memory, 128 lanes x 16 FP32 columns) = A (128 x 16) x B (16 x 16)^T, plus D when `accumulate`.
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                 ::"r"(tmem_d), "l"(a), "l"(b), "r"(kUmmaIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+// The products issued so far arrive on the barrier when they are done.
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"((uint32_t)__cvta_generic_to_shared(bar)) : "memory");
+}
+// Waits, a bounded number of times, for the barrier's phase `parity` to complete; false if it never did.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    for (int it = 0; it < (1 << 20); it++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
     }
+    return false;
+}
+// This warp's 32 lanes of tensor memory (its quarter of the 128), 16 columns from `taddr`, as FP32; the values may be
+// used only after a tcgen05.wait::ld.
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, float (&v)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]), "=f"(v[8]),
+                   "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Generic-proxy writes to shared memory made visible to the tensor cores' reads (before a barrier and the products).
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// One 16 -> 16 layer (bias, ReLU, bfloat16) on the tensor cores with tcgen05. The input is layer planes of `rows`
+// 16-byte rows (channels 8 h .. 8 h + 7 of pixel p in plane h, row p; pixels row by row, IW wide, zero past the
+// picture). Output row q = oy IW + ox of the product is output pixel (oy, ox): tap (dy, dx) multiplies the input from
+// row q + dy IW + dx, so each block of 128 output rows is 9 products (one per tap, accumulated in 16 tensor-memory
+// columns) whose A operand is the planes from the tap's row on; B is the tap's 16 x 16 weights. Thread 0 issues them,
+// every thread then reads its own row of each block (warp w: lanes 32 w .. 32 w + 31) and hands the output pixels
+// (ox < OW, oy < OW) with their 8 packed channel pairs to `store`. False if the products never completed.
+template <int IW, int OW, int BLOCKS, typename Store>
+__device__ __forceinline__ bool umma_layer(PredSmem &sm, const uint32_t *in, int rows, int layer, uint32_t &phase,
+                                           const float *bias, Store store)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    fence_async_smem();  // this thread's writes of the input (and of the weights) reach the tensor cores' reads
+    tc_fence_before();   // and its reads of tensor memory (the previous layer's) are done before the barrier
+    __syncthreads();
+    tc_fence_after();
+    // lane 0 of warp m issues block m's nine products and commits them (the barrier expects one arrival per warp);
+    // a descriptor's start field counts 16 bytes, so a tap's row offset is added to it directly
+    if (lane == 0) {
+        const int m = warp;
+        const uint32_t in_s = (uint32_t)__cvta_generic_to_shared(in), w_s = (uint32_t)__cvta_generic_to_shared(sm.wt);
+        const uint64_t a0 = umma_desc(in_s + 16u * 128u * m, 16u * rows, 128u), b0 = umma_desc(w_s + 512u * 9 * layer, 256u, 128u);
+        if (m < BLOCKS) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) umma_bf16(sm.tmem + 16u * m, a0 + (uint64_t)((k / 3) * IW + (k % 3)), b0 + (uint64_t)(32 * k), k > 0);
+        }
+        umma_commit(&sm.bar);  // with nothing issued it arrives at once
+    }
+    const bool ok = mbar_wait(&sm.bar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    if (!ok) return false;
+    auto emit = [&](int m, const float (&v)[16]) {
+        const int q = 128 * m + 32 * warp + lane, oy = q / IW, ox = q - oy * IW;
+        if (oy < OW && ox < OW) {
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                packed[i] = pack_bf16(fmaxf(v[2 * i] + bias[2 * i], 0.0f), fmaxf(v[2 * i + 1] + bias[2 * i + 1], 0.0f));
+            store(oy * OW + ox, packed);
+        }
+    };
+    const uint32_t tl = sm.tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll
+    for (int m = 0; m < BLOCKS; m += 2) {  // two loads in flight, then one wait
+        float v0[16], v1[16];
+        tmem_ld16_nowait(tl + 16u * m, v0);
+        if (m + 1 < BLOCKS) tmem_ld16_nowait(tl + 16u * (m + 1), v1);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        emit(m, v0);
+        if (m + 1 < BLOCKS) emit(m + 1, v1);
+    }
+    return true;
 }
 
 // Layer 0 (2 -> 16) on the tensor cores, 22 x 22 outputs from the 24 x 24 feature window: each FP32 feature enters as
 // a bfloat16 head and the bfloat16 of its remainder (k = 4 tap + 2 part + channel), so the products keep about 16 bits
-// of it; one 32-bit load gives a lane both channels of a pixel's part. Warp w takes m tiles w, w + 4, ...
+// of it; one 32-bit load gives a lane both channels of a pixel's part. Warp w takes m tiles w, w + 4, ... The output
+// goes to layer 1's two planes (channels 8 j .. 8 j + 7 of pixel p in plane j, row p).
 __device__ __forceinline__ void mma_layer0(const uint32_t (*fin)[2], uint32_t *out, const uint32_t *frags, const float *bias)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -376,7 +455,7 @@ __device__ __forceinline__ void mma_layer0(const uint32_t (*fin)[2], uint32_t *o
                 const int pr = 16 * mt + g + 8 * hrow;
                 if (pr >= npx) continue;
                 const float v0 = fmaxf(c[j][2 * hrow] + bias[ch], 0.0f), v1 = fmaxf(c[j][2 * hrow + 1] + bias[ch + 1], 0.0f);
-                out[pr * 8 + phys_half(pr, j) * 4 + t] = pack_bf16(v0, v1);
+                out[j * (kL1Rows * 4) + pr * 4 + t] = pack_bf16(v0, v1);  // plane j, row pr
             }
         }
     }
@@ -413,24 +492,51 @@ __device__ __forceinline__ float mma_head(const uint32_t *in, const uint32_t *fr
     return sum;
 }
 
-// Persistent: each block loads the parameters once, then takes tiles from a counter (need[total_tiles]) until none
-// is left.
+// Persistent: each block loads the parameters once, allocates its tensor-memory columns, then takes tiles from a
+// counter (need[total_tiles]) until none is left. Should a product never complete (a bounded wait), the block stops
+// using the tensor cores and gives every tile it takes the prediction +inf, so those tiles are computed exactly.
 __global__ void __launch_bounds__(kPT, 5) predict_kernel(const __grid_constant__ PredBatch b)
 {
     __shared__ PredSmem sm;
     __shared__ int next;
+    uint32_t(*feat)[2] = (uint32_t(*)[2])sm.a2;
+    static_assert(kFeatTile * kFeatTile * 2 <= 400 * 4, "the features stay below layer 2's padding rows");
     const int tid = threadIdx.x;
     if (tid < 16) sm.b0[tid] = b.params[net_b(0) + tid];
     for (int i = tid; i < 145; i += kPT) sm.w3[i] = b.params[net_w(3) + i];
     if (tid < 32) sm.b12[tid >> 4][tid & 15] = b.params[(tid < 16 ? net_b(1) : net_b(2)) + (tid & 15)];
+    // the planes past the pictures stay zero (only dropped output rows read them)
+    for (int i = tid; i < 2 * kL1Rows; i += kPT) ((uint4 *)sm.a1)[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < 2 * kL2Rows; i += kPT) ((uint4 *)sm.a2)[i] = make_uint4(0, 0, 0, 0);
+    // layers 1 and 2's weights from their mma.sync fragments (word i: layer 1 + (i / 128) / 9, tap (i / 128) % 9,
+    // n = 8 ((i / 64) % 2) + (i % 32) / 4, input channels c, c + 1 with c = 2 (i % 4) + 8 ((i / 32) % 2)) into the
+    // tensor cores' K-major tiles: half c / 8, row n, word (c % 8) / 2
+    for (int i = tid; i < kNetFrags12; i += kPT) {
+        const int lane = i & 31, r = (i >> 5) & 1, j = (i >> 6) & 1, lk = i >> 7, n = 8 * j + (lane >> 2);
+        sm.wt[lk * 128 + r * 64 + n * 4 + (lane & 3)] = b.frags[i];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(&sm.bar)), "r"(kPT / 32));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(&sm.tmem)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    uint32_t phase = 0;
+    bool broken = false;
     for (;;) {
         __syncthreads();  // every thread is done with the previous tile (and with `next`)
         if (tid == 0) next = (int)atomicAdd(b.need + b.total_tiles, 1u);
         __syncthreads();
         const int gt = next;
         if (gt >= b.total_tiles) break;
-        if (!b.need[gt]) {  // no pixel of the tile needs a c-value: nothing to predict (the same for the block)
-            if (tid == 0) b.pred[gt] = -INFINITY;
+        if (!b.need[gt] || broken) {  // nothing to predict, or no tensor cores: the same for the whole block
+            if (tid == 0) b.pred[gt] = b.need[gt] ? INFINITY : -INFINITY;
             continue;
         }
         const int j = find_job(b.njobs, gt, [&](int k) { return b.job[k].first_tile; });
@@ -443,23 +549,38 @@ __global__ void __launch_bounds__(kPT, 5) predict_kernel(const __grid_constant__
             float2 f = make_float2(0.0f, 0.0f);
             if (gu >= 0 && gu < fw && gv >= 0 && gv < fh) f = J.feat[(size_t)gv * fw + gu];
             const float h0 = bf16r(f.x), h1 = bf16r(f.y);
-            sm.f[i][0] = pack_bf16(h0, h1);
-            sm.f[i][1] = pack_bf16(f.x - h0, f.y - h1);  // the remainders are exact in FP32
+            feat[i][0] = pack_bf16(h0, h1);
+            feat[i][1] = pack_bf16(f.x - h0, f.y - h1);  // the remainders are exact in FP32
         }
         __syncthreads();
-        // the B fragments come from global memory (L1-resident: 13 KB for all blocks), leaving shared memory to the planes
-        mma_layer0(sm.f, sm.a1, b.frags + kNetFrags3, sm.b0);                   // layer 0: 22 x 22
-        __syncthreads();
-        mma_layer(sm.a1, 22, sm.a2, 20, b.frags, sm.b12[0]);                    // layer 1: 20 x 20
-        __syncthreads();
-        mma_layer(sm.a2, 20, sm.a1, 18, b.frags + 9 * 2 * 2 * 32, sm.b12[1]);   // layer 2: 18 x 18, into a1
-        __syncthreads();
+        // layer 0's B fragments come from global memory (L1-resident), layers 1 and 2's from `wt`
+        mma_layer0(feat, sm.a1, b.frags + kNetFrags3, sm.b0);  // layer 0: 22 x 22, into layer 1's planes
+        bool ok = umma_layer<22, 20, kL1Blocks>(sm, sm.a1, kL1Rows, 0, phase, sm.b12[0], [&](int q, const uint32_t(&pk)[8]) {
+            ((uint4 *)sm.a2)[q] = make_uint4(pk[0], pk[1], pk[2], pk[3]);  // layer 1: 20 x 20, into layer 2's planes
+            ((uint4 *)sm.a2)[kL2Rows + q] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        });
+        if (ok)
+            ok = umma_layer<20, 18, kL2Blocks>(sm, sm.a2, kL2Rows, 1, phase, sm.b12[1], [&](int q, const uint32_t(&pk)[8]) {
+                // layer 2: 18 x 18, into a1 in the head's layout
+                *(uint4 *)(sm.a1 + q * 8 + phys_half(q, 0) * 4) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                *(uint4 *)(sm.a1 + q * 8 + phys_half(q, 1) * 4) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            });
+        if (__syncthreads_or(!ok)) {
+            broken = true;
+            if (tid == 0) b.pred[gt] = INFINITY;
+            continue;
+        }
         // layer 3: 16 -> 1 on 16 x 16 (tensor cores), then the tile mean (a fixed order of additions)
         const float s = mma_head(sm.a1, b.frags + kNetFrags12);
         if ((tid & 31) == 0) sm.part[tid >> 5] = s;
         __syncthreads();
         if (tid == 0) b.pred[gt] = ((sm.part[0] + sm.part[1]) + (sm.part[2] + sm.part[3])) / 256.0f + sm.w3[144];
     }
+    if (broken) mbar_wait(&sm.bar, phase ^ 1u);  // once more, bounded, for the products that did not complete
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTmemCols));
 }
 
 // ---------------------------------------------------------------------------------------------------------------
