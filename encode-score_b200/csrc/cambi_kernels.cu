@@ -184,7 +184,13 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
         cnt += hv[q];
     }
     uint32_t m0 = hmode(yb - 1), m1 = hmode(yb);
-    uint32_t fsum = 0, fmask = 0, fn = 0;  // features of this lane's two columns over the current 4 rows
+    // features of this lane's two columns over the current 4 rows, as 16-bit pairs (a pair holds 2 rows of sums of
+    // values below 2^15, then it is folded into fsum; counts up to 4)
+    uint32_t fsum = 0, fsum2 = 0, fmask2 = 0, fn2 = 0;
+    // the smallest (value - need_lo) of the lane's masked pixels per half, wrapping for values below need_lo: a pixel
+    // needs a c-value when it is at most need_span (unmasked pixels count as 0x8000, above any span)
+    const uint32_t lo2 = (uint32_t)(b.need_lo & 0x7FFF) * 0x10001u;
+    uint32_t dmin = 0xFFFFFFFFu;
     bool need = false;
 #pragma unroll
     for (int i = 0; i < 8; i++) {
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
         cnt += hv[i + 6];
         const uint32_t m2 = hmode(y + 1);
         uint32_t v2 = mode3x2(m0, m1, m2);
-        if (y == 0 || y == h - 1) v2 = pair(y - ys, c);
+        if (y == 0 || y == h - 1) v2 = pair(y - ys, c);  // (the same for the whole warp)
         const uint32_t mk = (cnt + idx2) & 0x80008000u;
         const uint32_t word2 = v2 | mk;
         if (y < h) {
@@ -206,17 +212,21 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
             if ((i & 1) == 0 && x < w) dw[4 * g + i / 2 + 1][lane + 1] = (uint16_t)word2;
             if (feat) {
                 const uint32_t ok = (x + 1 < w) ? 0xFFFFFFFFu : (x < w ? 0x0000FFFFu : 0u);
-                const uint32_t vk = v2 & ok, mm = (mk >> 15) & ok & 0x10001u;
-                fsum += (vk & 0xFFFFu) + (vk >> 16);
-                fmask += (mm & 1u) + (mm >> 16);
-                fn += (ok & 1u) + (ok >> 31);
-                uint32_t hit;
+                const uint32_t mm = (mk >> 15) & ok & 0x10001u;
+                fsum2 += v2 & ok;
+                if (i & 1) {
+                    fsum += (fsum2 & 0xFFFFu) + (fsum2 >> 16);
+                    fsum2 = 0;
+                }
+                fmask2 += mm;
+                fn2 += ok & 0x10001u;
+                uint32_t hit = 0;
                 if (need_range) {
-                    // a masked value in lo .. lo + span, per half (the unsigned difference wraps below lo)
-                    hit = (((v2 & 0xFFFFu) - b.need_lo) <= (unsigned)b.need_span && (mk & 0x8000u) && (ok & 1u)) ||
-                          (((v2 >> 16) - b.need_lo) <= (unsigned)b.need_span && (mk >> 31) && (ok >> 31));
+                    // per half (value | 0x8000) - need_lo never borrows; flipping bit 15 leaves value - need_lo
+                    // modulo 2^16, which is at most need_span exactly when the value is in the range
+                    const uint32_t d = ((((v2 | 0x80008000u) - lo2) & (mm * 0xFFFFu)) ^ 0x80008000u);
+                    dmin = vmin_u16x2(dmin, d);
                 } else {
-                    hit = 0;
                     for (int k = 0; k < 2; k++) {
                         const uint16_t code = code_of((uint16_t)(word2 >> (16 * k)), b.band);
                         if (((ok >> (16 * k)) & 1u) && code != kNone && ((needbits[code >> 5] >> (code & 31)) & 1u)) hit = 1;
@@ -230,6 +240,8 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
         m1 = m2;
         if (feat && (i & 3) == 3) {
             // the 4 x 4 block of columns x - 2 l % 4 .. + 3: this lane's pair and its neighbour's
+            fsum += (fsum2 & 0xFFFFu) + (fsum2 >> 16);  // a last row past the picture leaves a pair unfolded
+            uint32_t fmask = (fmask2 & 0xFFFFu) + (fmask2 >> 16), fn = (fn2 & 0xFFFFu) + (fn2 >> 16);
             fsum += __shfl_xor_sync(0xffffffffu, fsum, 1);
             fmask += __shfl_xor_sync(0xffffffffu, fmask, 1);
             fn += __shfl_xor_sync(0xffffffffu, fn, 1);
@@ -241,10 +253,11 @@ __global__ void __launch_bounds__(256, 5) prep0_kernel(const __grid_constant__ P
                                           : fn ? (float)(((double)fsum / (double)fn - 512.0) / 256.0) : 0.0f;
                 J.feat[(size_t)v4 * fw + u] = make_float2(f0, __fmul_rn((float)fmask, 0.0625f));
             }
-            fsum = fmask = fn = 0;
+            fsum = fsum2 = fmask2 = fn2 = 0;
         }
     }
     if (feat) {
+        if (need_range) need = (dmin & 0xFFFFu) <= (unsigned)b.need_span || (dmin >> 16) <= (unsigned)b.need_span;
         need = __syncthreads_or(need);
         if (tid == 0) J.need[t] = need ? 1u : 0u;
     }
