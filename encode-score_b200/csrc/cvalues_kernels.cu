@@ -30,7 +30,7 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCvChunk = 4;                   // rows whose c-values are computed together (threads = 4 x tile width)
 // One column-count buffer, slid by one row between the rows' window counts (a slide and two barriers per row): two or
 // four buffers, each slid by two or four rows so that rows share barriers, measured slower (more slide work).
-constexpr int kListCap = 1024;                // positive c-values buffered per block before a flush
+constexpr int kListCap = 2048;                // positive c-values buffered per block before a flush (1024: 1 % slower)
 constexpr unsigned kNoRank = 0xFFu;           // rank plane: no relevant code
 constexpr int kMaxPlaneRank = 254;            // ranks a plane of absolute ranks can hold
 
